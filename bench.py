@@ -1,0 +1,421 @@
+#!/usr/bin/env python3
+"""Benchmark: Pi grid-points x scales per second on one or more B200s.
+
+Default workload (one step): compute_Π! on the 0.25-degree global sphere, 1440 x 720 cells,
+Gaussian alpha = 4, l = 100 km, ZeroFill, ~30% land -- one scale x one snapshot per GPU per step
+(weak scaling: every rank takes its own seeded snapshot).  Other workloads (--workload):
+  sweep24x8 : 24 scales (50-2000 km, log-spaced) x 8 snapshots per step, Pi and E(l)
+  cart256   : 256^2 doubly periodic Cartesian, dx = 1 km, l = 8 km (separable engine)
+  levels40  : regional 400 x 600 x 40 levels, FP32 storage, 6 scales 25-400 km, one mask per level
+
+`value` times the device-resident path (inputs already in HBM, an L2 flush between steps inside
+the timed region); `e2e` times the host C-ABI call (pinned host inputs copied in, Pi copied out)
+every step.  `--impl reference` times the CPU FP64 oracle -- the restated threaded reference path
+-- on the host's cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "coarsegrainingenergyfluxes.jl_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "Π grid-points×scales/s, 0.25° sphere; plain vs batched/closure; rel-L2 vs FP64"
+UNIT = "grid-points*scales/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sphere1", choices=["sphere1", "sweep24x8", "cart256", "levels40"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------------------------
+def sweep_scales():
+    return [50e3 * 40.0 ** (s / 23.0) for s in range(24)]
+
+
+def make_workload(name: str, rank: int):
+    """Returns dict(grid, u, v, scales, slice_masks, kernel, nslices, desc)."""
+    import cgef_b200 as cg
+    from cgef_b200 import synthetic as S
+    if name == "sphere1":
+        g = S.sphere_grid()
+        g = g.with_mask(S.land_mask(g, seed=1))
+        u, v = S.sphere_fields(g, seed=100 + rank)
+        return dict(grid=g, u=u[None], v=v[None], scales=[1e5], slice_masks=None, kernel=cg.GaussianKernel(4.0),
+                    desc="sphere-0.25deg-1440x720-gauss-a4-l100km-zerofill-30pct-land",
+                    dtype="f64")
+    if name == "sweep24x8":
+        g = S.sphere_grid()
+        g = g.with_mask(S.land_mask(g, seed=1))
+        us, vs = zip(*[S.sphere_fields(g, seed=100 + 8 * rank + t) for t in range(8)])
+        return dict(grid=g, u=np.stack(us), v=np.stack(vs), scales=sweep_scales(), slice_masks=None,
+                    kernel=cg.GaussianKernel(4.0),
+                    desc="sphere-0.25deg-1440x720-gauss-a4-24scales-50to2000km-x8snapshots-zerofill-30pct-land",
+                    dtype="f64")
+    if name == "cart256":
+        g = S.cartesian_grid()
+        u, v = S.cartesian_fields(seed=rank)
+        return dict(grid=g, u=u[None], v=v[None], scales=[8000.0], slice_masks=None, kernel=cg.GaussianKernel(4.0),
+                    desc="cartesian-256x256-dx1km-periodic-gauss-a4-l8km-zerofill", dtype="f64")
+    grid, U, V, M, _ = S.regional_levels(seed=2 + rank)
+    scales = [25e3 * 16.0 ** (s / 5.0) for s in range(6)]
+    return dict(grid=grid, u=U, v=V, scales=scales, slice_masks=M, kernel=cg.GaussianKernel(4.0),
+                desc="regional-0.25deg-400x600x40levels-f32-gauss-a4-6scales-25to400km-per-level-masks",
+                dtype="f32")
+
+
+def algorithmic_flops(plans, grid, nslices, slice_masks) -> float:
+    """Sum over active targets of footprint entries x K x 2 (K = 9 on the sphere, 5 on the plane)."""
+    K = 9 if grid.is_spherical else 5
+    total = 0.0
+    for p in plans:
+        if p.engine == "banded":
+            _, _, _, ptr = p.footprint()
+            n = np.diff(ptr).astype(np.float64)
+            if slice_masks is not None:
+                act = slice_masks.reshape(nslices, grid.ny, grid.nx).sum(axis=(0, 2)).astype(np.float64)
+            else:
+                m = np.ones(grid.shape) if grid.mask is None else grid.mask
+                act = m.sum(axis=1).astype(np.float64) * nslices
+            if n.size == 1:
+                n = np.full(grid.ny, n[0])
+            total += float((act * n).sum()) * K * 2
+        elif p.engine == "separable":
+            total += grid.nx * grid.ny * nslices * 2 * (2 * p.info.di_max + 1 + 2 * p.info.dj_lim + 1) * K
+    return total
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        self.proc = None
+        self.dev = device_index
+
+    def _smi_index(self):
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.dev)
+            return "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+        except Exception:
+            return str(self.dev)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self._smi_index(), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[4:]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        sm = [r[0] for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, val in zip(names, r[2][1:]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(r[1] for r in rows), "samples": len(rows),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU baseline / reference arm: the FP64 oracle's threaded path
+# ---------------------------------------------------------------------------------------------
+def oracle_rate(wl, budget_s: float, max_steps: int, warmup: int = 1):
+    import oracle as O
+    g = wl["grid"]
+    nthreads = O.max_threads()
+    nsl = wl["u"].shape[0]
+    scales = wl["scales"]
+    n_units = g.nx * g.ny
+    # one unit of work = Pi for one (slice, scale); run units round-robin until the budget ends
+    units = [(t, s) for s in range(len(scales)) for t in range(nsl)]
+    plans = {}
+
+    def plan_for(t, s):
+        key = (t if wl["slice_masks"] is not None else -1, s)
+        if key not in plans:
+            m = wl["slice_masks"][t] if wl["slice_masks"] is not None else g.mask
+            og = O.Grid(O.SPHERE if g.is_spherical else O.CART, g.nx, g.ny, g.x.start, g.x.step, g.y.start,
+                        g.y.step, g.geometry.R if g.is_spherical else 6.371e6, g.periodic[0], g.periodic[1], m)
+            plans[key] = O.Plan(og, O.GAUSSIAN, wl["kernel"].alpha, scales[s], O.ZEROFILL)
+        return plans[key]
+
+    def unit(k):
+        t, s = units[k % len(units)]
+        p = plan_for(t, s)
+        u = np.asarray(wl["u"][t], dtype=np.float64)
+        v = np.asarray(wl["v"][t], dtype=np.float64)
+        p.compute_pi(u, v, nthreads)
+
+    # warm-up (also builds the plans), then timed units
+    for k in range(min(warmup, len(units))):
+        plan_for(*units[k])
+    for k in range(warmup):
+        unit(k)
+    done = 0
+    t0 = time.perf_counter()
+    while done < max_steps * len(units):
+        unit(done)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    sample = f"{done} x compute_Pi unit(s) of {g.nx}x{g.ny} ({'/'.join(str(int(x)) for x in scales[:1])} m ...)"
+    return n_units * done / el, nthreads, done, el, sample
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        wl = make_workload(args.workload, 0)
+        steps = args.steps if args.steps is not None else 3
+        rate, nth, done, el, sample = oracle_rate(wl, budget_s=150.0, max_steps=steps, warmup=min(args.warmup, 1))
+        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded)", "config": {"workload": wl["desc"], "nx": wl["grid"].nx,
+                                                          "ny": wl["grid"].ny, "scales": len(wl["scales"]),
+                                                          "snapshots": int(wl["u"].shape[0])},
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
+                                 "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path"},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import cgef_b200 as cg
+    from cgef_b200 import _lib
+
+    wl = make_workload(args.workload, rank)
+    g = wl["grid"]
+    nsl = int(wl["u"].shape[0])
+    ns = len(wl["scales"])
+    plans = [cg.plan_filter(g.with_mask(None) if wl["slice_masks"] is not None else g, wl["kernel"], s)
+             for s in wl["scales"]]
+    L = _lib.load()
+    tdt = torch.float32 if wl["dtype"] == "f32" else torch.float64
+    du = torch.from_numpy(np.ascontiguousarray(wl["u"])).to(device="cuda", dtype=tdt)
+    dv = torch.from_numpy(np.ascontiguousarray(wl["v"])).to(device="cuda", dtype=tdt)
+    dm = None if wl["slice_masks"] is None else torch.from_numpy(wl["slice_masks"].astype(np.uint8)).cuda()
+    dt_code = _lib.F32 if tdt == torch.float32 else _lib.F64
+    import ctypes as C
+    parr = (C.c_void_p * ns)(*[p.handle.value for p in plans])
+    dPi = torch.empty((nsl, ns) + g.shape, dtype=tdt, device="cuda")
+    dE = torch.empty((nsl, ns), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        _lib.check(L.cgef_sweep_device(parr, ns, dt_code, du.data_ptr(), dv.data_ptr(), nsl,
+                                       None if dm is None else dm.data_ptr(), dPi.data_ptr(), dE.data_ptr(),
+                                       stream.cuda_stream))
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    steps = args.steps
+    if steps is None:
+        # about 5 s of timed work
+        step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        per = (time.perf_counter() - t0) / 3
+        steps = int(max(10, min(5000, 5.0 / max(per, 1e-6))))
+    for _ in range(max(args.warmup, 3)):
+        flush.fill_(1.0)
+        step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    L.cgef_reset_launch_count()
+    L.cgef_profile_reset()
+    L.cgef_profile_enable(1)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        flush.fill_(1.0)
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    L.cgef_profile_enable(0)
+    launches = int(L.cgef_launch_count())
+    clocks = sampler.stop()
+    elapsed_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    units_per_step = g.nx * g.ny * ns * nsl
+    value = world * units_per_step * steps / (elapsed_ms / 1e3)
+
+    # dominant kernel timing (CUDA events on the launch stream, inside the timed region)
+    kinds = {"banded": _lib.KERNEL_BANDED, "separable": _lib.KERNEL_SEPARABLE, "prefixsum": _lib.KERNEL_PREFIX}
+    kind = kinds[plans[0].engine]
+    tot = C.c_double()
+    cnt = C.c_int64()
+    _lib.check(L.cgef_profile_read(kind, C.byref(tot), C.byref(cnt)))
+    per_launch_ms = tot.value / max(cnt.value, 1)
+    flops_step = algorithmic_flops(plans, g, nsl, wl["slice_masks"])
+    launches_per_step = max(cnt.value // steps, 1)
+    flops_launch = flops_step / launches_per_step
+    peak = None
+    try:
+        pk = C.CDLL(os.path.join(ROOT, "coarsegrainingenergyfluxes.jl_b200", "cgef_b200", "libcgef_peak.so"))
+        pk.cgef_peak_fp64_tflops.restype = C.c_double
+        pk.cgef_peak_fp64_tflops.argtypes = [C.c_int]
+        peak = float(pk.cgef_peak_fp64_tflops(local))
+    except Exception:
+        peak = None
+    achieved = flops_launch / (per_launch_ms * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"{args.workload}:{plans[0].engine}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak and peak > 0 else None, "traffic": traffic,
+                "kernel": f"banded_kernel (FP64 FMA footprint gather, {plans[0].engine})",
+                "per_launch_ms": per_launch_ms, "launches": int(cnt.value),
+                "algorithmic_flops_per_launch": flops_launch,
+                "peak_source": "measured: DFMA loop over all SMs on this GPU (libcgef_peak.so), "
+                               "nominal B200 FP64 37 TFLOP/s; MEASURED_PEAKS.json holds no FP64 figure"}
+
+    # end to end through the host C ABI: pinned inputs in, Pi (and E) out, every step
+    e2e = None
+    if True:  # every rank, so the barriers pair up
+        hu = torch.from_numpy(np.ascontiguousarray(wl["u"])).to(dtype=tdt).pin_memory()
+        hv = torch.from_numpy(np.ascontiguousarray(wl["v"])).to(dtype=tdt).pin_memory()
+        hPi = torch.empty((nsl, ns) + g.shape, dtype=tdt).pin_memory()
+        hE = torch.empty((nsl, ns), dtype=torch.float64).pin_memory()
+        hm = None if wl["slice_masks"] is None else torch.from_numpy(wl["slice_masks"].astype(np.uint8)).pin_memory()
+
+        def host_step():
+            _lib.check(L.cgef_sweep(parr, ns, dt_code, hu.data_ptr(), hv.data_ptr(), nsl,
+                                    None if hm is None else hm.data_ptr(), hPi.data_ptr(), hE.data_ptr()))
+
+        host_step()
+        n_e2e = args.e2e_steps if args.e2e_steps is not None else max(3, min(steps, 200))
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            host_step()
+        el = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([el], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        bsz = 4 if tdt == torch.float32 else 8
+        e2e = {"value": world * units_per_step * n_e2e / el, "unit": UNIT,
+               "h2d_bytes_per_step": int(2 * nsl * g.nx * g.ny * bsz + (0 if hm is None else hm.numel())),
+               "d2h_bytes_per_step": int(nsl * ns * g.nx * g.ny * bsz + nsl * ns * 8), "steps": n_e2e,
+               "timing": "wall clock around synchronous cgef_sweep calls (host buffers, pinned)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, nth, done, el, sample = oracle_rate(wl, budget_s=20.0, max_steps=1, warmup=1)
+        cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
+               "sample": sample + f", {el:.1f} s; CPU {cpu_model()}; restated reference threaded path (FP64 oracle, OpenMP rows)"}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if wl["dtype"] == "f64" else "f64 (f32 storage)", "data": "synthetic (seeded)",
+            "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": nsl,
+                       "active_fraction": float(1.0 if g.mask is None else g.mask.mean()),
+                       "l2": "flushed between steps (256 MiB write, inside the timed region)",
+                       "parallelism": f"{world} rank(s), independent snapshots per rank"},
+            "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,136 @@
+"""ctypes binding of libcgef_b200.so (the C ABI of include/cgef_b200.h).
+
+The library is the product: every compute call below runs CUDA kernels.  There is no CPU
+fallback -- a missing library or device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+from . import build as _build
+
+CGEF_OK = 0
+CGEF_EINVAL = -1
+CGEF_ENOMEM = -2
+CGEF_ECUDA = -3
+CGEF_ESTRATEGY = -4
+CGEF_EUNSUPPORTED = -5
+CGEF_ENODEVICE = -6
+
+CARTESIAN, SPHERICAL = 0, 1
+TOPHAT, GAUSSIAN = 0, 1
+ZEROFILL, DEFORMABLE = 0, 1
+ENGINE_AUTO, ENGINE_BANDED, ENGINE_SEPARABLE, ENGINE_PREFIXSUM = 0, 1, 2, 3
+F64, F32 = 0, 1
+
+# Every symbol include/cgef_b200.h declares.
+EXPORTED = [
+    "cgef_version", "cgef_last_error", "cgef_device_count", "cgef_plan_create", "cgef_plan_destroy",
+    "cgef_plan_get_info", "cgef_plan_get_footprint", "cgef_filter", "cgef_filter_batch", "cgef_compute_pi",
+    "cgef_cumulative_energy", "cgef_sweep", "cgef_ddx", "cgef_ddy", "cgef_filter_device",
+    "cgef_compute_pi_device", "cgef_sweep_device", "cgef_launch_count", "cgef_reset_launch_count",
+    "cgef_profile_enable", "cgef_profile_read", "cgef_profile_reset",
+]
+KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN = 0, 1, 2, 3, 4
+
+
+class GridDesc(C.Structure):
+    _fields_ = [
+        ("geometry", C.c_int32), ("periodic_x", C.c_int32), ("periodic_y", C.c_int32), ("reserved", C.c_int32),
+        ("nx", C.c_int64), ("ny", C.c_int64),
+        ("x0", C.c_double), ("dx", C.c_double), ("y0", C.c_double), ("dy", C.c_double),
+        ("radius", C.c_double), ("mask", C.c_void_p),
+    ]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [
+        ("engine", C.c_int32), ("nbands", C.c_int32), ("nentries", C.c_int64), ("dj_lim", C.c_int32),
+        ("di_max", C.c_int32), ("kernel_radius", C.c_double), ("active_area", C.c_double),
+    ]
+
+
+class PiOutputs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in
+                ("pi", "ubar", "vbar", "tau_xx", "tau_xy", "tau_yy", "s_xx", "s_xy", "s_yy", "energy")]
+
+
+class CgefError(RuntimeError):
+    """A failed library call; `code` is the negative CGEF status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"cgef status {code}: {msg}")
+        self.code = code
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def library_path() -> str:
+    return _build.LIB_PATH
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Loads (building first, if needed and possible) libcgef_b200.so."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB_PATH
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise RuntimeError(f"libcgef_b200.so is not built ({path}); run `python -m cgef_b200.build`")
+        _build.build()
+    L = C.CDLL(path)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    L.cgef_version.restype = i32
+    L.cgef_last_error.restype = C.c_char_p
+    L.cgef_device_count.restype = i32
+    L.cgef_plan_create.argtypes = [C.POINTER(vp), C.POINTER(GridDesc), i32, dbl, dbl, i32, i32]
+    L.cgef_plan_create.restype = i32
+    L.cgef_plan_destroy.argtypes = [vp]
+    L.cgef_plan_destroy.restype = i32
+    L.cgef_plan_get_info.argtypes = [vp, C.POINTER(PlanInfo)]
+    L.cgef_plan_get_info.restype = i32
+    L.cgef_plan_get_footprint.argtypes = [vp, vp, vp, vp, vp]
+    L.cgef_plan_get_footprint.restype = i32
+    L.cgef_filter.argtypes = [vp, i32, vp, vp, i64]
+    L.cgef_filter.restype = i32
+    L.cgef_filter_batch.argtypes = [vp, i32, vp, vp, i32]
+    L.cgef_filter_batch.restype = i32
+    L.cgef_compute_pi.argtypes = [vp, i32, vp, vp, i64, vp, C.POINTER(PiOutputs)]
+    L.cgef_compute_pi.restype = i32
+    L.cgef_cumulative_energy.argtypes = [vp, i32, i32, vp, vp, vp]
+    L.cgef_cumulative_energy.restype = i32
+    L.cgef_sweep.argtypes = [vp, i32, i32, vp, vp, i64, vp, vp, vp]
+    L.cgef_sweep.restype = i32
+    L.cgef_ddx.argtypes = [vp, i32, vp, vp]
+    L.cgef_ddx.restype = i32
+    L.cgef_ddy.argtypes = [vp, i32, vp, vp]
+    L.cgef_ddy.restype = i32
+    L.cgef_filter_device.argtypes = [vp, i32, vp, vp, i64, vp]
+    L.cgef_filter_device.restype = i32
+    L.cgef_compute_pi_device.argtypes = [vp, i32, vp, vp, i64, vp, C.POINTER(PiOutputs), vp]
+    L.cgef_compute_pi_device.restype = i32
+    L.cgef_sweep_device.argtypes = [vp, i32, i32, vp, vp, i64, vp, vp, vp, vp]
+    L.cgef_sweep_device.restype = i32
+    L.cgef_launch_count.restype = i64
+    L.cgef_reset_launch_count.restype = None
+    L.cgef_profile_enable.argtypes = [i32]
+    L.cgef_profile_enable.restype = None
+    L.cgef_profile_read.argtypes = [i32, C.POINTER(dbl), C.POINTER(i64)]
+    L.cgef_profile_read.restype = i32
+    L.cgef_profile_reset.restype = None
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != CGEF_OK:
+        msg = load().cgef_last_error().decode(errors="replace")
+        raise CgefError(rc, msg)
+
+
+def device_count() -> int:
+    return int(load().cgef_device_count())

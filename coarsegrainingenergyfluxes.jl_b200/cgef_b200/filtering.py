@@ -1,0 +1,203 @@
+"""Filter plans and applies (Filtering.jl's public API for the real-space path).
+
+`plan_filter` builds the footprint once and keeps it resident on the GPU, as the reference's
+GPU extension does through `prepare_workspace` (Filtering.jl:2910-2912, 2931-2954); every
+`filter_apply*` call then runs the CUDA engines of libcgef_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _arrays as A
+from . import _lib
+from .errors import ArgumentError, DimensionMismatch
+from .grids import StructuredGrid
+from .kernels import AbstractFilterKernel, GaussianKernel, TopHatKernel
+
+
+class AbstractMaskStrategy:
+    code = -1
+
+    def __eq__(self, other):
+        return type(self) is type(other)
+
+    def __hash__(self):
+        return hash(type(self))
+
+    def __repr__(self):
+        return f"{type(self).__name__}()"
+
+
+class ZeroFill(AbstractMaskStrategy):
+    """Masked cells count in the denominator as zero-valued (Filtering.jl:36-48)."""
+
+    code = _lib.ZEROFILL
+
+
+class Deformable(AbstractMaskStrategy):
+    """Masked cells leave numerator and denominator (Filtering.jl:50-57)."""
+
+    code = _lib.DEFORMABLE
+
+
+_ENGINES = {"auto": _lib.ENGINE_AUTO, "banded": _lib.ENGINE_BANDED, "separable": _lib.ENGINE_SEPARABLE,
+            "prefixsum": _lib.ENGINE_PREFIXSUM}
+_ENGINE_NAMES = {v: k for k, v in _ENGINES.items()}
+
+
+def _validate_scale(scale: float) -> None:
+    # Filtering.jl:2917-2922
+    if not (np.isfinite(scale) and scale > 0):
+        raise ArgumentError(f"filter scale must be finite and positive, got {scale}")
+
+
+class PhysicalFilterPlan:
+    """A prebuilt, device-resident filter (Filtering.jl:2894-2901)."""
+
+    def __init__(self, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float,
+                 mask_strategy: AbstractMaskStrategy = ZeroFill(), engine: str = "auto"):
+        if not isinstance(grid, StructuredGrid):
+            raise ArgumentError("plan_filter needs a StructuredGrid")
+        if not isinstance(kernel, (TopHatKernel, GaussianKernel)):
+            raise ArgumentError(f"{type(kernel).__name__} is outside the supported path (TopHat, Gaussian)")
+        _validate_scale(float(scale))
+        if engine not in _ENGINES:
+            raise ArgumentError(f"engine must be one of {sorted(_ENGINES)}")
+        L = _lib.load()
+        keep: list = []
+        desc = grid._desc(keep)
+        h = C.c_void_p()
+        _lib.check(L.cgef_plan_create(C.byref(h), C.byref(desc), kernel.code, float(kernel.alpha), float(scale),
+                                      mask_strategy.code, _ENGINES[engine]))
+        self._h = h
+        self.grid = grid
+        self.kernel = kernel
+        self.scale = float(scale)
+        self.strategy = mask_strategy
+        info = _lib.PlanInfo()
+        _lib.check(L.cgef_plan_get_info(h, C.byref(info)))
+        self.info = info
+        self.engine = _ENGINE_NAMES[info.engine]
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if self._h is None:
+            raise ArgumentError("plan has been closed")
+        return self._h
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and _lib._lib is not None:
+            _lib._lib.cgef_plan_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def footprint(self):
+        """The banded footprint in the reference's CSR form (di, dj, w, ptr), 0-based."""
+        n = int(self.info.nentries)
+        nb = int(self.info.nbands)
+        di = np.zeros(n, np.int32)
+        dj = np.zeros(n, np.int32)
+        w = np.zeros(n, np.float64)
+        ptr = np.zeros(nb + 1, np.int64)
+        _lib.check(_lib.load().cgef_plan_get_footprint(self.handle, di.ctypes.data, dj.ctypes.data,
+                                                       w.ctypes.data, ptr.ctypes.data))
+        return di, dj, w, ptr
+
+    def __repr__(self):
+        return (f"PhysicalFilterPlan(engine={self.engine}, kernel={self.kernel!r}, scale={self.scale}, "
+                f"strategy={self.strategy!r})")
+
+
+def plan_filter(grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
+                mask_strategy: AbstractMaskStrategy = ZeroFill(), engine: str = "auto") -> PhysicalFilterPlan:
+    """Filtering.plan_filter: engine dispatched as the reference does (Gaussian on the plane ->
+    separable, top-hat -> prefix sum, Gaussian on the sphere -> banded footprint)."""
+    return PhysicalFilterPlan(grid, kernel, scale, mask_strategy, engine)
+
+
+def _check_field(a, grid: StructuredGrid, name: str, batched: bool = False):
+    shp = tuple(a.shape)
+    if batched:
+        if len(shp) != 3 or shp[1:] != grid.shape:
+            raise DimensionMismatch(f"{name} has shape {shp}; expected (batch, {grid.ny}, {grid.nx})")
+    elif shp != grid.shape:
+        raise DimensionMismatch(f"{name} has shape {shp}; grid expects {grid.shape} (ny, nx)")
+
+
+def filter_apply_batched(out, field, plan: PhysicalFilterPlan):
+    """Filtering.filter_apply_batched! over a leading batch axis of shape (batch, ny, nx) -- the
+    reference's trailing batch axis in column-major order (Filtering.jl:3286-3305).  One fused launch
+    covers the whole batch."""
+    _check_field(field, plan.grid, "field", batched=True)
+    if out is None:
+        out = A.empty_like(field)
+    if tuple(out.shape) != tuple(field.shape):
+        raise DimensionMismatch(f"out {tuple(out.shape)} and field {tuple(field.shape)} differ")
+    L = _lib.load()
+    dt = A.dtype_code(field)
+    if A.dtype_code(out) != dt:
+        raise ArgumentError("out and field must share a dtype")
+    nb = int(field.shape[0])
+    if A.is_device(field):
+        _lib.check(L.cgef_filter_device(plan.handle, dt, A.ptr(field), A.ptr(out), nb, A.stream_of(field)))
+    else:
+        field = np.ascontiguousarray(field)
+        _lib.check(L.cgef_filter(plan.handle, dt, A.ptr(field), A.ptr(out), nb))
+    return out
+
+
+def filter_apply(out, field, plan: PhysicalFilterPlan):
+    """Filtering.filter_apply! (Filtering.jl:3242-3256) on one (ny, nx) field."""
+    _check_field(field, plan.grid, "field")
+    if out is None:
+        out = A.empty_like(field)
+    _check_field(out, plan.grid, "out")
+    filter_apply_batched(out.reshape((1,) + tuple(out.shape)), field.reshape((1,) + tuple(field.shape)), plan)
+    return out
+
+
+def filter_apply_batch(outs: Optional[Sequence], fields: Sequence, plan: PhysicalFilterPlan) -> List:
+    """Filtering.filter_apply_batch! (Filtering.jl:3360-3375): several fields, one traversal."""
+    fields = list(fields)
+    if outs is None:
+        outs = [A.empty_like(f) for f in fields]
+    outs = list(outs)
+    if len(outs) != len(fields):
+        raise DimensionMismatch("outs and fields must have equal length")
+    for f in fields:
+        _check_field(f, plan.grid, "field")
+    if any(A.is_device(f) for f in fields):
+        # device fields: one fused launch per field group through the batched entry point
+        for o, f in zip(outs, fields):
+            filter_apply(o, f, plan)
+        return outs
+    dt = A.dtype_code(fields[0])
+    hf = [np.ascontiguousarray(f) for f in fields]
+    K = len(hf)
+    fin = (C.c_void_p * K)(*[f.ctypes.data for f in hf])
+    fout = (C.c_void_p * K)(*[A.ptr(o) for o in outs])
+    _lib.check(_lib.load().cgef_filter_batch(plan.handle, dt, fin, fout, K))
+    return outs
+
+
+def filter_field(out, field, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
+                 mask_strategy: AbstractMaskStrategy = ZeroFill(), filter_plan: Optional[PhysicalFilterPlan] = None):
+    """Filtering.filter_field! (Filtering.jl:168-217): plan (unless given) then apply."""
+    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy)
+    return filter_apply(out, field, plan)
+
+
+def filter_fields(outs, fields, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
+                  mask_strategy: AbstractMaskStrategy = ZeroFill(), filter_plan: Optional[PhysicalFilterPlan] = None):
+    """Filtering.filter_fields!: several fields sharing one plan."""
+    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy)
+    return filter_apply_batch(outs, fields, plan)

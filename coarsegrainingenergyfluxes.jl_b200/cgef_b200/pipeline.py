@@ -1,0 +1,189 @@
+"""Scale sweeps (Pipeline.jl): Pi at every scale and slice, E(l), k_l and the spectral density.
+
+One C-ABI call (`cgef_sweep`) computes the whole (slice x scale) sweep on the GPU: the inputs are
+staged once, every scale's plan runs its fused footprint pass over all slices, and E(l) is read
+from the same filtered velocities (Pipeline.jl:455-463).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _arrays as A
+from . import _lib
+from .diagnostics import AbstractSpectrumPolicy, NoSpectrum, StrictSpectrum, gate_spectrum, spectral_density
+from .errors import ArgumentError, DimensionMismatch
+from .filtering import AbstractMaskStrategy, PhysicalFilterPlan, ZeroFill, plan_filter
+from .grids import StructuredGrid
+from .kernels import AbstractFilterKernel, TopHatKernel
+
+
+@dataclass
+class CoarseGrainResult:
+    """Pipeline.CoarseGrainResult (Pipeline.jl:270-284); Pi has shape (nscales, ny, nx)."""
+
+    scales: np.ndarray
+    Pi: object
+    cumulative_energy: np.ndarray
+    wavenumber: np.ndarray
+    filtering_spectrum: np.ndarray
+
+    @property
+    def Π(self):
+        return self.Pi
+
+
+@dataclass
+class CoarseGrainBatchResult:
+    """Pipeline.CoarseGrainBatchResult (Pipeline.jl:606-651): Pi (batch..., nscales, ny, nx),
+    per-scale vectors (batch..., nscales) -- the reference's trailing axes in C order."""
+
+    Pi: object
+    scales: np.ndarray
+    cumulative_energy: np.ndarray
+    wavenumber: np.ndarray
+    filtering_spectrum: np.ndarray
+    batch_size: tuple
+
+    @property
+    def Π(self):
+        return self.Pi
+
+    @property
+    def slices(self) -> List[CoarseGrainResult]:
+        nb = int(np.prod(self.batch_size)) if self.batch_size else 1
+        flatPi = self.Pi.reshape((nb,) + tuple(self.Pi.shape[-3:]))
+        out = []
+        for t in range(nb):
+            idx = np.unravel_index(t, self.batch_size) if self.batch_size else ()
+            out.append(CoarseGrainResult(self.scales[idx], flatPi[t], self.cumulative_energy[idx],
+                                         self.wavenumber[idx], self.filtering_spectrum[idx]))
+        return out
+
+
+def _plans(grid, kernel, scales, mask_strategy, filter_plans):
+    if filter_plans is not None:
+        plans = list(filter_plans)
+        if len(plans) != len(scales):
+            raise DimensionMismatch("filter_plans must hold one plan per scale")
+        return plans
+    return [plan_filter(grid, kernel, float(s), mask_strategy=mask_strategy) for s in scales]
+
+
+def _sweep(u, v, grid, plans, nb, slice_masks, want_pi=True):
+    dt = A.dtype_code(u)
+    if A.dtype_code(v) != dt:
+        raise ArgumentError("u and v must share a dtype")
+    ns = len(plans)
+    L = _lib.load()
+    arr = (C.c_void_p * ns)(*[p.handle.value for p in plans])
+    ny, nx = grid.shape
+    if A.is_device(u):
+        import torch
+        Pi = torch.empty((nb, ns, ny, nx), dtype=u.dtype, device=u.device) if want_pi else None
+        E = torch.empty((nb, ns), dtype=torch.float64, device=u.device)
+        m = None if slice_masks is None else A.mask_bytes(slice_masks, u)
+        _lib.check(L.cgef_sweep_device(arr, ns, dt, A.ptr(u), A.ptr(v), nb, None if m is None else A.ptr(m),
+                                       None if Pi is None else A.ptr(Pi), A.ptr(E), A.stream_of(u)))
+        return Pi, E.cpu().numpy()
+    u = np.ascontiguousarray(u)
+    v = np.ascontiguousarray(v)
+    Pi = np.empty((nb, ns, ny, nx), dtype=u.dtype) if want_pi else None
+    E = np.empty((nb, ns), dtype=np.float64)
+    m = None if slice_masks is None else A.mask_bytes(slice_masks)
+    _lib.check(L.cgef_sweep(arr, ns, dt, A.ptr(u), A.ptr(v), nb, None if m is None else A.ptr(m),
+                            None if Pi is None else A.ptr(Pi), E.ctypes.data))
+    return Pi, E
+
+
+def _spectrum(E, k, spectrum):
+    if isinstance(spectrum, NoSpectrum):
+        return np.full_like(E, np.nan)
+    return spectral_density(E, k)
+
+
+def coarse_grain(u, v, grid: StructuredGrid, *, scales: Sequence[float], w=None,
+                 kernel: AbstractFilterKernel = TopHatKernel(), mask_strategy: AbstractMaskStrategy = ZeroFill(),
+                 filter_plans: Optional[Sequence[PhysicalFilterPlan]] = None, L: float = 1.0,
+                 spectrum: AbstractSpectrumPolicy = StrictSpectrum()) -> CoarseGrainResult:
+    """Pipeline.coarse_grain (Pipeline.jl:342-360, 412-468) for one (ny, nx) slice."""
+    if w is not None:
+        raise ArgumentError("the vertical velocity w is outside the supported path; pass None")
+    if tuple(u.shape) != grid.shape or tuple(v.shape) != grid.shape:
+        raise DimensionMismatch(f"u and v must have the grid's shape {grid.shape}")
+    gate_spectrum(kernel, spectrum)
+    scales = np.asarray(scales, dtype=np.float64)
+    plans = _plans(grid, kernel, scales, mask_strategy, filter_plans)
+    Pi, E = _sweep(u, v, grid, plans, 1, None)
+    k = float(L) / scales
+    return CoarseGrainResult(scales.copy(), Pi[0], E[0], k, _spectrum(E[0], k, spectrum))
+
+
+def coarse_grain_batch(u, v, grid: StructuredGrid, *, scales: Sequence[float], w=None,
+                       kernel: AbstractFilterKernel = TopHatKernel(),
+                       mask_strategy: AbstractMaskStrategy = ZeroFill(),
+                       filter_plans: Optional[Sequence[PhysicalFilterPlan]] = None, L: float = 1.0,
+                       spectrum: AbstractSpectrumPolicy = StrictSpectrum(), slice_masks=None) -> CoarseGrainBatchResult:
+    """Pipeline.coarse_grain_batch! (Pipeline.jl:686-717): u, v of shape (batch..., ny, nx) share the
+    grid; the whole batch runs batch-native, one fused pass per scale (the GPU driver,
+    Pipeline.jl:519-563).  `slice_masks` (batch..., ny, nx) gives every slice its own mask."""
+    if w is not None:
+        raise ArgumentError("the vertical velocity w is outside the supported path; pass None")
+    shp = tuple(u.shape)
+    if len(shp) < 3 or shp[-2:] != grid.shape or tuple(v.shape) != shp:
+        raise DimensionMismatch(f"u and v must be (batch..., {grid.ny}, {grid.nx}) and equal")
+    bsz = shp[:-2]
+    nb = int(np.prod(bsz))
+    gate_spectrum(kernel, spectrum)
+    scales = np.asarray(scales, dtype=np.float64)
+    plans = _plans(grid, kernel, scales, mask_strategy, filter_plans)
+    Pi, E = _sweep(u.reshape((nb,) + grid.shape), v.reshape((nb,) + grid.shape), grid, plans, nb, slice_masks)
+    ns = len(scales)
+    k = float(L) / scales
+    spec = np.stack([_spectrum(E[t], k, spectrum) for t in range(nb)])
+    return CoarseGrainBatchResult(Pi.reshape(bsz + (ns,) + grid.shape), np.broadcast_to(scales, bsz + (ns,)).copy(),
+                                  E.reshape(bsz + (ns,)), np.broadcast_to(k, bsz + (ns,)).copy(),
+                                  spec.reshape(bsz + (ns,)), bsz)
+
+
+def coarse_grain_profile(u, v, grid: StructuredGrid, **kw) -> CoarseGrainBatchResult:
+    """Pipeline.coarse_grain_profile! (Pipeline.jl:991-1007): levels are a batch axis."""
+    return coarse_grain_batch(u, v, grid, **kw)
+
+
+def coarse_grain_slices(us: Sequence, vs: Sequence, grids: Sequence[StructuredGrid], *, scales: Sequence[float],
+                        kernel: AbstractFilterKernel = TopHatKernel(),
+                        mask_strategy: AbstractMaskStrategy = ZeroFill(), L: float = 1.0,
+                        spectrum: AbstractSpectrumPolicy = StrictSpectrum()) -> List[CoarseGrainResult]:
+    """Pipeline.coarse_grain_slices! (Pipeline.jl:866-904): each slice brings its own grid.  Slices whose
+    grids differ only in their masks (levels under bathymetry) run as one batched sweep with a mask
+    per slice; any other group runs per grid."""
+    n = len(us)
+    if len(vs) != n or len(grids) != n:
+        raise DimensionMismatch("us, vs and grids must have equal length")
+    gate_spectrum(kernel, spectrum)
+    scales = np.asarray(scales, dtype=np.float64)
+    results: List[Optional[CoarseGrainResult]] = [None] * n
+    groups: List[List[int]] = []
+    for t in range(n):
+        for g in groups:
+            if grids[g[0]].same_geometry(grids[t]):
+                g.append(t)
+                break
+        else:
+            groups.append([t])
+    k = float(L) / scales
+    for g in groups:
+        base = grids[g[0]].with_mask(None)
+        plans = _plans(base, kernel, scales, mask_strategy, None)
+        masks = np.stack([np.ones(base.shape, np.uint8) if grids[t].mask is None else grids[t].mask.astype(np.uint8)
+                          for t in g])
+        u = np.stack([np.asarray(us[t]) for t in g])
+        v = np.stack([np.asarray(vs[t]) for t in g])
+        Pi, E = _sweep(u, v, base, plans, len(g), masks)
+        for q, t in enumerate(g):
+            results[t] = CoarseGrainResult(scales.copy(), Pi[q], E[q], k, _spectrum(E[q], k, spectrum))
+    return results  # type: ignore[return-value]

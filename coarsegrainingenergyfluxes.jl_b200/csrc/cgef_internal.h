@@ -1,0 +1,218 @@
+// Internal declarations shared by the host plan builder, the kernels and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "cgef_b200.h"
+
+namespace cgef {
+
+// Filtering.jl:1633 and every apply path: denominators at or below this give 0.
+constexpr double kNormEps = 1e-15;
+// Kernels.jl:307: relative weight at which a Gaussian footprint is truncated.
+constexpr double kGaussianTruncationTol = 1e-10;
+
+// Number of source columns whose weights one CTA stages in shared memory at a time.
+constexpr int kChunk = 512;
+// Target rows carried by one thread of the banded gather (register tile height).
+constexpr int kRows = 4;
+// Warps per CTA of the banded gather.
+constexpr int kWarps = 5;
+
+// One (target band j, source row offset dj) of the banded footprint: weights for longitude
+// offsets di in [-a, hi] live at w[woff + |di|] (the sphere's weight is even in di).  a < 0
+// means the row holds no entries.  hi is a or, where the band closes the ring on an even
+// ring, a - 1 (Filtering.jl:711-713).
+struct BandRow {
+  int32_t woff;
+  int32_t a;
+  int32_t hi;
+  int32_t pad;
+};
+
+// A CTA's work item of the banded gather: target columns [x0, x0 + width) and rows
+// [j0, j0 + kRows); split = 1 when the CTA's warps share 32 columns and divide the source
+// columns between them (the heavy polar bands).
+struct WorkItem {
+  int32_t x0;
+  int32_t j0;
+  int32_t split;
+  int32_t cost;
+};
+
+// Per (target row j, source row slot b) of the prefix-sum top-hat sweep (Filtering.jl:974-1097).
+struct PrefixRow {
+  int32_t jj;    // source row, or -1 when skipped
+  int32_t mode;  // 0 skip, 1 whole ring, 2 uniform window +-w, 3 general interval search
+  int32_t w;     // half-window in cells (mode 2)
+  int32_t pad;
+  double hw;     // half-width in axis-1 coordinate units (mode 3)
+  double wy;     // row measure factor
+};
+
+enum Mode { kModeFields = 0, kModePiCart = 1, kModePiSphere = 2 };
+
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace cgef
+
+struct cgef_plan {
+  int device = 0;
+  // grid
+  int geometry = 0, nx = 0, ny = 0, periodic_x = 0, periodic_y = 0;
+  double x0 = 0, dx = 0, y0 = 0, dy = 0, R = 0;
+  std::vector<uint8_t> h_mask;  // empty = all active
+  bool masked = false;
+  double active_area = 0;
+  // filter
+  int kernel = 0, strategy = 0, engine = 0;
+  double alpha = 0, scale = 0, rad = 0;
+  // host tables kept for introspection
+  std::vector<double> h_x, h_y;
+  std::vector<int32_t> h_di, h_dj;
+  std::vector<double> h_w;
+  std::vector<int64_t> h_ptr;
+  int64_t nentries = 0;
+  int dj_lim = 0, di_max = 0;
+  // device geometry tables
+  uint8_t* d_mask = nullptr;
+  double* d_x = nullptr;       // nx coordinates
+  double* d_sinlam = nullptr;  // nx
+  double* d_coslam = nullptr;  // nx
+  double* d_sinphi = nullptr;  // ny
+  double* d_cosphi = nullptr;  // ny
+  double* d_area = nullptr;    // ny: cell measure of row j
+  double* d_xscale = nullptr;  // ny: d/dx metric factor (1/(R cos phi) on the sphere, 0 at the pole guard)
+  double* d_tanfac = nullptr;  // ny: sin(phi)/(R cos phi) curvature factor (0 where |cos phi| <= 1e-12)
+  // banded engine
+  int D = 0;           // row half-width
+  int H = 0;           // column halo of the padded planes
+  int Amax = 0;        // widest column half-width over all rows
+  cgef::BandRow* d_rows = nullptr;  // ny * (2D+1)
+  double* d_w = nullptr;            // weights, half rows
+  double* d_den_zf = nullptr;       // ZeroFill denominator: ny (periodic x) or ny*nx
+  int den_zf_2d = 0;
+  std::vector<cgef::WorkItem> h_items;
+  cgef::WorkItem* d_items = nullptr;
+  // separable engine
+  int di_lim = 0, sep_dj_lim = 0;
+  double* d_gx = nullptr;
+  double* d_gy = nullptr;
+  double* d_px = nullptr;
+  double* d_py = nullptr;
+  // prefix-sum engine
+  int pre_nrep = 1, pre_ne = 0, pre_nb = 0;
+  double x_period = 0, y_period = 0;
+  double* d_xe = nullptr;         // ne extended coordinates
+  double* d_prefix_wx = nullptr;  // ne + 1
+  cgef::PrefixRow* d_prows = nullptr;  // ny * nb
+  // execution
+  cudaStream_t stream = nullptr;
+  cgef::DeviceBuffer ws[8];  // workspace slots, grown on demand
+};
+
+namespace cgef {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+double kernel_weight(int kernel, double alpha, double d, double ell);
+double kernel_radius(int kernel, double alpha, double ell);
+
+// Host plan construction (plan_build.cpp).
+int build_plan_tables(cgef_plan* p);
+
+// Workspace slot of at least `bytes` bytes.
+int ensure_ws(cgef_plan* p, int slot, size_t bytes, void** out);
+
+void count_launch(int64_t n = 1);
+
+// Tracing: events around one launch of `kind` on stream `st` (no-ops unless enabled).
+void prof_begin(int kind, cudaStream_t st);
+void prof_end(int kind, cudaStream_t st);
+
+// ---- launchers (kernels.cu) ----
+struct StageArgs {
+  const void* a;  // field 0 (u) or nullptr
+  const void* b;  // field 1 (v) or nullptr
+  const void* const* fields;  // kModeFields: nf fields (each nbatch*ny*nx)
+  int nf;
+  int dtype;
+  const uint8_t* mask;  // device mask (ny*nx) or nullptr
+  int64_t mask_slice_stride;  // 0 = shared mask
+  int nbatch;
+};
+
+// Writes padded FP64 planes [nbatch][np][ny][pitch] with halo H (wrapped or zero), masked
+// values, planetary components on the sphere for kModePiSphere, and a mask plane when
+// `with_mask_plane`.
+int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* planes, int pitch, int halo, int np,
+                 bool with_mask_plane, cudaStream_t st);
+
+struct GatherOut {
+  double* o[9];  // kModeFields: one plane per field; Pi modes: ubar, vbar, txx, txy, tyy
+  int64_t slice_stride;
+};
+
+int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                  const uint8_t* mask, int64_t mask_slice_stride, const GatherOut& out, cudaStream_t st);
+
+int launch_separable(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                     const uint8_t* mask, int64_t mask_slice_stride, double* rowbuf, const GatherOut& out,
+                     cudaStream_t st);
+
+int launch_prefix(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                  const uint8_t* mask, int64_t mask_slice_stride, double* prefix, const GatherOut& out,
+                  cudaStream_t st);
+
+struct StrainArgs {
+  const double* ubar;
+  const double* vbar;
+  const double* txx;
+  const double* txy;
+  const double* tyy;
+  int64_t in_slice_stride;
+  const uint8_t* mask;
+  int64_t mask_slice_stride;
+  int nbatch;
+  int dtype;
+  // outputs (dtype), each with out_slice_stride between slices; nullptr = skip
+  void* pi;
+  void* ubar_o;
+  void* vbar_o;
+  void* txx_o;
+  void* txy_o;
+  void* tyy_o;
+  void* sxx_o;
+  void* sxy_o;
+  void* syy_o;
+  int64_t out_slice_stride;
+  // energy: per-slice numerator and active area partials, reduced into energy[slice*estride]
+  double* partials;  // nbatch * nblocks * 2, or nullptr
+  double* energy;    // nullptr = skip
+  int64_t energy_stride;
+};
+
+int launch_strain(const cgef_plan* p, const StrainArgs& a, cudaStream_t st);
+
+// Plain derivative of one field (ddx / ddy).
+int launch_derivative(const cgef_plan* p, int axis, int dtype, const void* f, void* out, cudaStream_t st);
+
+// Converts FP64 planes to the caller's dtype: dst[s*dst_stride + k] = src[s*src_stride + k].
+int launch_convert(const double* src, int64_t src_stride, void* dst, int64_t dst_stride, int dtype, int64_t n,
+                   int nbatch, cudaStream_t st);
+
+// Energy of `fields` (ubar, vbar planes) per slice.
+int launch_energy(const cgef_plan* p, const double* ubar, const double* vbar, int64_t slice_stride,
+                  const uint8_t* mask, int64_t mask_slice_stride, int nbatch, double* partials, double* energy,
+                  int64_t energy_stride, cudaStream_t st);
+
+}  // namespace cgef

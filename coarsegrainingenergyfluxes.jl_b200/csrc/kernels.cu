@@ -1,0 +1,1169 @@
+// Device kernels of the coarse-graining path (sm_100a).
+//
+// stage      : raw u, v (or K fields) -> padded FP64 planes with a wrapped/zero halo; masked
+//              values; planetary-Cartesian components on the sphere (Diagnostics.jl:555-573).
+// banded     : the footprint direct sum (Filtering.jl:2550-2598) -- every CTA walks the source
+//              rows of its target rows once, applying per-band weights staged in shared memory
+//              to all fields and their products (formed on the fly) with FP64 FMA; the epilogue
+//              normalises, forms tau = (u_i u_j)bar - ubar_i ubar_j in FP64 and rotates to the
+//              local frame (Diagnostics.jl:596-650).
+// separable  : row pass + column pass of the square-truncated Gaussian (Filtering.jl:1211-1280,
+//              1472-1524).
+// prefix     : exact top-hat by per-row prefix sums and interval sweeps (Filtering.jl:894-1078).
+// strain     : ReduceInRun 3-node derivatives of ubar, vbar, curvature terms, Pi = -S:tau and
+//              the area-weighted energy partial sums (Diagnostics.jl:652-699, 1086-1134).
+//
+// This file is compiled with --fmad=false: every product and sum outside the explicit fma()
+// accumulations is rounded separately, as in the reference's Julia code.
+#include <cstdint>
+
+#include "cgef_internal.h"
+
+namespace cgef {
+
+namespace {
+
+__device__ __forceinline__ int wrap(int a, int n) {
+  int r = a % n;
+  return r < 0 ? r + n : r;
+}
+
+template <typename T>
+__device__ __forceinline__ double ld(const void* p, int64_t k) {
+  return static_cast<double>(static_cast<const T*>(p)[k]);
+}
+
+__device__ __forceinline__ double load_any(const void* p, int dtype, int64_t k) {
+  return dtype == CGEF_F32 ? ld<float>(p, k) : ld<double>(p, k);
+}
+
+__device__ __forceinline__ void store_any(void* p, int dtype, int64_t k, double v) {
+  if (dtype == CGEF_F32)
+    static_cast<float*>(p)[k] = static_cast<float>(v);
+  else
+    static_cast<double*>(p)[k] = v;
+}
+
+// ------------------------------------------------------------------------------------------
+// stage
+// ------------------------------------------------------------------------------------------
+struct StageK {
+  const void* f[4];
+  int nf;
+  int dtype;
+  const uint8_t* mask;
+  int64_t mask_stride;
+  int nx, ny, pitch, halo, np, periodic_x, with_mask;
+  int64_t in_slice_stride;  // nx*ny
+  int64_t plane_stride;     // ny*pitch
+  int64_t slice_stride;     // np*plane_stride
+  const double* sinlam;
+  const double* coslam;
+  const double* sinphi;
+  const double* cosphi;
+  double* planes;
+};
+
+template <int MODE>
+__global__ void stage_kernel(StageK a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const int s = blockIdx.z;
+  if (p >= a.pitch) return;
+  int i = p - a.halo;
+  bool inside = true;
+  if (i < 0 || i >= a.nx) {
+    if (a.periodic_x)
+      i = wrap(i, a.nx);
+    else
+      inside = false;
+  }
+  double vals[4] = {0.0, 0.0, 0.0, 0.0};
+  double mval = 0.0;
+  if (inside) {
+    const int64_t k = s * a.in_slice_stride + static_cast<int64_t>(j) * a.nx + i;
+    const bool act = a.mask == nullptr || a.mask[s * a.mask_stride + static_cast<int64_t>(j) * a.nx + i] != 0;
+    mval = act ? 1.0 : 0.0;
+    if (act) {
+      if (MODE == kModePiSphere) {
+        const double u = load_any(a.f[0], a.dtype, k), v = load_any(a.f[1], a.dtype, k);
+        const double sl = a.sinlam[i], cl = a.coslam[i], sp = a.sinphi[j], cp = a.cosphi[j];
+        vals[0] = -sl * u - sp * cl * v;
+        vals[1] = cl * u - sp * sl * v;
+        vals[2] = cp * v;
+      } else {
+        for (int m = 0; m < a.nf; ++m) vals[m] = load_any(a.f[m], a.dtype, k);
+      }
+    }
+  }
+  double* out = a.planes + s * a.slice_stride + static_cast<int64_t>(j) * a.pitch + p;
+  const int nv = MODE == kModePiSphere ? 3 : a.nf;
+  for (int m = 0; m < nv; ++m) out[m * a.plane_stride] = vals[m];
+  if (a.with_mask) out[nv * a.plane_stride] = mval;
+}
+
+// ------------------------------------------------------------------------------------------
+// banded gather
+// ------------------------------------------------------------------------------------------
+template <int MODE, int NF, bool DEF>
+struct Cfg {
+  static constexpr int NV = MODE == kModePiSphere ? 3 : (MODE == kModePiCart ? 2 : NF);
+  static constexpr int NA0 = MODE == kModePiSphere ? 9 : (MODE == kModePiCart ? 5 : NF);
+  static constexpr int NA = NA0 + (DEF ? 1 : 0);
+  static constexpr int NP = NV + (DEF ? 1 : 0);
+};
+
+struct BandedK {
+  const double* planes;
+  int64_t plane_stride, slice_stride;
+  int pitch, halo;
+  const BandRow* rows;
+  int band_stride;  // 2D+1 on the sphere (one band per row), 0 on the plane
+  const double* w;
+  int D;
+  const WorkItem* items;
+  int nslices;
+  const double* den_zf;
+  int den_zf_2d;
+  const uint8_t* mask;
+  int64_t mask_stride;
+  int nx, ny, periodic_y;
+  const double* sinlam;
+  const double* coslam;
+  const double* sinphi;
+  const double* cosphi;
+  double* out[9];
+  int64_t out_stride;
+};
+
+// Expands the staged values of one source cell into the accumulated quantities: the fields
+// themselves, then (Pi modes) their pairwise products in the reference's order, then the mask.
+template <int MODE, int NF, bool DEF>
+__device__ __forceinline__ void expand(const double (&v)[Cfg<MODE, NF, DEF>::NP], double (&q)[Cfg<MODE, NF, DEF>::NA]) {
+  using C = Cfg<MODE, NF, DEF>;
+  if (MODE == kModePiSphere) {
+    q[0] = v[0];
+    q[1] = v[1];
+    q[2] = v[2];
+    q[3] = v[0] * v[0];
+    q[4] = v[0] * v[1];
+    q[5] = v[0] * v[2];
+    q[6] = v[1] * v[1];
+    q[7] = v[1] * v[2];
+    q[8] = v[2] * v[2];
+  } else if (MODE == kModePiCart) {
+    q[0] = v[0];
+    q[1] = v[1];
+    q[2] = v[0] * v[0];
+    q[3] = v[0] * v[1];
+    q[4] = v[1] * v[1];
+  } else {
+#pragma unroll
+    for (int m = 0; m < NF; ++m) q[m] = v[m];
+  }
+  if (DEF) q[C::NA - 1] = v[C::NP - 1];
+}
+
+// Normalised epilogue shared by the direct-sum engines.  F holds the NA0 filtered quantities
+// (already divided by the denominator); writes the mode's outputs at offset o.
+template <int MODE, int NA0>
+__device__ __forceinline__ void write_outputs(double* const (&out)[9], int64_t o, const double (&F)[NA0], bool zero,
+                                              double sl, double cl, double sp, double cp) {
+  if (MODE == kModeFields) {
+#pragma unroll
+    for (int m = 0; m < NA0; ++m) out[m][o] = zero ? 0.0 : F[m];
+    return;
+  }
+  if (zero) {
+#pragma unroll
+    for (int m = 0; m < 5; ++m) out[m][o] = 0.0;
+    return;
+  }
+  if (MODE == kModePiCart) {
+    // Diagnostics.jl:525-527
+    out[0][o] = F[0];
+    out[1][o] = F[1];
+    out[2][o] = F[2] - F[0] * F[0];
+    out[3][o] = F[3] - F[0] * F[1];
+    out[4][o] = F[4] - F[1] * F[1];
+    return;
+  }
+  // Sphere (Diagnostics.jl:596-650): planetary ubar and tau, rotated to east/north.
+  const double ub0 = F[0], ub1 = F[1], ub2 = F[2];
+  const double e0 = -sl, e1 = cl, e2 = 0.0;
+  const double n0 = -sp * cl, n1 = -sp * sl, n2 = cp;
+  out[0][o] = e0 * ub0 + e1 * ub1 + e2 * ub2;
+  out[1][o] = n0 * ub0 + n1 * ub1 + n2 * ub2;
+  const double t00 = F[3] - ub0 * ub0;
+  const double t01 = F[4] - ub0 * ub1;
+  const double t02 = F[5] - ub0 * ub2;
+  const double t11 = F[6] - ub1 * ub1;
+  const double t12 = F[7] - ub1 * ub2;
+  const double t22 = F[8] - ub2 * ub2;
+  const double te0 = t00 * e0 + t01 * e1 + t02 * e2;
+  const double te1 = t01 * e0 + t11 * e1 + t12 * e2;
+  const double te2 = t02 * e0 + t12 * e1 + t22 * e2;
+  const double tn0 = t00 * n0 + t01 * n1 + t02 * n2;
+  const double tn1 = t01 * n0 + t11 * n1 + t12 * n2;
+  const double tn2 = t02 * n0 + t12 * n1 + t22 * n2;
+  out[2][o] = e0 * te0 + e1 * te1 + e2 * te2;
+  out[3][o] = e0 * tn0 + e1 * tn1 + e2 * tn2;
+  out[4][o] = n0 * tn0 + n1 * tn1 + n2 * tn2;
+}
+
+template <int MODE, int NF, bool DEF>
+__global__ void __launch_bounds__(32 * kWarps, 2) banded_kernel(BandedK a) {
+  using C = Cfg<MODE, NF, DEF>;
+  extern __shared__ double smem[];  // [kRows][kChunk] weights; reused by the split reduction
+  __shared__ int s_a[kRows], s_hi[kRows], s_off[kRows];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int nw = blockDim.x >> 5;
+  const int item_id = blockIdx.x / a.nslices;
+  const int slice = blockIdx.x - item_id * a.nslices;
+  const WorkItem it = a.items[item_id];
+  const bool split = it.split != 0;
+  const int col = it.x0 + (split ? lane : tid);
+  const int j0 = it.j0;
+
+  double acc[kRows][C::NA];
+#pragma unroll
+  for (int t = 0; t < kRows; ++t)
+#pragma unroll
+    for (int m = 0; m < C::NA; ++m) acc[t][m] = 0.0;
+
+  const double* base = a.planes + slice * a.slice_stride + a.halo + col;
+
+  // Inactive targets output 0 (Filtering.jl:2561), so a warp whose targets are all masked skips
+  // the sums, and a CTA with none active only writes its zeros.
+  bool any_act = false;
+  if (col < a.nx) {
+#pragma unroll
+    for (int t = 0; t < kRows; ++t) {
+      const int j = j0 + t;
+      if (j < a.ny)
+        any_act |= a.mask == nullptr || a.mask[slice * a.mask_stride + static_cast<int64_t>(j) * a.nx + col] != 0;
+    }
+  }
+  const bool warp_act = __any_sync(0xffffffffu, any_act);
+  const bool cta_act = __syncthreads_or(any_act) != 0;
+
+  for (int jr = j0 - a.D; cta_act && jr <= j0 + kRows - 1 + a.D; ++jr) {
+    int jj = jr;
+    if (jr < 0 || jr >= a.ny) {
+      if (!a.periodic_y) continue;
+      jj = wrap(jr, a.ny);
+    }
+    __syncthreads();  // previous row's readers of s_a / smem are done
+    if (tid < kRows) {
+      const int j = j0 + tid;
+      const int dj = jr - j;
+      BandRow r{0, -1, -1, 0};
+      if (j < a.ny && dj >= -a.D && dj <= a.D) r = a.rows[static_cast<int64_t>(j) * a.band_stride + dj + a.D];
+      s_a[tid] = r.a;
+      s_hi[tid] = r.hi;
+      s_off[tid] = r.woff;
+    }
+    __syncthreads();
+    int A = -1, HI = -1;
+#pragma unroll
+    for (int t = 0; t < kRows; ++t) {
+      A = max(A, s_a[t]);
+      HI = max(HI, s_hi[t]);
+    }
+    if (A < 0) continue;
+    const double* src = base + static_cast<int64_t>(jj) * a.pitch;
+    for (int c0 = -A; c0 <= HI; c0 += kChunk) {
+      const int cn = min(kChunk, HI - c0 + 1);
+      if (c0 != -A) __syncthreads();
+      for (int idx = tid; idx < kRows * cn; idx += blockDim.x) {
+        const int t = idx / cn;
+        const int k = idx - t * cn;
+        const int di = c0 + k;
+        const int at = s_a[t];
+        smem[t * kChunk + k] = (at >= 0 && di >= -at && di <= s_hi[t]) ? a.w[s_off[t] + abs(di)] : 0.0;
+      }
+      __syncthreads();
+      int kb = 0, ke = warp_act ? cn : 0;
+      if (split && warp_act) {
+        kb = (warp * cn) / nw;
+        ke = ((warp + 1) * cn) / nw;
+      }
+      const double* s = src + c0;
+#pragma unroll 2
+      for (int k = kb; k < ke; ++k) {
+        double v[C::NP];
+#pragma unroll
+        for (int pl = 0; pl < C::NP; ++pl) v[pl] = __ldg(s + pl * a.plane_stride + k);
+        double q[C::NA];
+        expand<MODE, NF, DEF>(v, q);
+#pragma unroll
+        for (int t = 0; t < kRows; ++t) {
+          const double wt = smem[t * kChunk + k];
+#pragma unroll
+          for (int m = 0; m < C::NA; ++m) acc[t][m] = fma(wt, q[m], acc[t][m]);
+        }
+      }
+    }
+  }
+
+  if (split && cta_act) {
+    // Deterministic cross-warp sum: warp 0 adds the partials of warps 0..nw-1 in order.
+#pragma unroll
+    for (int t = 0; t < kRows; ++t) {
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < C::NA; ++m) smem[(warp * C::NA + m) * 32 + lane] = acc[t][m];
+      __syncthreads();
+      if (warp == 0) {
+#pragma unroll
+        for (int m = 0; m < C::NA; ++m) {
+          double s = smem[m * 32 + lane];
+          for (int w2 = 1; w2 < nw; ++w2) s += smem[(w2 * C::NA + m) * 32 + lane];
+          acc[t][m] = s;
+        }
+      }
+    }
+  }
+  if (split && warp != 0) return;
+
+  if (col >= a.nx) return;
+  const double sl = a.sinlam ? a.sinlam[col] : 0.0;
+  const double cl = a.coslam ? a.coslam[col] : 0.0;
+#pragma unroll
+  for (int t = 0; t < kRows; ++t) {
+    const int j = j0 + t;
+    if (j >= a.ny) break;
+    const int64_t pix = static_cast<int64_t>(j) * a.nx + col;
+    const bool act = a.mask == nullptr || a.mask[slice * a.mask_stride + pix] != 0;
+    double den;
+    if (DEF)
+      den = acc[t][C::NA - 1];
+    else
+      den = a.den_zf_2d ? a.den_zf[pix] : a.den_zf[j];
+    const bool zero = !act || !(den > kNormEps);
+    double F[C::NA0];
+#pragma unroll
+    for (int m = 0; m < C::NA0; ++m) F[m] = zero ? 0.0 : acc[t][m] / den;
+    const double sp = a.sinphi ? a.sinphi[j] : 0.0;
+    const double cp = a.cosphi ? a.cosphi[j] : 0.0;
+    write_outputs<MODE, C::NA0>(a.out, slice * a.out_stride + pix, F, zero, sl, cl, sp, cp);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// separable (Cartesian Gaussian)
+// ------------------------------------------------------------------------------------------
+struct SepK {
+  const double* planes;
+  int64_t plane_stride, slice_stride;
+  int pitch, halo;
+  const double* gx;
+  const double* gy;
+  const double* px;
+  const double* py;
+  int di_lim, dj_lim, periodic_y;
+  int nx, ny;
+  double* rowbuf;  // [slice][NA][ny][nx]
+  int64_t rb_plane, rb_slice;
+  const uint8_t* mask;
+  int64_t mask_stride;
+  double* out[9];
+  int64_t out_stride;
+};
+
+template <int MODE, int NF, bool DEF>
+__global__ void sep_row_kernel(SepK a) {
+  using C = Cfg<MODE, NF, DEF>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const int s = blockIdx.z;
+  if (i >= a.nx) return;
+  double acc[C::NA];
+#pragma unroll
+  for (int m = 0; m < C::NA; ++m) acc[m] = 0.0;
+  const double* src = a.planes + s * a.slice_stride + static_cast<int64_t>(j) * a.pitch + a.halo + i;
+  for (int k = -a.di_lim; k <= a.di_lim; ++k) {
+    const double w = a.gx[k + a.di_lim];
+    double v[C::NP];
+#pragma unroll
+    for (int pl = 0; pl < C::NP; ++pl) v[pl] = src[pl * a.plane_stride + k];
+    double q[C::NA];
+    expand<MODE, NF, DEF>(v, q);
+#pragma unroll
+    for (int m = 0; m < C::NA; ++m) acc[m] = fma(w, q[m], acc[m]);
+  }
+  double* o = a.rowbuf + s * a.rb_slice + static_cast<int64_t>(j) * a.nx + i;
+#pragma unroll
+  for (int m = 0; m < C::NA; ++m) o[m * a.rb_plane] = acc[m];
+}
+
+template <int MODE, int NF, bool DEF>
+__global__ void sep_col_kernel(SepK a) {
+  using C = Cfg<MODE, NF, DEF>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const int s = blockIdx.z;
+  if (i >= a.nx) return;
+  double acc[C::NA];
+#pragma unroll
+  for (int m = 0; m < C::NA; ++m) acc[m] = 0.0;
+  const double* rb = a.rowbuf + s * a.rb_slice + i;
+  for (int k = -a.dj_lim; k <= a.dj_lim; ++k) {
+    int jj = j + k;
+    if (jj < 0 || jj >= a.ny) {
+      if (!a.periodic_y) continue;
+      jj = wrap(jj, a.ny);
+    }
+    const double w = a.gy[k + a.dj_lim];
+#pragma unroll
+    for (int m = 0; m < C::NA; ++m) acc[m] = fma(w, rb[m * a.rb_plane + static_cast<int64_t>(jj) * a.nx], acc[m]);
+  }
+  const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+  const bool act = a.mask == nullptr || a.mask[s * a.mask_stride + pix] != 0;
+  double F[C::NA0];
+  bool zero = !act;
+  if (DEF) {
+    // invrenorm = 1/conv(mask), 0 where the local mass vanishes (Filtering.jl:1436-1445)
+    const double den = acc[C::NA - 1];
+    const double inv = den > kNormEps ? 1.0 / den : 0.0;
+#pragma unroll
+    for (int m = 0; m < C::NA0; ++m) F[m] = acc[m] * inv;
+  } else {
+    const double den = a.px[i] * a.py[j];
+#pragma unroll
+    for (int m = 0; m < C::NA0; ++m) F[m] = den > kNormEps ? acc[m] / den : 0.0;
+  }
+  if (zero) {
+#pragma unroll
+    for (int m = 0; m < C::NA0; ++m) F[m] = 0.0;
+  }
+  if (MODE == kModePiCart && !zero) {
+    // masked cells output 0 before tau is formed (Filtering.jl:1521-1523), so tau there is 0
+  }
+  write_outputs<MODE, C::NA0>(a.out, s * a.out_stride + pix, F, MODE != kModeFields && zero, 0.0, 0.0, 0.0, 0.0);
+}
+
+// ------------------------------------------------------------------------------------------
+// prefix-sum top-hat
+// ------------------------------------------------------------------------------------------
+struct PreK {
+  const double* planes;
+  int64_t plane_stride, slice_stride;
+  int pitch, halo;
+  int nx, ny, ne, nb, nslices;
+  double wx;
+  double* P;  // [slice][NA][ny][ne+1]
+  int64_t P_plane, P_slice;
+  const double* xe;
+  const double* prefix_wx;
+  const PrefixRow* rows;
+  const double* x;
+  double x0, dx;
+  int nrep;
+  const uint8_t* mask;
+  int64_t mask_stride;
+  double* out[9];
+  int64_t out_stride;
+  const double* sinlam;
+  const double* coslam;
+  const double* sinphi;
+  const double* cosphi;
+};
+
+// One thread per (slice, quantity, row): the reference's sequential running sum, in its order
+// (prefixsum_fill_numerator_row!, Filtering.jl:894-907).
+template <int MODE, int NF, bool DEF>
+__global__ void prefix_scan_kernel(PreK a) {
+  using C = Cfg<MODE, NF, DEF>;
+  const int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t total = static_cast<int64_t>(a.nslices) * C::NA * a.ny;
+  if (gid >= total) return;
+  const int j = static_cast<int>(gid % a.ny);
+  const int m = static_cast<int>((gid / a.ny) % C::NA);
+  const int s = static_cast<int>(gid / (static_cast<int64_t>(a.ny) * C::NA));
+  const double* row = a.planes + s * a.slice_stride + static_cast<int64_t>(j) * a.pitch + a.halo;
+  double* P = a.P + s * a.P_slice + m * a.P_plane + static_cast<int64_t>(j) * (a.ne + 1);
+  double acc = 0.0;
+  P[0] = 0.0;
+  for (int k = 0; k < a.ne; ++k) {
+    const int i = k % a.nx;
+    double v[C::NP];
+#pragma unroll
+    for (int pl = 0; pl < C::NP; ++pl) v[pl] = row[pl * a.plane_stride + i];
+    double q[C::NA];
+    expand<MODE, NF, DEF>(v, q);
+    double qm = 0.0;
+#pragma unroll
+    for (int mm = 0; mm < C::NA; ++mm)
+      if (mm == m) qm = q[mm];
+    acc = acc + qm * a.wx;
+    P[k + 1] = acc;
+  }
+}
+
+__device__ __forceinline__ int lower_index(const double* xe, int ne, double xlo, int est) {
+  int k = est < 0 ? 0 : (est > ne ? ne : est);
+  while (k > 0 && xe[k - 1] >= xlo) --k;
+  while (k < ne && xe[k] < xlo) ++k;
+  return k;  // first k with xe[k] >= xlo (ne if none)
+}
+
+__device__ __forceinline__ int upper_index(const double* xe, int ne, double xhi, int est) {
+  int h = est < -1 ? -1 : (est > ne - 1 ? ne - 1 : est);
+  while (h + 1 < ne && xe[h + 1] <= xhi) ++h;
+  while (h >= 0 && xe[h] > xhi) --h;
+  return h;  // last h with xe[h] <= xhi (-1 if none)
+}
+
+template <int MODE, int NF, bool DEF>
+__global__ void prefix_sweep_kernel(PreK a) {
+  using C = Cfg<MODE, NF, DEF>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const int s = blockIdx.z;
+  if (i >= a.nx) return;
+  double num[C::NA0];
+#pragma unroll
+  for (int m = 0; m < C::NA0; ++m) num[m] = 0.0;
+  double den = 0.0;
+  const double xc = a.x[i];
+  const int off = a.nrep == 3 ? a.nx : 0;
+  const int64_t pitchP = a.ne + 1;
+  const double* Ps = a.P + s * a.P_slice;
+  for (int b = 0; b < a.nb; ++b) {
+    const PrefixRow pr = a.rows[static_cast<int64_t>(j) * a.nb + b];
+    if (pr.mode == 0) continue;
+    int lo, hi;
+    if (pr.mode == 1) {
+      lo = 0;
+      hi = a.nx - 1;
+    } else if (pr.mode == 2) {
+      lo = i - pr.w < 0 ? 0 : i - pr.w;
+      hi = i + pr.w > a.nx - 1 ? a.nx - 1 : i + pr.w;
+    } else {
+      const double xlo = xc - pr.hw, xhi = xc + pr.hw;
+      const int est_lo = static_cast<int>(floor((xlo - a.x0) / a.dx)) + off;
+      const int est_hi = static_cast<int>(floor((xhi - a.x0) / a.dx)) + off;
+      lo = lower_index(a.xe, a.ne, xlo, est_lo);
+      hi = upper_index(a.xe, a.ne, xhi, est_hi);
+      if (hi < lo) continue;
+    }
+    const int64_t rbase = static_cast<int64_t>(pr.jj) * pitchP;
+#pragma unroll
+    for (int m = 0; m < C::NA0; ++m) {
+      const double* Pr = Ps + m * a.P_plane + rbase;
+      num[m] = num[m] + pr.wy * (Pr[hi + 1] - Pr[lo]);
+    }
+    double dd;
+    if (DEF) {
+      const double* Pd = Ps + (C::NA - 1) * a.P_plane + rbase;
+      dd = Pd[hi + 1] - Pd[lo];
+    } else {
+      dd = a.prefix_wx[hi + 1] - a.prefix_wx[lo];
+    }
+    den = den + pr.wy * dd;
+  }
+  const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+  const bool act = a.mask == nullptr || a.mask[s * a.mask_stride + pix] != 0;
+  const bool zero = !act || !(den > kNormEps);
+  double F[C::NA0];
+#pragma unroll
+  for (int m = 0; m < C::NA0; ++m) F[m] = zero ? 0.0 : num[m] / den;
+  const double sl = a.sinlam ? a.sinlam[i] : 0.0, cl = a.coslam ? a.coslam[i] : 0.0;
+  const double sp = a.sinphi ? a.sinphi[j] : 0.0, cp = a.cosphi ? a.cosphi[j] : 0.0;
+  write_outputs<MODE, C::NA0>(a.out, s * a.out_stride + pix, F, zero, sl, cl, sp, cp);
+}
+
+// ------------------------------------------------------------------------------------------
+// derivatives, strain, Pi, energy
+// ------------------------------------------------------------------------------------------
+// ReduceInRun 3-node first derivative along one axis (Derivatives.jl:26-31): centred with both
+// neighbours active; 3-node one-sided when only one side has two active cells (the bounded end
+// too); 2-node in a run of two; 0 for an isolated cell.
+struct Line {
+  const double* f;
+  const uint8_t* m;  // activity, same indexing as f; nullptr = all active
+  int64_t stride;    // element stride along the axis (f and m)
+  int n;
+  int periodic;
+  double h;
+};
+
+__device__ __forceinline__ int nb_index(int p, int off, int n, int periodic) {
+  int q = p + off;
+  if (q < 0 || q >= n) {
+    if (!periodic || n < 2) return -1;
+    q = wrap(q, n);
+  }
+  return q;
+}
+
+__device__ __forceinline__ bool act_at(const Line& L, int q) { return q >= 0 && (L.m == nullptr || L.m[q * L.stride] != 0); }
+
+__device__ double stencil(const Line& L, int p) {
+  const int m1 = nb_index(p, -1, L.n, L.periodic), p1 = nb_index(p, 1, L.n, L.periodic);
+  const bool am1 = act_at(L, m1), ap1 = act_at(L, p1);
+  if (am1 && ap1) return (L.f[p1 * L.stride] - L.f[m1 * L.stride]) / (2.0 * L.h);
+  if (ap1) {
+    const int p2 = nb_index(p, 2, L.n, L.periodic);
+    if (act_at(L, p2) && p2 != p)
+      return (-3.0 * L.f[p * L.stride] + 4.0 * L.f[p1 * L.stride] - L.f[p2 * L.stride]) / (2.0 * L.h);
+    return (L.f[p1 * L.stride] - L.f[p * L.stride]) / L.h;
+  }
+  if (am1) {
+    const int m2 = nb_index(p, -2, L.n, L.periodic);
+    if (act_at(L, m2) && m2 != p)
+      return (3.0 * L.f[p * L.stride] - 4.0 * L.f[m1 * L.stride] + L.f[m2 * L.stride]) / (2.0 * L.h);
+    return (L.f[p * L.stride] - L.f[m1 * L.stride]) / L.h;
+  }
+  return 0.0;
+}
+
+struct StrainK {
+  const double* ub;
+  const double* vb;
+  const double* txx;
+  const double* txy;
+  const double* tyy;
+  int64_t in_stride;
+  const uint8_t* mask;
+  int64_t mask_stride;
+  int nx, ny, periodic_x, periodic_y, sphere, dtype;
+  double dx, dy, yscale;
+  const double* xscale;
+  const double* tanfac;
+  const double* area;
+  void* pi;
+  void* ub_o;
+  void* vb_o;
+  void* txx_o;
+  void* txy_o;
+  void* tyy_o;
+  void* sxx_o;
+  void* sxy_o;
+  void* syy_o;
+  int64_t out_stride;
+  double* partials;  // [slice][block][2]
+};
+
+constexpr int kStrainBX = 32, kStrainBY = 8;
+
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
+  // deterministic: warp shuffles in a fixed tree, then warp results in order
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, off);
+    b += __shfl_down_sync(0xffffffffu, b, off);
+  }
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = (blockDim.x * blockDim.y) >> 5;
+  if (lane == 0) {
+    sh[2 * warp] = a;
+    sh[2 * warp + 1] = b;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double sa = 0.0, sb = 0.0;
+    for (int w = 0; w < nw; ++w) {
+      sa += sh[2 * w];
+      sb += sh[2 * w + 1];
+    }
+    a = sa;
+    b = sb;
+  }
+}
+
+__global__ void strain_kernel(StrainK a) {
+  __shared__ double sh[2 * (kStrainBX * kStrainBY / 32)];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int s = blockIdx.z;
+  double e_num = 0.0, e_area = 0.0;
+  if (i < a.nx && j < a.ny) {
+    const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+    const int64_t o = s * a.out_stride + pix;
+    const uint8_t* mk = a.mask ? a.mask + s * a.mask_stride : nullptr;
+    const bool act = mk == nullptr || mk[pix] != 0;
+    const double* ub = a.ub + s * a.in_stride;
+    const double* vb = a.vb + s * a.in_stride;
+    double sxx = 0.0, sxy = 0.0, syy = 0.0, pi = 0.0;
+    const double u0 = ub[pix], v0 = vb[pix];
+    const double txx = a.txx[s * a.in_stride + pix], txy = a.txy[s * a.in_stride + pix],
+                 tyy = a.tyy[s * a.in_stride + pix];
+    if (act) {
+      Line Lx{ub + static_cast<int64_t>(j) * a.nx, mk ? mk + static_cast<int64_t>(j) * a.nx : nullptr, 1, a.nx,
+              a.periodic_x, a.dx};
+      Line Ly{ub + i, mk ? mk + i : nullptr, a.nx, a.ny, a.periodic_y, a.dy};
+      const double xs = a.xscale[j];
+      const double dudx = a.nx < 2 ? 0.0 : stencil(Lx, i) * xs;
+      const double dudy = a.ny < 2 ? 0.0 : stencil(Ly, j) * a.yscale;
+      Lx.f = vb + static_cast<int64_t>(j) * a.nx;
+      Ly.f = vb + i;
+      const double dvdx = a.nx < 2 ? 0.0 : stencil(Lx, i) * xs;
+      const double dvdy = a.ny < 2 ? 0.0 : stencil(Ly, j) * a.yscale;
+      sxx = dudx;
+      syy = dvdy;
+      if (a.sphere) {
+        const double tf = a.tanfac[j];
+        sxx -= v0 * tf;                          // S_ee = du/dx - v tan(phi)/R
+        sxy = 0.5 * (dudy + dvdx + u0 * tf);     // S_en
+      } else {
+        sxy = 0.5 * (dudy + dvdx);
+      }
+      pi = -(sxx * txx + 2.0 * sxy * txy + syy * tyy);
+      const double ar = a.area[j];
+      e_num = (u0 * u0 + v0 * v0) * ar;
+      e_area = ar;
+    }
+    if (a.pi) store_any(a.pi, a.dtype, o, pi);
+    if (a.ub_o) store_any(a.ub_o, a.dtype, o, u0);
+    if (a.vb_o) store_any(a.vb_o, a.dtype, o, v0);
+    if (a.txx_o) store_any(a.txx_o, a.dtype, o, txx);
+    if (a.txy_o) store_any(a.txy_o, a.dtype, o, txy);
+    if (a.tyy_o) store_any(a.tyy_o, a.dtype, o, tyy);
+    if (a.sxx_o) store_any(a.sxx_o, a.dtype, o, sxx);
+    if (a.sxy_o) store_any(a.sxy_o, a.dtype, o, sxy);
+    if (a.syy_o) store_any(a.syy_o, a.dtype, o, syy);
+  }
+  if (a.partials) {
+    block_sum2(e_num, e_area, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      const int64_t nblk = static_cast<int64_t>(gridDim.x) * gridDim.y;
+      const int64_t b = static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x;
+      a.partials[(s * nblk + b) * 2] = e_num;
+      a.partials[(s * nblk + b) * 2 + 1] = e_area;
+    }
+  }
+}
+
+struct EnergyK {
+  const double* ub;
+  const double* vb;
+  int64_t in_stride;
+  const uint8_t* mask;
+  int64_t mask_stride;
+  int nx, ny;
+  const double* area;
+  double* partials;
+};
+
+__global__ void energy_partial_kernel(EnergyK a) {
+  __shared__ double sh[2 * (kStrainBX * kStrainBY / 32)];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int s = blockIdx.z;
+  double e_num = 0.0, e_area = 0.0;
+  if (i < a.nx && j < a.ny) {
+    const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+    const bool act = a.mask == nullptr || a.mask[s * a.mask_stride + pix] != 0;
+    if (act) {
+      const double u0 = a.ub[s * a.in_stride + pix], v0 = a.vb[s * a.in_stride + pix];
+      e_num = (u0 * u0 + v0 * v0) * a.area[j];
+      e_area = a.area[j];
+    }
+  }
+  block_sum2(e_num, e_area, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const int64_t nblk = static_cast<int64_t>(gridDim.x) * gridDim.y;
+    const int64_t b = static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x;
+    a.partials[(s * nblk + b) * 2] = e_num;
+    a.partials[(s * nblk + b) * 2 + 1] = e_area;
+  }
+}
+
+// One block per slice: sums the block partials in a fixed order; E = 1/2 sum / area.
+__global__ void energy_finish_kernel(const double* partials, int64_t nblk, double* energy, int64_t estride) {
+  __shared__ double sa[256], sb[256];
+  const int s = blockIdx.x;
+  double a = 0.0, b = 0.0;
+  for (int64_t k = threadIdx.x; k < nblk; k += blockDim.x) {
+    a += partials[(s * nblk + k) * 2];
+    b += partials[(s * nblk + k) * 2 + 1];
+  }
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (static_cast<int>(threadIdx.x) < w) {
+      sa[threadIdx.x] += sa[threadIdx.x + w];
+      sb[threadIdx.x] += sb[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) energy[s * estride] = sb[0] > 0.0 ? 0.5 * sa[0] / sb[0] : 0.0;
+}
+
+struct DerivK {
+  const void* f;
+  void* out;
+  int dtype;
+  const uint8_t* mask;
+  int nx, ny, periodic_x, periodic_y, axis;
+  double dx, dy, yscale;
+  const double* xscale;
+  double* scratch;  // FP64 copy of f
+};
+
+__global__ void to_f64_kernel(const void* f, int dtype, double* out, int64_t n) {
+  const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = load_any(f, dtype, k);
+}
+
+__global__ void derivative_kernel(DerivK a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= a.nx || j >= a.ny) return;
+  const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+  const bool act = a.mask == nullptr || a.mask[pix] != 0;
+  double d = 0.0;
+  if (act) {
+    if (a.axis == 0) {
+      Line L{a.scratch + static_cast<int64_t>(j) * a.nx, a.mask ? a.mask + static_cast<int64_t>(j) * a.nx : nullptr, 1,
+             a.nx, a.periodic_x, a.dx};
+      d = a.nx < 2 ? 0.0 : stencil(L, i) * a.xscale[j];
+    } else {
+      Line L{a.scratch + i, a.mask ? a.mask + i : nullptr, a.nx, a.ny, a.periodic_y, a.dy};
+      d = a.ny < 2 ? 0.0 : stencil(L, j) * a.yscale;
+    }
+  }
+  store_any(a.out, a.dtype, pix, d);
+}
+
+__global__ void convert_kernel(const double* src, int64_t src_stride, void* dst, int64_t dst_stride, int dtype,
+                               int64_t n) {
+  const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (k < n) store_any(dst, dtype, s * dst_stride + k, src[s * src_stride + k]);
+}
+
+inline int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  count_launch();
+  return CGEF_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------------------------
+int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* planes, int pitch, int halo, int np,
+                 bool with_mask_plane, cudaStream_t st) {
+  StageK a{};
+  a.f[0] = s.a;
+  a.f[1] = s.b;
+  if (mode == kModeFields) {
+    if (s.nf > 4) return fail(CGEF_EINVAL, "stage: at most 4 fields per pass");
+    for (int m = 0; m < s.nf; ++m) a.f[m] = s.fields[m];
+  }
+  a.nf = mode == kModePiCart ? 2 : (mode == kModePiSphere ? 3 : s.nf);
+  a.dtype = s.dtype;
+  a.mask = s.mask;
+  a.mask_stride = s.mask_slice_stride;
+  a.nx = p->nx;
+  a.ny = p->ny;
+  a.pitch = pitch;
+  a.halo = halo;
+  a.np = np;
+  a.periodic_x = p->periodic_x;
+  a.with_mask = with_mask_plane ? 1 : 0;
+  a.in_slice_stride = static_cast<int64_t>(p->nx) * p->ny;
+  a.plane_stride = static_cast<int64_t>(p->ny) * pitch;
+  a.slice_stride = np * a.plane_stride;
+  a.sinlam = p->d_sinlam;
+  a.coslam = p->d_coslam;
+  a.sinphi = p->d_sinphi;
+  a.cosphi = p->d_cosphi;
+  a.planes = planes;
+  dim3 block(256), grid((pitch + 255) / 256, p->ny, s.nbatch);
+  prof_begin(CGEF_KERNEL_STAGE, st);
+  if (mode == kModePiSphere)
+    stage_kernel<kModePiSphere><<<grid, block, 0, st>>>(a);
+  else
+    stage_kernel<kModeFields><<<grid, block, 0, st>>>(a);
+  prof_end(CGEF_KERNEL_STAGE, st);
+  return check_launch("stage_kernel");
+}
+
+namespace {
+
+template <int MODE, int NF, bool DEF>
+int run_banded(const cgef_plan* p, const BandedK& a, int nitems, int nbatch, cudaStream_t st) {
+  using C = Cfg<MODE, NF, DEF>;
+  const size_t smem_w = sizeof(double) * kRows * kChunk;
+  const size_t smem_r = sizeof(double) * kWarps * C::NA * 32;
+  const size_t smem = smem_w > smem_r ? smem_w : smem_r;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(banded_kernel<MODE, NF, DEF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    attr_set = true;
+  }
+  (void)p;
+  dim3 grid(static_cast<unsigned>(nitems) * nbatch), block(32 * kWarps);
+  prof_begin(CGEF_KERNEL_BANDED, st);
+  banded_kernel<MODE, NF, DEF><<<grid, block, smem, st>>>(a);
+  prof_end(CGEF_KERNEL_BANDED, st);
+  return check_launch("banded_kernel");
+}
+
+template <int MODE, int NF>
+int dispatch_banded(const cgef_plan* p, bool def, const BandedK& a, int nitems, int nbatch, cudaStream_t st) {
+  return def ? run_banded<MODE, NF, true>(p, a, nitems, nbatch, st) : run_banded<MODE, NF, false>(p, a, nitems, nbatch, st);
+}
+
+}  // namespace
+
+int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                  const uint8_t* mask, int64_t mask_slice_stride, const GatherOut& out, cudaStream_t st) {
+  const bool def = p->strategy == CGEF_DEFORMABLE;
+  BandedK a{};
+  a.planes = planes;
+  a.plane_stride = static_cast<int64_t>(p->ny) * pitch;
+  a.slice_stride = np * a.plane_stride;
+  a.pitch = pitch;
+  a.halo = p->H;
+  a.rows = p->d_rows;
+  a.band_stride = p->geometry == CGEF_SPHERICAL ? 2 * p->D + 1 : 0;
+  a.w = p->d_w;
+  a.D = p->D;
+  a.items = p->d_items;
+  a.nslices = nbatch;
+  a.den_zf = p->d_den_zf;
+  a.den_zf_2d = p->den_zf_2d;
+  a.mask = mask;
+  a.mask_stride = mask_slice_stride;
+  a.nx = p->nx;
+  a.ny = p->ny;
+  a.periodic_y = p->periodic_y;
+  const bool sph = mode == kModePiSphere;
+  a.sinlam = sph ? p->d_sinlam : nullptr;
+  a.coslam = sph ? p->d_coslam : nullptr;
+  a.sinphi = sph ? p->d_sinphi : nullptr;
+  a.cosphi = sph ? p->d_cosphi : nullptr;
+  for (int m = 0; m < 9; ++m) a.out[m] = out.o[m];
+  a.out_stride = out.slice_stride;
+  const int nitems = static_cast<int>(p->h_items.size());
+  if (mode == kModePiSphere) return dispatch_banded<kModePiSphere, 1>(p, def, a, nitems, nbatch, st);
+  if (mode == kModePiCart) return dispatch_banded<kModePiCart, 1>(p, def, a, nitems, nbatch, st);
+  switch (nf) {
+    case 1: return dispatch_banded<kModeFields, 1>(p, def, a, nitems, nbatch, st);
+    case 2: return dispatch_banded<kModeFields, 2>(p, def, a, nitems, nbatch, st);
+    case 3: return dispatch_banded<kModeFields, 3>(p, def, a, nitems, nbatch, st);
+    case 4: return dispatch_banded<kModeFields, 4>(p, def, a, nitems, nbatch, st);
+    default: return fail(CGEF_EINVAL, "banded: 1..4 fields per pass");
+  }
+}
+
+namespace {
+
+template <int MODE, int NF, bool DEF>
+int run_sep(const SepK& a, int nbatch, int nx, int ny, cudaStream_t st) {
+  dim3 block(128), grid((nx + 127) / 128, ny, nbatch);
+  prof_begin(CGEF_KERNEL_SEPARABLE, st);
+  sep_row_kernel<MODE, NF, DEF><<<grid, block, 0, st>>>(a);
+  int rc = check_launch("sep_row_kernel");
+  if (rc) return rc;
+  sep_col_kernel<MODE, NF, DEF><<<grid, block, 0, st>>>(a);
+  prof_end(CGEF_KERNEL_SEPARABLE, st);
+  return check_launch("sep_col_kernel");
+}
+
+template <int MODE, int NF>
+int dispatch_sep(bool def, const SepK& a, int nbatch, int nx, int ny, cudaStream_t st) {
+  return def ? run_sep<MODE, NF, true>(a, nbatch, nx, ny, st) : run_sep<MODE, NF, false>(a, nbatch, nx, ny, st);
+}
+
+}  // namespace
+
+int launch_separable(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                     const uint8_t* mask, int64_t mask_slice_stride, double* rowbuf, const GatherOut& out,
+                     cudaStream_t st) {
+  const bool def = p->strategy == CGEF_DEFORMABLE && (p->masked || mask_slice_stride != 0);
+  SepK a{};
+  a.planes = planes;
+  a.plane_stride = static_cast<int64_t>(p->ny) * pitch;
+  a.slice_stride = np * a.plane_stride;
+  a.pitch = pitch;
+  a.halo = p->H;
+  a.gx = p->d_gx;
+  a.gy = p->d_gy;
+  a.px = p->d_px;
+  a.py = p->d_py;
+  a.di_lim = p->di_lim;
+  a.dj_lim = p->sep_dj_lim;
+  a.periodic_y = p->periodic_y;
+  a.nx = p->nx;
+  a.ny = p->ny;
+  a.rowbuf = rowbuf;
+  a.rb_plane = static_cast<int64_t>(p->nx) * p->ny;
+  const int na = (mode == kModePiCart ? 5 : nf) + (def ? 1 : 0);
+  a.rb_slice = na * a.rb_plane;
+  a.mask = mask;
+  a.mask_stride = mask_slice_stride;
+  for (int m = 0; m < 9; ++m) a.out[m] = out.o[m];
+  a.out_stride = out.slice_stride;
+  if (mode == kModePiCart) return dispatch_sep<kModePiCart, 1>(def, a, nbatch, p->nx, p->ny, st);
+  if (mode == kModePiSphere) return fail(CGEF_EUNSUPPORTED, "separable engine is Cartesian only (Filtering.jl:1149-1151)");
+  switch (nf) {
+    case 1: return dispatch_sep<kModeFields, 1>(def, a, nbatch, p->nx, p->ny, st);
+    case 2: return dispatch_sep<kModeFields, 2>(def, a, nbatch, p->nx, p->ny, st);
+    case 3: return dispatch_sep<kModeFields, 3>(def, a, nbatch, p->nx, p->ny, st);
+    case 4: return dispatch_sep<kModeFields, 4>(def, a, nbatch, p->nx, p->ny, st);
+    default: return fail(CGEF_EINVAL, "separable: 1..4 fields per pass");
+  }
+}
+
+namespace {
+
+template <int MODE, int NF, bool DEF>
+int run_prefix(const PreK& a, int nbatch, int nx, int ny, cudaStream_t st) {
+  using C = Cfg<MODE, NF, DEF>;
+  const int64_t nthreads = static_cast<int64_t>(C::NA) * ny * nbatch;
+  prof_begin(CGEF_KERNEL_PREFIX, st);
+  prefix_scan_kernel<MODE, NF, DEF><<<static_cast<unsigned>((nthreads + 127) / 128), 128, 0, st>>>(a);
+  int rc = check_launch("prefix_scan_kernel");
+  if (rc) return rc;
+  dim3 block(128), grid((nx + 127) / 128, ny, nbatch);
+  prefix_sweep_kernel<MODE, NF, DEF><<<grid, block, 0, st>>>(a);
+  prof_end(CGEF_KERNEL_PREFIX, st);
+  return check_launch("prefix_sweep_kernel");
+}
+
+template <int MODE, int NF>
+int dispatch_prefix(bool def, const PreK& a, int nbatch, int nx, int ny, cudaStream_t st) {
+  return def ? run_prefix<MODE, NF, true>(a, nbatch, nx, ny, st) : run_prefix<MODE, NF, false>(a, nbatch, nx, ny, st);
+}
+
+}  // namespace
+
+int launch_prefix(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                  const uint8_t* mask, int64_t mask_slice_stride, double* prefix, const GatherOut& out,
+                  cudaStream_t st) {
+  const bool def = p->strategy == CGEF_DEFORMABLE && (p->masked || mask_slice_stride != 0);
+  PreK a{};
+  a.planes = planes;
+  a.plane_stride = static_cast<int64_t>(p->ny) * pitch;
+  a.slice_stride = np * a.plane_stride;
+  a.pitch = pitch;
+  a.halo = p->H;
+  a.nx = p->nx;
+  a.ny = p->ny;
+  a.ne = p->pre_ne;
+  a.nb = p->pre_nb;
+  a.nslices = nbatch;
+  a.wx = p->dx;
+  a.P = prefix;
+  a.P_plane = static_cast<int64_t>(p->ny) * (p->pre_ne + 1);
+  const int na = (mode == kModePiSphere ? 9 : (mode == kModePiCart ? 5 : nf)) + (def ? 1 : 0);
+  a.P_slice = na * a.P_plane;
+  a.xe = p->d_xe;
+  a.prefix_wx = p->d_prefix_wx;
+  a.rows = p->d_prows;
+  a.x = p->d_x;
+  a.x0 = p->x0;
+  a.dx = p->dx;
+  a.nrep = p->pre_nrep;
+  a.mask = mask;
+  a.mask_stride = mask_slice_stride;
+  for (int m = 0; m < 9; ++m) a.out[m] = out.o[m];
+  a.out_stride = out.slice_stride;
+  const bool sph = mode == kModePiSphere;
+  a.sinlam = sph ? p->d_sinlam : nullptr;
+  a.coslam = sph ? p->d_coslam : nullptr;
+  a.sinphi = sph ? p->d_sinphi : nullptr;
+  a.cosphi = sph ? p->d_cosphi : nullptr;
+  if (mode == kModePiSphere) return dispatch_prefix<kModePiSphere, 1>(def, a, nbatch, p->nx, p->ny, st);
+  if (mode == kModePiCart) return dispatch_prefix<kModePiCart, 1>(def, a, nbatch, p->nx, p->ny, st);
+  switch (nf) {
+    case 1: return dispatch_prefix<kModeFields, 1>(def, a, nbatch, p->nx, p->ny, st);
+    case 2: return dispatch_prefix<kModeFields, 2>(def, a, nbatch, p->nx, p->ny, st);
+    case 3: return dispatch_prefix<kModeFields, 3>(def, a, nbatch, p->nx, p->ny, st);
+    case 4: return dispatch_prefix<kModeFields, 4>(def, a, nbatch, p->nx, p->ny, st);
+    default: return fail(CGEF_EINVAL, "prefix: 1..4 fields per pass");
+  }
+}
+
+int launch_strain(const cgef_plan* p, const StrainArgs& s, cudaStream_t st) {
+  StrainK a{};
+  a.ub = s.ubar;
+  a.vb = s.vbar;
+  a.txx = s.txx;
+  a.txy = s.txy;
+  a.tyy = s.tyy;
+  a.in_stride = s.in_slice_stride;
+  a.mask = s.mask;
+  a.mask_stride = s.mask_slice_stride;
+  a.nx = p->nx;
+  a.ny = p->ny;
+  a.periodic_x = p->periodic_x;
+  a.periodic_y = p->periodic_y;
+  a.sphere = p->geometry == CGEF_SPHERICAL;
+  a.dtype = s.dtype;
+  a.dx = p->dx;
+  a.dy = p->dy;
+  a.yscale = p->geometry == CGEF_SPHERICAL ? 1.0 / p->R : 1.0;
+  a.xscale = p->d_xscale;
+  a.tanfac = p->d_tanfac;
+  a.area = p->d_area;
+  a.pi = s.pi;
+  a.ub_o = s.ubar_o;
+  a.vb_o = s.vbar_o;
+  a.txx_o = s.txx_o;
+  a.txy_o = s.txy_o;
+  a.tyy_o = s.tyy_o;
+  a.sxx_o = s.sxx_o;
+  a.sxy_o = s.sxy_o;
+  a.syy_o = s.syy_o;
+  a.out_stride = s.out_slice_stride;
+  a.partials = s.energy ? s.partials : nullptr;
+  dim3 block(kStrainBX, kStrainBY), grid((p->nx + kStrainBX - 1) / kStrainBX, (p->ny + kStrainBY - 1) / kStrainBY,
+                                         s.nbatch);
+  prof_begin(CGEF_KERNEL_STRAIN, st);
+  strain_kernel<<<grid, block, 0, st>>>(a);
+  prof_end(CGEF_KERNEL_STRAIN, st);
+  int rc = check_launch("strain_kernel");
+  if (rc || !s.energy) return rc;
+  const int64_t nblk = static_cast<int64_t>(grid.x) * grid.y;
+  energy_finish_kernel<<<s.nbatch, 256, 0, st>>>(s.partials, nblk, s.energy, s.energy_stride);
+  return check_launch("energy_finish_kernel");
+}
+
+int launch_energy(const cgef_plan* p, const double* ubar, const double* vbar, int64_t slice_stride,
+                  const uint8_t* mask, int64_t mask_slice_stride, int nbatch, double* partials, double* energy,
+                  int64_t energy_stride, cudaStream_t st) {
+  EnergyK a{ubar, vbar, slice_stride, mask, mask_slice_stride, p->nx, p->ny, p->d_area, partials};
+  dim3 block(kStrainBX, kStrainBY), grid((p->nx + kStrainBX - 1) / kStrainBX, (p->ny + kStrainBY - 1) / kStrainBY,
+                                         nbatch);
+  energy_partial_kernel<<<grid, block, 0, st>>>(a);
+  int rc = check_launch("energy_partial_kernel");
+  if (rc) return rc;
+  const int64_t nblk = static_cast<int64_t>(grid.x) * grid.y;
+  energy_finish_kernel<<<nbatch, 256, 0, st>>>(partials, nblk, energy, energy_stride);
+  return check_launch("energy_finish_kernel");
+}
+
+int launch_derivative(const cgef_plan* p, int axis, int dtype, const void* f, void* out, cudaStream_t st) {
+  const int64_t n = static_cast<int64_t>(p->nx) * p->ny;
+  void* scratch = nullptr;
+  int rc = ensure_ws(const_cast<cgef_plan*>(p), 7, n * sizeof(double), &scratch);
+  if (rc) return rc;
+  to_f64_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(f, dtype, static_cast<double*>(scratch), n);
+  if ((rc = check_launch("to_f64_kernel"))) return rc;
+  DerivK a{f, out, dtype, p->d_mask, p->nx, p->ny, p->periodic_x, p->periodic_y, axis, p->dx, p->dy,
+           p->geometry == CGEF_SPHERICAL ? 1.0 / p->R : 1.0, p->d_xscale, static_cast<double*>(scratch)};
+  dim3 block(kStrainBX, kStrainBY), grid((p->nx + kStrainBX - 1) / kStrainBX, (p->ny + kStrainBY - 1) / kStrainBY);
+  derivative_kernel<<<grid, block, 0, st>>>(a);
+  return check_launch("derivative_kernel");
+}
+
+int launch_convert(const double* src, int64_t src_stride, void* dst, int64_t dst_stride, int dtype, int64_t n,
+                   int nbatch, cudaStream_t st) {
+  dim3 grid(static_cast<unsigned>((n + 255) / 256), nbatch);
+  convert_kernel<<<grid, 256, 0, st>>>(src, src_stride, dst, dst_stride, dtype, n);
+  return check_launch("convert_kernel");
+}
+
+}  // namespace cgef

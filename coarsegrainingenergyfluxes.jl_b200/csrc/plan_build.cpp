@@ -1,0 +1,445 @@
+// Host-side plan construction: the footprint tables every engine reads, built once per
+// (grid, kernel, scale, mask strategy) as Filtering.plan_filter does (Filtering.jl:2931-2954).
+// Geometry follows the reference's documented conventions: great-circle distance in the
+// haversine form (Filtering.jl:264-265), cell measure R^2 cos(phi) dlambda dphi
+// (docs/src/theory.md:307), kernel weights and radii of Kernels.jl:318-379.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "cgef_internal.h"
+
+namespace cgef {
+
+double kernel_weight(int kernel, double alpha, double d, double ell) {
+  if (kernel == CGEF_TOPHAT) return d <= ell / 2.0 ? 1.0 : 0.0;  // Kernels.jl:318-320
+  double q = d / ell;
+  return std::exp(-alpha * (q * q));  // Kernels.jl:322-324
+}
+
+double kernel_radius(int kernel, double alpha, double ell) {
+  if (kernel == CGEF_TOPHAT) return ell / 2.0;                       // Kernels.jl:354
+  return ell * std::sqrt(-std::log(kGaussianTruncationTol) / alpha);  // Kernels.jl:356-359
+}
+
+namespace {
+
+inline double coord(double x0, double d, int i) { return std::fma(static_cast<double>(i), d, x0); }
+
+double sphere_distance(double R, double x1, double y1, double x2, double y2) {
+  double sdp = std::sin((y2 - y1) / 2.0), sdl = std::sin((x2 - x1) / 2.0);
+  double h = sdp * sdp + std::cos(y1) * std::cos(y2) * sdl * sdl;
+  if (h > 1.0) h = 1.0;
+  return 2.0 * R * std::asin(std::sqrt(h));
+}
+
+// Column half-width that certainly covers the part of row phi2 within rad of (0, phi1): the
+// spherical band formula plus a two-cell margin, capped at `cap`.  Inclusion itself is decided by
+// the distance test, so only coverage matters here.
+int sphere_row_window(double R, double dx, double phi1, double phi2, double rad, int cap) {
+  double den = std::cos(phi1) * std::cos(phi2);
+  double num = std::cos(rad / R) - std::sin(phi1) * std::sin(phi2);
+  if (den <= 0.0) return cap;
+  double c = num / den;
+  if (c <= -1.0) return cap;
+  if (c > 1.0) return std::min(2, cap);
+  double w = std::floor(std::acos(c) / std::fabs(dx)) + 2.0;
+  return w > cap ? cap : static_cast<int>(w);
+}
+
+// Connectivity.metric_band (Filtering.jl:761-765, 1004): axis-1 half-width of the top-hat
+// support between rows y_t and y_s, negative when the row is out of reach.
+double metric_band(int geometry, double R, double y_t, double y_s, double rad) {
+  if (geometry == CGEF_CARTESIAN) {
+    double dy = y_s - y_t;
+    double r2 = rad * rad - dy * dy;
+    return r2 < 0.0 ? -1.0 : std::sqrt(r2);
+  }
+  double den = std::cos(y_t) * std::cos(y_s);
+  double num = std::cos(rad / R) - std::sin(y_t) * std::sin(y_s);
+  if (den <= 0.0) return num <= 0.0 ? M_PI : -1.0;
+  double c = num / den;
+  if (c > 1.0) return -1.0;
+  if (c < -1.0) return M_PI;
+  return std::acos(c);
+}
+
+template <typename T>
+int upload(const cgef_plan* p, T** dst, const T* src, size_t n) {
+  if (n == 0 || p->device < 0) {  // no device: host tables only
+    *dst = nullptr;
+    return CGEF_OK;
+  }
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), n * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(plan table)");
+  e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(plan table)");
+  return CGEF_OK;
+}
+
+struct Banded {
+  int D = 0;
+  int Amax = 0;
+  std::vector<BandRow> rows;  // ny * (2D+1) (sphere) or 2D+1 (Cartesian, one band)
+  std::vector<double> w;      // half rows
+  std::vector<int32_t> di, dj;
+  std::vector<double> wcsr;
+  std::vector<int64_t> ptr;
+};
+
+// Banded footprint (Filtering.jl:636-732).  Each (band, row offset) holds a contiguous
+// longitude interval [-a, hi]; weights are stored once per |di| because the kernel of the
+// great-circle (or Euclidean) distance is even in di.  A column inside the interval that fails
+// d <= rad keeps weight 0, which adds nothing to either sum, so the entry set is the reference's.
+void build_banded(const cgef_plan* p, Banded& B) {
+  const int nx = p->nx, ny = p->ny;
+  const double rad = p->rad;
+  const bool sphere = p->geometry == CGEF_SPHERICAL;
+  if (!sphere) {
+    const int di_lim = p->dx > 0 ? static_cast<int>(std::ceil(rad / p->dx)) : 0;
+    const int dj_lim = p->dy > 0 ? static_cast<int>(std::ceil(rad / p->dy)) : 0;
+    const double A = p->dx * p->dy;
+    B.D = dj_lim;
+    B.rows.assign(2 * dj_lim + 1, BandRow{0, -1, -1, 0});
+    B.ptr.push_back(0);
+    for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
+      int a = -1;
+      std::vector<double> half;
+      for (int ddi = 0; ddi <= di_lim; ++ddi) {
+        double x = ddi * p->dx, y = ddj * p->dy;
+        double d = std::sqrt(x * x + y * y);
+        if (d <= rad) a = ddi;
+      }
+      for (int ddi = -di_lim; ddi <= di_lim; ++ddi) {
+        double x = ddi * p->dx, y = ddj * p->dy;
+        double d = std::sqrt(x * x + y * y);
+        if (d <= rad) {
+          B.di.push_back(ddi);
+          B.dj.push_back(ddj);
+          B.wcsr.push_back(kernel_weight(p->kernel, p->alpha, d, p->scale) * A);
+        }
+      }
+      BandRow& r = B.rows[ddj + dj_lim];
+      if (a >= 0) {
+        r.woff = static_cast<int32_t>(B.w.size());
+        r.a = a;
+        r.hi = a;
+        for (int ddi = 0; ddi <= a; ++ddi) {
+          double x = ddi * p->dx, y = ddj * p->dy;
+          double d = std::sqrt(x * x + y * y);
+          B.w.push_back(d <= rad ? kernel_weight(p->kernel, p->alpha, d, p->scale) * A : 0.0);
+        }
+        B.Amax = std::max(B.Amax, a);
+      }
+    }
+    B.ptr.push_back(static_cast<int64_t>(B.di.size()));
+    return;
+  }
+  const int dj_lim = p->dy > 0 ? static_cast<int>(std::ceil(rad / (p->R * p->dy))) : 0;
+  const int half = nx / 2;
+  B.D = dj_lim;
+  B.rows.assign(static_cast<size_t>(ny) * (2 * dj_lim + 1), BandRow{0, -1, -1, 0});
+  B.ptr.push_back(0);
+  for (int j = 0; j < ny; ++j) {
+    const double phi = coord(p->y0, p->dy, j);
+    bool closed = false;
+    for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
+      int jj = j + ddj;
+      if (jj < 0 || jj >= ny) continue;
+      if (sphere_row_window(p->R, p->dx, phi, coord(p->y0, p->dy, jj), rad, half) >= half) closed = true;
+    }
+    for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
+      int jj = j + ddj;
+      if (jj < 0 || jj >= ny) continue;
+      const double phi2 = coord(p->y0, p->dy, jj);
+      const double A = p->R * p->R * std::cos(phi2) * p->dx * p->dy;
+      const int win = closed ? half : sphere_row_window(p->R, p->dx, phi, phi2, rad, half);
+      const int lo = -win;
+      const int hi = (closed && 2 * half + 1 > nx) ? half - 1 : win;
+      // weights by |di|; inclusion exactly as the reference (d <= rad at each visited offset)
+      int amax = -1;
+      std::vector<double> wabs(static_cast<size_t>(win) + 1, 0.0);
+      for (int ddi = lo; ddi <= hi; ++ddi) {
+        double d = sphere_distance(p->R, 0.0, phi, static_cast<double>(ddi) * p->dx, phi2);
+        if (d <= rad) {
+          double wv = kernel_weight(p->kernel, p->alpha, d, p->scale) * A;
+          B.di.push_back(ddi);
+          B.dj.push_back(ddj);
+          B.wcsr.push_back(wv);
+          wabs[std::abs(ddi)] = wv;
+          amax = std::max(amax, std::abs(ddi));
+        }
+      }
+      BandRow& r = B.rows[static_cast<size_t>(j) * (2 * dj_lim + 1) + (ddj + dj_lim)];
+      if (amax >= 0) {
+        r.woff = static_cast<int32_t>(B.w.size());
+        r.a = amax;
+        r.hi = std::min(amax, hi);
+        for (int k = 0; k <= amax; ++k) B.w.push_back(wabs[k]);
+        B.Amax = std::max(B.Amax, amax);
+      }
+    }
+    B.ptr.push_back(static_cast<int64_t>(B.di.size()));
+  }
+}
+
+}  // namespace
+
+int build_plan_tables(cgef_plan* p) {
+  const int nx = p->nx, ny = p->ny;
+  const bool sphere = p->geometry == CGEF_SPHERICAL;
+  p->rad = kernel_radius(p->kernel, p->alpha, p->scale);
+  p->h_x.resize(nx);
+  p->h_y.resize(ny);
+  for (int i = 0; i < nx; ++i) p->h_x[i] = coord(p->x0, p->dx, i);
+  for (int j = 0; j < ny; ++j) p->h_y[j] = coord(p->y0, p->dy, j);
+  std::vector<double> sinlam(nx), coslam(nx), sinphi(ny), cosphi(ny), area(ny), xscale(ny), tanfac(ny);
+  for (int i = 0; i < nx; ++i) {
+    sinlam[i] = std::sin(p->h_x[i]);
+    coslam[i] = std::cos(p->h_x[i]);
+  }
+  for (int j = 0; j < ny; ++j) {
+    double phi = p->h_y[j];
+    sinphi[j] = std::sin(phi);
+    cosphi[j] = std::cos(phi);
+    if (sphere) {
+      area[j] = p->R * p->R * std::cos(phi) * p->dx * p->dy;
+      double c = std::cos(phi);
+      xscale[j] = std::fabs(c) < std::sqrt(2.220446049250313e-16) ? 0.0 : 1.0 / (p->R * c);
+      double sp = std::sin(phi), cp = std::cos(phi);
+      tanfac[j] = std::fabs(cp) > 1e-12 ? sp / (p->R * cp) : 0.0;
+    } else {
+      area[j] = p->dx * p->dy;
+      xscale[j] = 1.0;
+      tanfac[j] = 0.0;
+    }
+  }
+  p->active_area = 0.0;
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i)
+      if (p->h_mask.empty() || p->h_mask[static_cast<size_t>(j) * nx + i]) p->active_area += area[j];
+
+  Banded B;
+  std::vector<double> den_zf;
+  std::vector<double> gx, gy, px, py;
+  std::vector<double> xe, prefix_wx;
+  std::vector<PrefixRow> prows;
+
+  if (p->engine == CGEF_ENGINE_BANDED) {
+    build_banded(p, B);
+    p->D = B.D;
+    p->Amax = B.Amax;
+    p->dj_lim = B.D;
+    p->di_max = B.Amax;
+    p->h_di = B.di;
+    p->h_dj = B.dj;
+    p->h_w = B.wcsr;
+    p->h_ptr = B.ptr;
+    p->nentries = static_cast<int64_t>(B.di.size());
+    const int nb = sphere ? ny : 1;
+    // ZeroFill denominator: the footprint mass over in-domain entries, in CSR order
+    // (Filtering.jl:2574-2582 accumulate w for every in-domain entry).
+    const int64_t W = 2 * B.D + 1;
+    (void)nb;
+    if (p->periodic_x) {
+      p->den_zf_2d = 0;
+      den_zf.assign(ny, 0.0);
+      for (int j = 0; j < ny; ++j) {
+        int b = sphere ? j : 0;
+        double s = 0.0;
+        for (int64_t k = B.ptr[b]; k < B.ptr[b + 1]; ++k) {
+          int jj = j + B.dj[k];
+          if ((jj < 0 || jj >= ny) && !p->periodic_y) continue;
+          s += B.wcsr[k];
+        }
+        den_zf[j] = s;
+      }
+    } else {
+      p->den_zf_2d = 1;
+      den_zf.assign(static_cast<size_t>(ny) * nx, 0.0);
+      for (int j = 0; j < ny; ++j) {
+        int b = sphere ? j : 0;
+        // interior columns see every entry; edge columns are summed entry by entry
+        double full = 0.0;
+        for (int64_t k = B.ptr[b]; k < B.ptr[b + 1]; ++k) {
+          int jj = j + B.dj[k];
+          if ((jj < 0 || jj >= ny) && !p->periodic_y) continue;
+          full += B.wcsr[k];
+        }
+        for (int i = 0; i < nx; ++i) {
+          double s = full;
+          if (i < B.Amax || i >= nx - B.Amax) {
+            s = 0.0;
+            for (int64_t k = B.ptr[b]; k < B.ptr[b + 1]; ++k) {
+              int jj = j + B.dj[k];
+              if ((jj < 0 || jj >= ny) && !p->periodic_y) continue;
+              int ii = i + B.di[k];
+              if (ii < 0 || ii >= nx) continue;
+              s += B.wcsr[k];
+            }
+          }
+          den_zf[static_cast<size_t>(j) * nx + i] = s;
+        }
+      }
+    }
+    (void)W;
+    // Work items: kRows target rows x (32 * kWarps) columns, or 32 columns with the warps
+    // dividing the source columns where a band is heavy; longest first.
+    const int wide = 32 * kWarps;
+    std::vector<WorkItem> items;
+    std::vector<double> rowcost;  // per row group: sum over source rows of the union width
+    const int ngroups = (ny + kRows - 1) / kRows;
+    rowcost.assign(ngroups, 0.0);
+    for (int g = 0; g < ngroups; ++g) {
+      int j0 = g * kRows;
+      double c = 0.0;
+      for (int jr = j0 - B.D; jr <= j0 + kRows - 1 + B.D; ++jr) {
+        if (!p->periodic_y && (jr < 0 || jr >= ny)) continue;
+        int A = -1;
+        for (int t = 0; t < kRows; ++t) {
+          int j = j0 + t;
+          if (j >= ny) continue;
+          int dj = jr - j;
+          if (dj < -B.D || dj > B.D) continue;
+          const BandRow& r = B.rows[(sphere ? static_cast<size_t>(j) * W : 0) + (dj + B.D)];
+          A = std::max(A, r.a);
+        }
+        if (A >= 0) c += 2.0 * A + 1.0;
+      }
+      rowcost[g] = c;
+    }
+    const int ntx_wide = (nx + wide - 1) / wide;
+    double total = 0.0;
+    for (int g = 0; g < ngroups; ++g) total += rowcost[g] * ntx_wide * wide;
+    int sms = 148;
+    {
+      int dev = 0;
+      cudaDeviceProp prop;
+      if (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
+        sms = prop.multiProcessorCount;
+      else
+        cudaGetLastError();
+    }
+    const double heavy = total / sms / 6.0;
+    for (int g = 0; g < ngroups; ++g) {
+      int j0 = g * kRows;
+      bool split = rowcost[g] * wide > heavy;
+      if (split) {
+        for (int x = 0; x < nx; x += 32)
+          items.push_back(WorkItem{x, j0, 1, static_cast<int32_t>(std::min(rowcost[g] * 32.0, 2e9))});
+      } else {
+        for (int x = 0; x < nx; x += wide)
+          items.push_back(WorkItem{x, j0, 0, static_cast<int32_t>(std::min(rowcost[g] * wide / kWarps, 2e9))});
+      }
+    }
+    std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
+    p->h_items = items;
+    p->H = std::max(B.Amax, 1);
+    int rc;
+    if ((rc = upload(p, &p->d_rows, B.rows.data(), B.rows.size())) != CGEF_OK) return rc;
+    if (B.w.empty()) B.w.push_back(0.0);
+    if ((rc = upload(p, &p->d_w, B.w.data(), B.w.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_items, items.data(), items.size())) != CGEF_OK) return rc;
+  } else if (p->engine == CGEF_ENGINE_SEPARABLE) {
+    // Filtering.jl:1391-1463: square truncation, lim = ceil(rad / step), point-sampled profile.
+    p->di_lim = p->dx > 0 ? static_cast<int>(std::ceil(p->rad / p->dx)) : 0;
+    p->sep_dj_lim = p->dy > 0 ? static_cast<int>(std::ceil(p->rad / p->dy)) : 0;
+    p->dj_lim = p->sep_dj_lim;
+    p->di_max = p->di_lim;
+    for (int k = -p->di_lim; k <= p->di_lim; ++k)
+      gx.push_back(kernel_weight(CGEF_GAUSSIAN, p->alpha, std::fabs(static_cast<double>(k) * p->dx), p->scale));
+    for (int k = -p->sep_dj_lim; k <= p->sep_dj_lim; ++k)
+      gy.push_back(kernel_weight(CGEF_GAUSSIAN, p->alpha, std::fabs(static_cast<double>(k) * p->dy), p->scale));
+    auto profile = [](int lim, const std::vector<double>& g, int n, int periodic) {
+      std::vector<double> out(n);
+      for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int dd = -lim; dd <= lim; ++dd) {
+          int ii = i + dd;
+          if ((ii >= 0 && ii < n) || periodic) s += g[dd + lim];
+        }
+        out[i] = s;
+      }
+      return out;
+    };
+    px = profile(p->di_lim, gx, nx, p->periodic_x);
+    py = profile(p->sep_dj_lim, gy, ny, p->periodic_y);
+    p->H = std::max(p->di_lim, 1);
+    int rc;
+    if ((rc = upload(p, &p->d_gx, gx.data(), gx.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_gy, gy.data(), gy.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_px, px.data(), px.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_py, py.data(), py.size())) != CGEF_OK) return rc;
+  } else {
+    // Prefix-sum top-hat (Filtering.jl:833-907): measure factors, the tripled periodic axis,
+    // the row band and per (row, band slot) the support half-width (Filtering.jl:990-1005).
+    const double wxv = p->dx;
+    p->x_period = (p->periodic_x && nx > 1) ? nx * p->dx : 0.0;
+    p->y_period = (p->periodic_y && ny > 1) ? ny * p->dy : 0.0;
+    const double dy_phys = sphere ? p->R * p->dy : p->dy;
+    int lim = (std::isfinite(dy_phys) && dy_phys > 0) ? static_cast<int>(std::ceil(p->rad / dy_phys)) : 0;
+    p->dj_lim = std::min(lim, ny - 1);
+    p->pre_nrep = (p->periodic_x && nx > 1) ? 3 : 1;
+    p->pre_ne = p->pre_nrep * nx;
+    xe.resize(p->pre_ne);
+    for (int r = 0; r < p->pre_nrep; ++r)
+      for (int t = 0; t < nx; ++t)
+        xe[static_cast<size_t>(r) * nx + t] =
+            p->h_x[t] + (p->pre_nrep == 3 ? static_cast<double>(r - 1) * p->x_period : 0.0);
+    prefix_wx.resize(p->pre_ne + 1);
+    prefix_wx[0] = 0.0;
+    for (int k = 0; k < p->pre_ne; ++k) prefix_wx[k + 1] = prefix_wx[k] + wxv;
+    const int nbs = std::min(2 * p->dj_lim + 1, ny);
+    p->pre_nb = nbs;
+    prows.assign(static_cast<size_t>(ny) * nbs, PrefixRow{-1, 0, 0, 0, 0.0, 0.0});
+    const bool uniform_fast = !p->periodic_x && p->pre_ne == nx && p->dx > 0;
+    for (int j = 0; j < ny; ++j) {
+      const double y_t = p->h_y[j];
+      for (int b = 0; b < nbs; ++b) {
+        PrefixRow& pr = prows[static_cast<size_t>(j) * nbs + b];
+        int jj_raw = j - p->dj_lim + b;
+        if (!(p->periodic_y || (jj_raw >= 0 && jj_raw < ny))) continue;
+        int jj = ((jj_raw % ny) + ny) % ny;
+        double dyv = p->h_y[jj] - y_t;
+        if (p->periodic_y && p->y_period > 0.0) dyv -= p->y_period * std::round(dyv / p->y_period);
+        double hw = metric_band(p->geometry, p->R, y_t, y_t + dyv, p->rad);
+        if (hw < 0.0) continue;
+        pr.jj = jj;
+        pr.hw = hw;
+        pr.wy = sphere ? p->R * p->R * std::cos(p->h_y[jj]) * p->dy : p->dy;
+        if (p->periodic_x && p->pre_ne > nx && 2.0 * hw >= p->x_period) {
+          pr.mode = 1;
+        } else if (uniform_fast) {
+          int w = 0;
+          while ((w + 1) * p->dx <= hw) ++w;
+          pr.mode = 2;
+          pr.w = w;
+        } else {
+          pr.mode = 3;
+        }
+      }
+    }
+    p->H = 1;
+    int rc;
+    if ((rc = upload(p, &p->d_xe, xe.data(), xe.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_prefix_wx, prefix_wx.data(), prefix_wx.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_prows, prows.data(), prows.size())) != CGEF_OK) return rc;
+  }
+
+  int rc;
+  if ((rc = upload(p, &p->d_x, p->h_x.data(), nx)) != CGEF_OK) return rc;
+  if ((rc = upload(p, &p->d_sinlam, sinlam.data(), nx)) != CGEF_OK) return rc;
+  if ((rc = upload(p, &p->d_coslam, coslam.data(), nx)) != CGEF_OK) return rc;
+  if ((rc = upload(p, &p->d_sinphi, sinphi.data(), ny)) != CGEF_OK) return rc;
+  if ((rc = upload(p, &p->d_cosphi, cosphi.data(), ny)) != CGEF_OK) return rc;
+  if ((rc = upload(p, &p->d_area, area.data(), ny)) != CGEF_OK) return rc;
+  if ((rc = upload(p, &p->d_xscale, xscale.data(), ny)) != CGEF_OK) return rc;
+  if ((rc = upload(p, &p->d_tanfac, tanfac.data(), ny)) != CGEF_OK) return rc;
+  if (!p->h_mask.empty())
+    if ((rc = upload(p, &p->d_mask, p->h_mask.data(), p->h_mask.size())) != CGEF_OK) return rc;
+  return CGEF_OK;
+}
+
+}  // namespace cgef

@@ -1,0 +1,190 @@
+/*
+ * cgef_b200.h -- C ABI of the B200 coarse-graining library (libcgef_b200.so).
+ *
+ * Drop-in replacement for the real-space hot path of jbphyswx/CoarseGrainingEnergyFluxes.jl:
+ * the footprint filter behind `Filtering.plan_filter` / `filter_apply!` / `filter_apply_batch!`,
+ * the strain stencils of `Derivatives.ddx!`/`ddy!`, the flux `Diagnostics.compute_Π!`, the
+ * area-weighted `cumulative_energy!`, and the scale-by-slice sweep of `Pipeline.coarse_grain!` /
+ * `coarse_grain_batch!` / `coarse_grain_slices!`.  Every entry point below names the reference
+ * interface it replaces (file:line in the reference repository).
+ *
+ * Conventions
+ *  - Fields are the reference's column-major (Nx, Ny[, batch...]) arrays, i.e. C row-major
+ *    [batch][ny][nx] with the x (longitude) index fastest.
+ *  - Host-buffer entry points (`cgef_filter`, `cgef_compute_pi`, ...) are synchronous and copy
+ *    through device memory owned by the plan; `*_device` entry points take device pointers and a
+ *    cudaStream_t (passed as void*) and return without synchronising.
+ *  - All calls return CGEF_OK (0) or a negative status; `cgef_last_error()` gives the message of
+ *    the calling thread's last failure.
+ *  - A plan is used by one host thread at a time (the reference's "one plan per task",
+ *    Derivatives.jl:74-77); different plans may run concurrently.
+ *  - Arithmetic is FP64 on the device: footprint sums accumulate with double-precision FMA and
+ *    the subtraction tau = (uu)bar - ubar ubar, the normalisation and the energy reductions are
+ *    FP64.  `dtype` selects only the storage type of inputs and outputs.
+ */
+#ifndef CGEF_B200_H
+#define CGEF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGEF_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+  CGEF_OK = 0,
+  CGEF_EINVAL = -1,       /* bad shape / argument: ArgumentError, DimensionMismatch in the reference */
+  CGEF_ENOMEM = -2,       /* device or host allocation failed */
+  CGEF_ECUDA = -3,        /* a CUDA runtime call failed */
+  CGEF_ESTRATEGY = -4,    /* plan built for another mask strategy (Filtering.jl:952-965, 1484-1503) */
+  CGEF_EUNSUPPORTED = -5, /* combination outside the supported path */
+  CGEF_ENODEVICE = -6     /* no CUDA device visible */
+};
+
+/* Geometry (FlowGeometries.Geometry.CartesianGeometry / SphericalGeometry). */
+enum { CGEF_CARTESIAN = 0, CGEF_SPHERICAL = 1 };
+/* Kernels (Kernels.jl:28 TopHatKernel, :59-62 GaussianKernel). */
+enum { CGEF_TOPHAT = 0, CGEF_GAUSSIAN = 1 };
+/* Mask strategies (Filtering.jl:36-48 ZeroFill, :50-57 Deformable). */
+enum { CGEF_ZEROFILL = 0, CGEF_DEFORMABLE = 1 };
+/* Engines: AUTO dispatches as the reference does (Filtering.jl:636-749, 1121-1141, 1533-1561):
+ * Gaussian on Cartesian -> SEPARABLE, top-hat -> PREFIXSUM, otherwise BANDED. */
+enum { CGEF_ENGINE_AUTO = 0, CGEF_ENGINE_BANDED = 1, CGEF_ENGINE_SEPARABLE = 2, CGEF_ENGINE_PREFIXSUM = 3 };
+/* Storage types of caller buffers. */
+enum { CGEF_F64 = 0, CGEF_F32 = 1 };
+
+/* A uniform 2-D structured grid (FlowGeometries.Grids.StructuredGrid over two ranges).
+ * Coordinates: x_i = x0 + i*dx, y_j = y0 + j*dy, evaluated as fma(i, dx, x0); radians on the
+ * sphere (x = longitude, y = latitude).  `mask` is host memory, ny*nx bytes, nonzero = active
+ * (NULL = every cell active); it is copied at plan creation. */
+typedef struct cgef_grid_desc {
+  int32_t geometry;
+  int32_t periodic_x;
+  int32_t periodic_y;
+  int32_t reserved;
+  int64_t nx;
+  int64_t ny;
+  double x0, dx, y0, dy;
+  double radius; /* sphere radius in metres (ignored on the plane) */
+  const uint8_t* mask;
+} cgef_grid_desc;
+
+typedef struct cgef_plan cgef_plan;
+
+typedef struct cgef_plan_info {
+  int32_t engine;     /* CGEF_ENGINE_* actually built */
+  int32_t nbands;     /* banded: 1 (Cartesian) or ny (sphere); 0 otherwise */
+  int64_t nentries;   /* banded: footprint entries summed over bands */
+  int32_t dj_lim;     /* row half-width of the footprint */
+  int32_t di_max;     /* widest column half-width over all bands (banded/separable) */
+  double kernel_radius;
+  double active_area; /* sum of active-cell areas of the plan's grid mask */
+} cgef_plan_info;
+
+/* Optional outputs of the flux computation; every non-NULL buffer holds nbatch*ny*nx values of
+ * the call's dtype, except `energy` (nbatch doubles).  Local-frame components on the sphere
+ * (east/north), Diagnostics.jl:596-650. */
+typedef struct cgef_pi_outputs {
+  void* pi;      /* -(Sxx tau_xx + 2 Sxy tau_xy + Syy tau_yy) on active cells, else 0 (no rho0) */
+  void* ubar;
+  void* vbar;
+  void* tau_xx;
+  void* tau_xy;
+  void* tau_yy;
+  void* s_xx;
+  void* s_xy;
+  void* s_yy;
+  double* energy; /* E = 1/2 <|ubar|^2>, area weighted over active cells (Diagnostics.jl:1086-1134) */
+} cgef_pi_outputs;
+
+/* Library/ABI version (CGEF_ABI_VERSION). */
+int32_t cgef_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* cgef_last_error(void);
+
+/* Number of visible CUDA devices (0 when none; never fails). */
+int32_t cgef_device_count(void);
+
+/* Filtering.plan_filter (Filtering.jl:2931-2954) plus the GPU extension's prepare_workspace
+ * upload (Filtering.jl:2910-2912; ext/CoarseGrainingEnergyFluxesKernelAbstractionsExt.jl:474-571):
+ * builds the engine's tables on the host once and keeps them resident on the current device.
+ * scale must be finite and positive (Filtering.jl:2917-2922). */
+int32_t cgef_plan_create(cgef_plan** out, const cgef_grid_desc* grid, int32_t kernel, double alpha, double scale,
+                         int32_t mask_strategy, int32_t engine);
+
+/* Releases the plan's device and host memory. */
+int32_t cgef_plan_destroy(cgef_plan* plan);
+
+/* Plan statistics. */
+int32_t cgef_plan_get_info(const cgef_plan* plan, cgef_plan_info* info);
+
+/* Banded footprint of the plan in the reference's CSR form (FilterFootprint, Filtering.jl:327-336):
+ * di/dj/w have nentries entries, ptr has nbands+1 (0-based offsets).  Any pointer may be NULL. */
+int32_t cgef_plan_get_footprint(const cgef_plan* plan, int32_t* di, int32_t* dj, double* w, int64_t* ptr);
+
+/* Filtering.filter_apply! (Filtering.jl:3242-3256) and filter_apply_batched! over a trailing
+ * batch axis (Filtering.jl:3286-3305), replacing gpu_filter_field! / gpu_filter_field_batched!
+ * (Filtering.jl:195-197, 3342-3344).  field/out: nbatch*ny*nx host values of dtype. */
+int32_t cgef_filter(cgef_plan* plan, int32_t dtype, const void* field, void* out, int64_t nbatch);
+
+/* Filtering.filter_apply_batch! (Filtering.jl:3360-3375): k separate fields through one
+ * footprint traversal.  fields[m]/outs[m]: ny*nx host values of dtype. */
+int32_t cgef_filter_batch(cgef_plan* plan, int32_t dtype, const void* const* fields, void* const* outs, int32_t k);
+
+/* Diagnostics.compute_Π! for a 2-D StructuredGrid (Diagnostics.jl:389-416, 472-702), batched over
+ * nbatch slices sharing the grid (the batch-native driver, Pipeline.jl:519-563).  slice_masks is
+ * NULL (use the plan's grid mask) or nbatch*ny*nx host bytes, one mask per slice
+ * (coarse_grain_slices!, Pipeline.jl:866-904). */
+int32_t cgef_compute_pi(cgef_plan* plan, int32_t dtype, const void* u, const void* v, int64_t nbatch,
+                        const uint8_t* slice_masks, const cgef_pi_outputs* out);
+
+/* Diagnostics.cumulative_energy! (Diagnostics.jl:1144-1217): u, v (ny*nx, dtype) filtered as
+ * scalars at every plan's scale; spectrum[s] = 1/2 <|ubar|^2>.  All plans share one grid. */
+int32_t cgef_cumulative_energy(cgef_plan* const* plans, int32_t nscales, int32_t dtype, const void* u,
+                               const void* v, double* spectrum);
+
+/* Pipeline.coarse_grain! / coarse_grain_batch! / coarse_grain_profile! (Pipeline.jl:412-468,
+ * 686-717, 991-1007): Pi and E(l) for every (slice, scale).  pi: NULL or
+ * nbatch*nscales*ny*nx values of dtype ([slice][scale][ny][nx], the reference's trailing
+ * (Nscales, batch) axes); energy: NULL or nbatch*nscales doubles ([slice][scale]). */
+int32_t cgef_sweep(cgef_plan* const* plans, int32_t nscales, int32_t dtype, const void* u, const void* v,
+                   int64_t nbatch, const uint8_t* slice_masks, void* pi, double* energy);
+
+/* Derivatives.ddx! / ddy! (Derivatives.jl:42-51, 141-142): 3-node first derivative with the
+ * ReduceInRun mask policy and the sphere's metric division; f/out: ny*nx host values of dtype. */
+int32_t cgef_ddx(cgef_plan* plan, int32_t dtype, const void* f, void* out);
+int32_t cgef_ddy(cgef_plan* plan, int32_t dtype, const void* f, void* out);
+
+/* Device-pointer forms of the calls above: same semantics, buffers in device memory of the
+ * plan's device, work queued on `stream` (a cudaStream_t; NULL = legacy default stream). */
+int32_t cgef_filter_device(cgef_plan* plan, int32_t dtype, const void* field, void* out, int64_t nbatch,
+                           void* stream);
+int32_t cgef_compute_pi_device(cgef_plan* plan, int32_t dtype, const void* u, const void* v, int64_t nbatch,
+                               const uint8_t* slice_masks, const cgef_pi_outputs* out, void* stream);
+int32_t cgef_sweep_device(cgef_plan* const* plans, int32_t nscales, int32_t dtype, const void* u, const void* v,
+                          int64_t nbatch, const uint8_t* slice_masks, void* pi, double* energy, void* stream);
+
+/* Tracing (no counterpart in the reference, which has none).  Kernel launches made by this
+ * thread's calls since the last reset. */
+int64_t cgef_launch_count(void);
+void cgef_reset_launch_count(void);
+
+/* Per-kernel device timing: while enabled, this thread's calls bracket every launch of the kinds
+ * below with CUDA events on the launch's own stream.  `cgef_profile_read` waits for the recorded
+ * events and returns the summed duration (ms) and launch count of one kind since the last reset. */
+enum { CGEF_KERNEL_STAGE = 0, CGEF_KERNEL_BANDED = 1, CGEF_KERNEL_SEPARABLE = 2, CGEF_KERNEL_PREFIX = 3,
+       CGEF_KERNEL_STRAIN = 4, CGEF_KERNEL_KINDS = 5 };
+void cgef_profile_enable(int32_t enable);
+int32_t cgef_profile_read(int32_t kind, double* total_ms, int64_t* launches);
+void cgef_profile_reset(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CGEF_B200_H */
