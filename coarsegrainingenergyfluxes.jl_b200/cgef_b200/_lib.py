@@ -31,7 +31,7 @@ EXPORTED = [
     "cgef_plan_get_info", "cgef_plan_get_footprint", "cgef_filter", "cgef_filter_batch", "cgef_compute_pi",
     "cgef_cumulative_energy", "cgef_sweep", "cgef_ddx", "cgef_ddy", "cgef_filter_device",
     "cgef_compute_pi_device", "cgef_sweep_device", "cgef_launch_count", "cgef_reset_launch_count",
-    "cgef_profile_enable", "cgef_profile_read", "cgef_profile_reset",
+    "cgef_profile_enable", "cgef_profile_read", "cgef_profile_reset", "cgef_filter_device_noalloc",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN = 0, 1, 2, 3, 4
 
@@ -111,6 +111,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_ddy.restype = i32
     L.cgef_filter_device.argtypes = [vp, i32, vp, vp, i64, vp]
     L.cgef_filter_device.restype = i32
+    L.cgef_filter_device_noalloc.argtypes = [vp, i32, vp, vp, i64, vp]
+    L.cgef_filter_device_noalloc.restype = i32
     L.cgef_compute_pi_device.argtypes = [vp, i32, vp, vp, i64, vp, C.POINTER(PiOutputs), vp]
     L.cgef_compute_pi_device.restype = i32
     L.cgef_sweep_device.argtypes = [vp, i32, i32, vp, vp, i64, vp, vp, vp, vp]

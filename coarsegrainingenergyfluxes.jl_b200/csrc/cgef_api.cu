@@ -20,6 +20,7 @@ struct ProfRec {
   cudaEvent_t a, b;
 };
 thread_local bool g_prof = false;
+thread_local bool g_prof_suspended = false;
 thread_local std::vector<ProfRec> g_recs;
 thread_local cudaEvent_t g_open = nullptr;
 thread_local int g_open_kind = -1;
@@ -41,8 +42,10 @@ void drain_profile() {
 }
 }  // namespace
 
+void prof_suspend(bool suspend) { g_prof_suspended = suspend; }
+
 void prof_begin(int kind, cudaStream_t st) {
-  if (!g_prof) return;
+  if (!g_prof || g_prof_suspended) return;
   cudaEvent_t e;
   if (cudaEventCreate(&e) != cudaSuccess) return;
   cudaEventRecord(e, st);
@@ -51,7 +54,7 @@ void prof_begin(int kind, cudaStream_t st) {
 }
 
 void prof_end(int kind, cudaStream_t st) {
-  if (!g_prof || g_open == nullptr || g_open_kind != kind) return;
+  if (!g_prof || g_prof_suspended || g_open == nullptr || g_open_kind != kind) return;
   cudaEvent_t e;
   if (cudaEventCreate(&e) != cudaSuccess) return;
   cudaEventRecord(e, st);

@@ -138,6 +138,8 @@ void count_launch(int64_t n = 1);
 // Tracing: events around one launch of `kind` on stream `st` (no-ops unless enabled).
 void prof_begin(int kind, cudaStream_t st);
 void prof_end(int kind, cudaStream_t st);
+// Suspends tracing on this thread (the allocation-free entry point creates no events).
+void prof_suspend(bool suspend);
 
 // ---- launchers (kernels.cu) ----
 struct StageArgs {

@@ -169,6 +169,19 @@ int32_t cgef_compute_pi_device(cgef_plan* plan, int32_t dtype, const void* u, co
 int32_t cgef_sweep_device(cgef_plan* const* plans, int32_t nscales, int32_t dtype, const void* u, const void* v,
                           int64_t nbatch, const uint8_t* slice_masks, void* pi, double* energy, void* stream);
 
+/* cgef_filter_device without any device allocation.  No counterpart in the reference.
+ * For callers that cannot let a library allocate device memory during a call: a host whose device
+ * memory is owned by its own pool allocator (a Julia or PyTorch caching allocator, which a library
+ * cudaMalloc would bypass and which can leave no memory for it), or a loop with a fixed memory
+ * budget.  The scratch is one 64 MiB array compiled into the library, which every GPU that loads
+ * the library holds until the process exits; a grid and batch needing more is rejected with
+ * CGEF_EINVAL.  The first call on each device resolves the array's device address (with that
+ * device current); make that first call before any stream capture.  All calls share the array and
+ * it keeps the last call's contents, so calls that overlap on the GPU race: serialise them.
+ * Same arguments and results as cgef_filter_device. */
+int32_t cgef_filter_device_noalloc(cgef_plan* plan, int32_t dtype, const void* field, void* out, int64_t nbatch,
+                                   void* stream);
+
 /* Tracing (no counterpart in the reference, which has none).  Kernel launches made by this
  * thread's calls since the last reset. */
 int64_t cgef_launch_count(void);
