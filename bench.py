@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--workload", default="sphere1", choices=["sphere1", "sweep24x8", "cart256", "levels40"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--snapshots", type=int, default=1, help="snapshots per step of the sphere1 workload")
     return ap.parse_args()
 
 
@@ -52,16 +53,18 @@ def sweep_scales():
     return [50e3 * 40.0 ** (s / 23.0) for s in range(24)]
 
 
-def make_workload(name: str, rank: int):
+def make_workload(name: str, rank: int, snapshots: int = 1):
     """Returns dict(grid, u, v, scales, slice_masks, kernel, nslices, desc)."""
     import cgef_b200 as cg
     from cgef_b200 import synthetic as S
     if name == "sphere1":
         g = S.sphere_grid()
         g = g.with_mask(S.land_mask(g, seed=1))
-        u, v = S.sphere_fields(g, seed=100 + rank)
-        return dict(grid=g, u=u[None], v=v[None], scales=[1e5], slice_masks=None, kernel=cg.GaussianKernel(4.0),
-                    desc="sphere-0.25deg-1440x720-gauss-a4-l100km-zerofill-30pct-land",
+        us, vs = zip(*[S.sphere_fields(g, seed=100 + snapshots * rank + t) for t in range(snapshots)])
+        return dict(grid=g, u=np.stack(us), v=np.stack(vs), scales=[1e5], slice_masks=None,
+                    kernel=cg.GaussianKernel(4.0),
+                    desc="sphere-0.25deg-1440x720-gauss-a4-l100km-zerofill-30pct-land"
+                         + ("" if snapshots == 1 else f"-x{snapshots}snapshots"),
                     dtype="f64")
     if name == "sweep24x8":
         g = S.sphere_grid()
@@ -234,7 +237,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        wl = make_workload(args.workload, 0)
+        wl = make_workload(args.workload, 0, args.snapshots)
         steps = args.steps if args.steps is not None else 3
         rate, nth, done, el, sample = oracle_rate(wl, budget_s=150.0, max_steps=steps, warmup=min(args.warmup, 1))
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
@@ -259,7 +262,7 @@ def main():
     import cgef_b200 as cg
     from cgef_b200 import _lib
 
-    wl = make_workload(args.workload, rank)
+    wl = make_workload(args.workload, rank, args.snapshots)
     g = wl["grid"]
     nsl = int(wl["u"].shape[0])
     ns = len(wl["scales"])

@@ -53,17 +53,19 @@ def build_peak_probe(force: bool = False) -> str:
     return PEAK_LIB_PATH
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB_PATH
+def build(verbose: bool = False, force: bool = False, out: str = LIB_PATH, defines=()) -> str:
+    """Compiles the library to `out` (default: in place); `defines` are extra -D tuning macros."""
+    if not force and out == LIB_PATH and not needs_build():
+        return out
     cmd = [
         _nvcc(), "-O3", "-std=c++17",
         "-gencode", "arch=compute_100a,code=sm_100a",
         "-lineinfo", "--fmad=false",
         "-Xcompiler", "-fPIC", "-shared",
         "-I", INCLUDE, "-I", CSRC,
+        *[f"-D{d}" for d in defines],
         *[os.path.join(CSRC, s) for s in SOURCES],
-        "-o", LIB_PATH + ".tmp",
+        "-o", out + ".tmp",
     ]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
@@ -76,8 +78,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
         raise RuntimeError("nvcc failed building libcgef_b200.so")
     if verbose:
         sys.stderr.write(r.stderr)
-    os.replace(LIB_PATH + ".tmp", LIB_PATH)
-    return LIB_PATH
+    os.replace(out + ".tmp", out)
+    return out
 
 
 if __name__ == "__main__":

@@ -103,7 +103,7 @@ using namespace cgef;
 namespace {
 
 constexpr int kSlotPlanes = 0, kSlotGather = 1, kSlotPartials = 2, kSlotIn = 3, kSlotOut = 4, kSlotAux = 5,
-              kSlotMask = 6;
+              kSlotMask = 6, kSlotSplit = 8;
 
 size_t dsize(int dtype) { return dtype == CGEF_F32 ? sizeof(float) : sizeof(double); }
 
@@ -130,7 +130,7 @@ struct DeviceGuard {
 };
 
 int pitch_for(const cgef_plan* p, int halo) {
-  const int wide = 32 * kWarps;
+  const int wide = kTileCols;
   int nxr = ((p->nx + wide - 1) / wide) * wide;
   int pitch = halo + nxr + halo + 32;
   return ((pitch + 31) / 32) * 32;
@@ -148,8 +148,16 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
   go.slice_stride = 5 * N;
   const int mode = mode_for(p);
   (void)halo;
-  if (p->engine == CGEF_ENGINE_BANDED)
-    return launch_banded(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, go, st);
+  if (p->engine == CGEF_ENGINE_BANDED) {
+    const int na = (mode == kModePiSphere ? 9 : 5) + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
+    void* part = nullptr;
+    const size_t pb = banded_partials_bytes(p, na, nbatch);
+    if (pb > 0) {
+      int rc = ensure_ws(p, kSlotSplit, pb, &part);
+      if (rc) return rc;
+    }
+    return launch_banded(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st);
+  }
   if (p->engine == CGEF_ENGINE_SEPARABLE) {
     const int na = 5 + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
     void* rb = nullptr;
@@ -262,7 +270,12 @@ int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int
   for (int m = 0; m < nf; ++m) go.o[m] = outs[m];
   go.slice_stride = ostride;
   double* pl = static_cast<double*>(planes);
-  if (p->engine == CGEF_ENGINE_BANDED) return launch_banded(p, kModeFields, nf, pl, pitch, np, nbatch, mask, mstride, go, st);
+  if (p->engine == CGEF_ENGINE_BANDED) {
+    void* part = nullptr;
+    const size_t pb = banded_partials_bytes(p, nf + (def ? 1 : 0), nbatch);
+    if (pb > 0 && (rc = ensure_ws(p, kSlotSplit, pb, &part))) return rc;
+    return launch_banded(p, kModeFields, nf, pl, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st);
+  }
   if (p->engine == CGEF_ENGINE_SEPARABLE) {
     void* rb = nullptr;
     if ((rc = ensure_ws(p, kSlotAux, sizeof(double) * (nf + 1) * N * nbatch, &rb))) return rc;
@@ -491,8 +504,8 @@ int32_t cgef_plan_destroy(cgef_plan* p) {
   if (p->device >= 0) {
     DeviceGuard dg(p->device);
     void* ptrs[] = {p->d_mask, p->d_x, p->d_sinlam, p->d_coslam, p->d_sinphi, p->d_cosphi, p->d_area, p->d_xscale,
-                    p->d_tanfac, p->d_rows, p->d_w, p->d_den_zf, p->d_items, p->d_gx, p->d_gy, p->d_px, p->d_py,
-                    p->d_xe, p->d_prefix_wx, p->d_prows};
+                    p->d_tanfac, p->d_rows, p->d_w, p->d_den_zf, p->d_items, p->d_groups, p->d_gx, p->d_gy, p->d_px,
+                    p->d_py, p->d_xe, p->d_prefix_wx, p->d_prows};
     for (void* q : ptrs)
       if (q) cudaFree(q);
     for (auto& b : p->ws)

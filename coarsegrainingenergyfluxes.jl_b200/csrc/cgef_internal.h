@@ -16,12 +16,18 @@ constexpr double kNormEps = 1e-15;
 // Kernels.jl:307: relative weight at which a Gaussian footprint is truncated.
 constexpr double kGaussianTruncationTol = 1e-10;
 
-// Number of source columns whose weights one CTA stages in shared memory at a time.
-constexpr int kChunk = 512;
+#ifndef CGEF_ROWS
+#define CGEF_ROWS 4
+#endif
+#ifndef CGEF_WARPS
+#define CGEF_WARPS 4
+#endif
 // Target rows carried by one thread of the banded gather (register tile height).
-constexpr int kRows = 4;
-// Warps per CTA of the banded gather.
-constexpr int kWarps = 5;
+constexpr int kRows = CGEF_ROWS;
+// Warps per CTA of the banded gather; every warp works on its own item.
+constexpr int kWarps = CGEF_WARPS;
+// Width of the staged planes' column tiling (the pitch is padded to a multiple of this).
+constexpr int kTileCols = 160;
 
 // One (target band j, source row offset dj) of the banded footprint: weights for longitude
 // offsets di in [-a, hi] live at w[woff + |di|] (the sphere's weight is even in di).  a < 0
@@ -34,14 +40,26 @@ struct BandRow {
   int32_t pad;
 };
 
-// A CTA's work item of the banded gather: target columns [x0, x0 + width) and rows
-// [j0, j0 + kRows); split = 1 when the CTA's warps share 32 columns and divide the source
-// columns between them (the heavy polar bands).
+// A warp's work item of the banded gather: 32 target columns from x0, kRows target rows from
+// j0, and the source rows [jr0, jr1) (raw, possibly outside the grid on a periodic axis).  slot
+// is -1 when the item covers every source row and finishes the targets itself; otherwise the
+// item writes its partial sums to partial slot `slot` and a combine pass adds the slots of the
+// group in order (the heavy polar bands are split this way).
 struct WorkItem {
   int32_t x0;
   int32_t j0;
-  int32_t split;
+  int32_t jr0;
+  int32_t jr1;
+  int32_t slot;
   int32_t cost;
+};
+
+// A split target tile: its partial slots are [slot0, slot0 + nslots).
+struct SplitGroup {
+  int32_t x0;
+  int32_t j0;
+  int32_t slot0;
+  int32_t nslots;
 };
 
 // Per (target row j, source row slot b) of the prefix-sum top-hat sweep (Filtering.jl:974-1097).
@@ -101,6 +119,9 @@ struct cgef_plan {
   int den_zf_2d = 0;
   std::vector<cgef::WorkItem> h_items;
   cgef::WorkItem* d_items = nullptr;
+  std::vector<cgef::SplitGroup> h_groups;
+  cgef::SplitGroup* d_groups = nullptr;
+  int nslots = 0;
   // separable engine
   int di_lim = 0, sep_dj_lim = 0;
   double* d_gx = nullptr;
@@ -115,7 +136,7 @@ struct cgef_plan {
   cgef::PrefixRow* d_prows = nullptr;  // ny * nb
   // execution
   cudaStream_t stream = nullptr;
-  cgef::DeviceBuffer ws[8];  // workspace slots, grown on demand
+  cgef::DeviceBuffer ws[10];  // workspace slots, grown on demand
 };
 
 namespace cgef {
@@ -164,8 +185,17 @@ struct GatherOut {
   int64_t slice_stride;
 };
 
+// `partials` holds banded_partials_bytes() of scratch for the split tiles (may be null when the
+// plan has none).
 int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
-                  const uint8_t* mask, int64_t mask_slice_stride, const GatherOut& out, cudaStream_t st);
+                  const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
+                  cudaStream_t st);
+
+// Bytes of partial-sum scratch a banded launch of `na` accumulated quantities over `nbatch`
+// slices needs.
+inline size_t banded_partials_bytes(const cgef_plan* p, int na, int nbatch) {
+  return sizeof(double) * static_cast<size_t>(p->nslots) * nbatch * kRows * na * 32;
+}
 
 int launch_separable(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                      const uint8_t* mask, int64_t mask_slice_stride, double* rowbuf, const GatherOut& out,

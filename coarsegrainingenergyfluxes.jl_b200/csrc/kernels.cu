@@ -19,9 +19,20 @@
 
 #include "cgef_internal.h"
 
+#ifndef CGEF_BANDED_MINB
+#define CGEF_BANDED_MINB 4
+#endif
+#ifndef CGEF_BANDED_UNROLL
+#define CGEF_BANDED_UNROLL 2
+#endif
+
 namespace cgef {
 
 namespace {
+
+// Resident CTAs per SM the banded gather is compiled for, and the unroll of its inner loop.
+constexpr int kBandedMinBlocks = CGEF_BANDED_MINB;
+constexpr int kBandedUnroll = CGEF_BANDED_UNROLL;
 
 __device__ __forceinline__ int wrap(int a, int n) {
   int r = a % n;
@@ -122,7 +133,11 @@ struct BandedK {
   const double* w;
   int D;
   const WorkItem* items;
+  int nitems;
   int nslices;
+  const SplitGroup* groups;
+  int ngroups;
+  double* partials;
   const double* den_zf;
   int den_zf_2d;
   const uint8_t* mask;
@@ -211,20 +226,48 @@ __device__ __forceinline__ void write_outputs(double* const (&out)[9], int64_t o
   out[4][o] = n0 * tn0 + n1 * tn1 + n2 * tn2;
 }
 
+// Finishes one target (row t of a tile) from its accumulated sums: normalise, then write the
+// mode's outputs.
 template <int MODE, int NF, bool DEF>
-__global__ void __launch_bounds__(32 * kWarps, 2) banded_kernel(BandedK a) {
+__device__ __forceinline__ void finish_target(const BandedK& a, const double (&acc)[Cfg<MODE, NF, DEF>::NA], int slice,
+                                              int j, int col) {
   using C = Cfg<MODE, NF, DEF>;
-  extern __shared__ double smem[];  // [kRows][kChunk] weights; reused by the split reduction
-  __shared__ int s_a[kRows], s_hi[kRows], s_off[kRows];
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const int warp = tid >> 5;
-  const int nw = blockDim.x >> 5;
-  const int item_id = blockIdx.x / a.nslices;
-  const int slice = blockIdx.x - item_id * a.nslices;
+  const int64_t pix = static_cast<int64_t>(j) * a.nx + col;
+  const bool act = a.mask == nullptr || a.mask[slice * a.mask_stride + pix] != 0;
+  double den;
+  if (DEF)
+    den = acc[C::NA - 1];
+  else
+    den = a.den_zf_2d ? a.den_zf[pix] : a.den_zf[j];
+  const bool zero = !act || !(den > kNormEps);
+  double F[C::NA0];
+#pragma unroll
+  for (int m = 0; m < C::NA0; ++m) F[m] = zero ? 0.0 : acc[m] / den;
+  const double sl = a.sinlam ? a.sinlam[col] : 0.0;
+  const double cl = a.coslam ? a.coslam[col] : 0.0;
+  const double sp = a.sinphi ? a.sinphi[j] : 0.0;
+  const double cp = a.cosphi ? a.cosphi[j] : 0.0;
+  write_outputs<MODE, C::NA0>(a.out, slice * a.out_stride + pix, F, zero, sl, cl, sp, cp);
+}
+
+// One warp = one work item: 32 consecutive target columns (one per lane) x kRows target rows,
+// summed over the item's source rows.  For each source row the warp stages, 32 columns at a time,
+// the kRows rows' weights (zero outside each row's own interval) in its own shared-memory slab,
+// then every lane streams its three (or K) staged values along the row and applies the kRows
+// weights to all accumulated quantities with FP64 FMA.  Warps never wait for one another.
+template <int MODE, int NF, bool DEF>
+__global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(BandedK a) {
+  using C = Cfg<MODE, NF, DEF>;
+  __shared__ double wbuf[kWarps][kRows][32];
+  __shared__ int rint[kWarps][3][kRows];  // per warp: a, hi, woff of the kRows rows for the current source row
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int64_t gid = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
+  if (gid >= static_cast<int64_t>(a.nitems) * a.nslices) return;
+  const int item_id = static_cast<int>(gid / a.nslices);
+  const int slice = static_cast<int>(gid - static_cast<int64_t>(item_id) * a.nslices);
   const WorkItem it = a.items[item_id];
-  const bool split = it.split != 0;
-  const int col = it.x0 + (split ? lane : tid);
+  const int col = it.x0 + lane;
   const int j0 = it.j0;
 
   double acc[kRows][C::NA];
@@ -233,10 +276,7 @@ __global__ void __launch_bounds__(32 * kWarps, 2) banded_kernel(BandedK a) {
 #pragma unroll
     for (int m = 0; m < C::NA; ++m) acc[t][m] = 0.0;
 
-  const double* base = a.planes + slice * a.slice_stride + a.halo + col;
-
-  // Inactive targets output 0 (Filtering.jl:2561), so a warp whose targets are all masked skips
-  // the sums, and a CTA with none active only writes its zeros.
+  // Inactive targets output 0 (Filtering.jl:2561): a warp with no active target skips the sums.
   bool any_act = false;
   if (col < a.nx) {
 #pragma unroll
@@ -247,108 +287,117 @@ __global__ void __launch_bounds__(32 * kWarps, 2) banded_kernel(BandedK a) {
     }
   }
   const bool warp_act = __any_sync(0xffffffffu, any_act);
-  const bool cta_act = __syncthreads_or(any_act) != 0;
 
-  for (int jr = j0 - a.D; cta_act && jr <= j0 + kRows - 1 + a.D; ++jr) {
+  const double* base = a.planes + slice * a.slice_stride + a.halo + col;
+  double* wb = &wbuf[warp][0][0];
+  for (int jr = it.jr0; warp_act && jr < it.jr1; ++jr) {
     int jj = jr;
     if (jr < 0 || jr >= a.ny) {
       if (!a.periodic_y) continue;
       jj = wrap(jr, a.ny);
     }
-    __syncthreads();  // previous row's readers of s_a / smem are done
-    if (tid < kRows) {
-      const int j = j0 + tid;
+    // lanes 0..kRows-1 fetch the rows' intervals into the warp's slab
+    if (lane < kRows) {
+      int ra = -1, rhi = -1, roff = 0;
+      const int j = j0 + lane;
       const int dj = jr - j;
-      BandRow r{0, -1, -1, 0};
-      if (j < a.ny && dj >= -a.D && dj <= a.D) r = a.rows[static_cast<int64_t>(j) * a.band_stride + dj + a.D];
-      s_a[tid] = r.a;
-      s_hi[tid] = r.hi;
-      s_off[tid] = r.woff;
+      if (j < a.ny && dj >= -a.D && dj <= a.D) {
+        const BandRow r = a.rows[static_cast<int64_t>(j) * a.band_stride + dj + a.D];
+        ra = r.a;
+        rhi = r.hi;
+        roff = r.woff;
+      }
+      rint[warp][0][lane] = ra;
+      rint[warp][1][lane] = rhi;
+      rint[warp][2][lane] = roff;
     }
-    __syncthreads();
+    __syncwarp();
     int A = -1, HI = -1;
 #pragma unroll
     for (int t = 0; t < kRows; ++t) {
-      A = max(A, s_a[t]);
-      HI = max(HI, s_hi[t]);
+      A = max(A, rint[warp][0][t]);
+      HI = max(HI, rint[warp][1][t]);
     }
-    if (A < 0) continue;
+    if (A < 0) {
+      __syncwarp();
+      continue;
+    }
     const double* src = base + static_cast<int64_t>(jj) * a.pitch;
-    for (int c0 = -A; c0 <= HI; c0 += kChunk) {
-      const int cn = min(kChunk, HI - c0 + 1);
-      if (c0 != -A) __syncthreads();
-      for (int idx = tid; idx < kRows * cn; idx += blockDim.x) {
-        const int t = idx / cn;
-        const int k = idx - t * cn;
-        const int di = c0 + k;
-        const int at = s_a[t];
-        smem[t * kChunk + k] = (at >= 0 && di >= -at && di <= s_hi[t]) ? a.w[s_off[t] + abs(di)] : 0.0;
+    for (int c0 = -A; c0 <= HI; c0 += 32) {
+      const int k = c0 + lane;
+      double wv[kRows];
+#pragma unroll
+      for (int t = 0; t < kRows; ++t) {
+        const int at = rint[warp][0][t];
+        wv[t] = (at >= 0 && k >= -at && k <= rint[warp][1][t]) ? __ldg(a.w + rint[warp][2][t] + abs(k)) : 0.0;
       }
-      __syncthreads();
-      int kb = 0, ke = warp_act ? cn : 0;
-      if (split && warp_act) {
-        kb = (warp * cn) / nw;
-        ke = ((warp + 1) * cn) / nw;
-      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < kRows; ++t) wb[t * 32 + lane] = wv[t];
+      __syncwarp();
+      const int cn = min(32, HI - c0 + 1);
       const double* s = src + c0;
-#pragma unroll 2
-      for (int k = kb; k < ke; ++k) {
+#pragma unroll kBandedUnroll
+      for (int kk = 0; kk < cn; ++kk) {
         double v[C::NP];
 #pragma unroll
-        for (int pl = 0; pl < C::NP; ++pl) v[pl] = __ldg(s + pl * a.plane_stride + k);
+        for (int pl = 0; pl < C::NP; ++pl) v[pl] = __ldg(s + pl * a.plane_stride + kk);
         double q[C::NA];
         expand<MODE, NF, DEF>(v, q);
 #pragma unroll
         for (int t = 0; t < kRows; ++t) {
-          const double wt = smem[t * kChunk + k];
+          const double wt = wb[t * 32 + kk];
 #pragma unroll
           for (int m = 0; m < C::NA; ++m) acc[t][m] = fma(wt, q[m], acc[t][m]);
         }
       }
     }
+    __syncwarp();
   }
 
-  if (split && cta_act) {
-    // Deterministic cross-warp sum: warp 0 adds the partials of warps 0..nw-1 in order.
+  if (it.slot >= 0) {
+    // partial sums of a split tile: [slot][slice][t][m][lane]
+    double* pp = a.partials + ((static_cast<int64_t>(it.slot) * a.nslices + slice) * kRows * C::NA) * 32 + lane;
 #pragma unroll
-    for (int t = 0; t < kRows; ++t) {
-      __syncthreads();
+    for (int t = 0; t < kRows; ++t)
 #pragma unroll
-      for (int m = 0; m < C::NA; ++m) smem[(warp * C::NA + m) * 32 + lane] = acc[t][m];
-      __syncthreads();
-      if (warp == 0) {
-#pragma unroll
-        for (int m = 0; m < C::NA; ++m) {
-          double s = smem[m * 32 + lane];
-          for (int w2 = 1; w2 < nw; ++w2) s += smem[(w2 * C::NA + m) * 32 + lane];
-          acc[t][m] = s;
-        }
-      }
-    }
+      for (int m = 0; m < C::NA; ++m) pp[(t * C::NA + m) * 32] = acc[t][m];
+    return;
   }
-  if (split && warp != 0) return;
-
   if (col >= a.nx) return;
-  const double sl = a.sinlam ? a.sinlam[col] : 0.0;
-  const double cl = a.coslam ? a.coslam[col] : 0.0;
 #pragma unroll
   for (int t = 0; t < kRows; ++t) {
     const int j = j0 + t;
     if (j >= a.ny) break;
-    const int64_t pix = static_cast<int64_t>(j) * a.nx + col;
-    const bool act = a.mask == nullptr || a.mask[slice * a.mask_stride + pix] != 0;
-    double den;
-    if (DEF)
-      den = acc[t][C::NA - 1];
-    else
-      den = a.den_zf_2d ? a.den_zf[pix] : a.den_zf[j];
-    const bool zero = !act || !(den > kNormEps);
-    double F[C::NA0];
+    finish_target<MODE, NF, DEF>(a, acc[t], slice, j, col);
+  }
+}
+
+// Adds the partial slots of every split tile in slot order (deterministic) and finishes it.
+template <int MODE, int NF, bool DEF>
+__global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
+  using C = Cfg<MODE, NF, DEF>;
+  const int lane = threadIdx.x & 31;
+  const int64_t gid = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (gid >= static_cast<int64_t>(a.ngroups) * a.nslices) return;
+  const int gi = static_cast<int>(gid / a.nslices);
+  const int slice = static_cast<int>(gid - static_cast<int64_t>(gi) * a.nslices);
+  const SplitGroup g = a.groups[gi];
+  const int col = g.x0 + lane;
+  if (col >= a.nx) return;
+  double acc[C::NA];
+  for (int t = 0; t < kRows; ++t) {
+    const int j = g.j0 + t;
+    if (j >= a.ny) break;
 #pragma unroll
-    for (int m = 0; m < C::NA0; ++m) F[m] = zero ? 0.0 : acc[t][m] / den;
-    const double sp = a.sinphi ? a.sinphi[j] : 0.0;
-    const double cp = a.cosphi ? a.cosphi[j] : 0.0;
-    write_outputs<MODE, C::NA0>(a.out, slice * a.out_stride + pix, F, zero, sl, cl, sp, cp);
+    for (int m = 0; m < C::NA; ++m) acc[m] = 0.0;
+    for (int q = 0; q < g.nslots; ++q) {
+      const double* pp =
+          a.partials + ((static_cast<int64_t>(g.slot0 + q) * a.nslices + slice) * kRows * C::NA + t * C::NA) * 32 + lane;
+#pragma unroll
+      for (int m = 0; m < C::NA; ++m) acc[m] += pp[m * 32];
+    }
+    finish_target<MODE, NF, DEF>(a, acc, slice, j, col);
   }
 }
 
@@ -890,34 +939,31 @@ int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* plane
 namespace {
 
 template <int MODE, int NF, bool DEF>
-int run_banded(const cgef_plan* p, const BandedK& a, int nitems, int nbatch, cudaStream_t st) {
-  using C = Cfg<MODE, NF, DEF>;
-  const size_t smem_w = sizeof(double) * kRows * kChunk;
-  const size_t smem_r = sizeof(double) * kWarps * C::NA * 32;
-  const size_t smem = smem_w > smem_r ? smem_w : smem_r;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(banded_kernel<MODE, NF, DEF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(smem));
-    attr_set = true;
-  }
-  (void)p;
-  dim3 grid(static_cast<unsigned>(nitems) * nbatch), block(32 * kWarps);
+int run_banded(const BandedK& a, cudaStream_t st) {
+  const int64_t warps = static_cast<int64_t>(a.nitems) * a.nslices;
+  const unsigned blocks = static_cast<unsigned>((warps + kWarps - 1) / kWarps);
   prof_begin(CGEF_KERNEL_BANDED, st);
-  banded_kernel<MODE, NF, DEF><<<grid, block, smem, st>>>(a);
+  banded_kernel<MODE, NF, DEF><<<blocks, 32 * kWarps, 0, st>>>(a);
+  int rc = check_launch("banded_kernel");
+  if (rc == CGEF_OK && a.ngroups > 0) {
+    const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices;
+    banded_combine_kernel<MODE, NF, DEF><<<static_cast<unsigned>((cw + 3) / 4), 128, 0, st>>>(a);
+    rc = check_launch("banded_combine_kernel");
+  }
   prof_end(CGEF_KERNEL_BANDED, st);
-  return check_launch("banded_kernel");
+  return rc;
 }
 
 template <int MODE, int NF>
-int dispatch_banded(const cgef_plan* p, bool def, const BandedK& a, int nitems, int nbatch, cudaStream_t st) {
-  return def ? run_banded<MODE, NF, true>(p, a, nitems, nbatch, st) : run_banded<MODE, NF, false>(p, a, nitems, nbatch, st);
+int dispatch_banded(bool def, const BandedK& a, cudaStream_t st) {
+  return def ? run_banded<MODE, NF, true>(a, st) : run_banded<MODE, NF, false>(a, st);
 }
 
 }  // namespace
 
 int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
-                  const uint8_t* mask, int64_t mask_slice_stride, const GatherOut& out, cudaStream_t st) {
+                  const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
+                  cudaStream_t st) {
   const bool def = p->strategy == CGEF_DEFORMABLE;
   BandedK a{};
   a.planes = planes;
@@ -930,7 +976,12 @@ int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, in
   a.w = p->d_w;
   a.D = p->D;
   a.items = p->d_items;
+  a.nitems = static_cast<int>(p->h_items.size());
   a.nslices = nbatch;
+  a.groups = p->d_groups;
+  a.ngroups = static_cast<int>(p->h_groups.size());
+  a.partials = partials;
+  if (a.ngroups > 0 && partials == nullptr) return fail(CGEF_EINVAL, "banded: split tiles need a partials buffer");
   a.den_zf = p->d_den_zf;
   a.den_zf_2d = p->den_zf_2d;
   a.mask = mask;
@@ -945,14 +996,13 @@ int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, in
   a.cosphi = sph ? p->d_cosphi : nullptr;
   for (int m = 0; m < 9; ++m) a.out[m] = out.o[m];
   a.out_stride = out.slice_stride;
-  const int nitems = static_cast<int>(p->h_items.size());
-  if (mode == kModePiSphere) return dispatch_banded<kModePiSphere, 1>(p, def, a, nitems, nbatch, st);
-  if (mode == kModePiCart) return dispatch_banded<kModePiCart, 1>(p, def, a, nitems, nbatch, st);
+  if (mode == kModePiSphere) return dispatch_banded<kModePiSphere, 1>(def, a, st);
+  if (mode == kModePiCart) return dispatch_banded<kModePiCart, 1>(def, a, st);
   switch (nf) {
-    case 1: return dispatch_banded<kModeFields, 1>(p, def, a, nitems, nbatch, st);
-    case 2: return dispatch_banded<kModeFields, 2>(p, def, a, nitems, nbatch, st);
-    case 3: return dispatch_banded<kModeFields, 3>(p, def, a, nitems, nbatch, st);
-    case 4: return dispatch_banded<kModeFields, 4>(p, def, a, nitems, nbatch, st);
+    case 1: return dispatch_banded<kModeFields, 1>(def, a, st);
+    case 2: return dispatch_banded<kModeFields, 2>(def, a, st);
+    case 3: return dispatch_banded<kModeFields, 3>(def, a, st);
+    case 4: return dispatch_banded<kModeFields, 4>(def, a, st);
     default: return fail(CGEF_EINVAL, "banded: 1..4 fields per pass");
   }
 }

@@ -56,7 +56,7 @@ extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const
   const int64_t N = static_cast<int64_t>(p->nx) * p->ny;
   const bool def = p->strategy == CGEF_DEFORMABLE;
   const int np = 1 + (def ? 1 : 0);
-  const int wide = 32 * kWarps;
+  const int wide = kTileCols;
   const int nxr = ((p->nx + wide - 1) / wide) * wide;
   const int pitch = ((p->H + nxr + p->H + 32 + 31) / 32) * 32;
 
@@ -67,6 +67,7 @@ extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const
   if (p->engine == CGEF_ENGINE_SEPARABLE) engine_b = round256(sizeof(double) * 2 * static_cast<size_t>(N) * nbatch);
   if (p->engine == CGEF_ENGINE_PREFIXSUM)
     engine_b = round256(sizeof(double) * 2 * static_cast<size_t>(p->ny) * (p->pre_ne + 1) * nbatch);
+  if (p->engine == CGEF_ENGINE_BANDED) engine_b = round256(banded_partials_bytes(p, np, nbatch));
   const size_t result_b = dtype == CGEF_F64 ? 0 : round256(sizeof(double) * static_cast<size_t>(N) * nbatch);
   const size_t need = planes_b + engine_b + result_b;
   if (need > kNoallocScratchBytes)
@@ -100,7 +101,7 @@ extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const
     go.slice_stride = N;
     if (rc == CGEF_OK) {
       if (p->engine == CGEF_ENGINE_BANDED)
-        rc = launch_banded(p, kModeFields, 1, planes, pitch, np, nbatch, p->d_mask, 0, go, st);
+        rc = launch_banded(p, kModeFields, 1, planes, pitch, np, nbatch, p->d_mask, 0, engine_b ? aux : nullptr, go, st);
       else if (p->engine == CGEF_ENGINE_SEPARABLE)
         rc = launch_separable(p, kModeFields, 1, planes, pitch, np, nbatch, p->d_mask, 0, aux, go, st);
       else

@@ -284,56 +284,84 @@ int build_plan_tables(cgef_plan* p) {
       }
     }
     (void)W;
-    // Work items: kRows target rows x (32 * kWarps) columns, or 32 columns with the warps
-    // dividing the source columns where a band is heavy; longest first.
-    const int wide = 32 * kWarps;
-    std::vector<WorkItem> items;
-    std::vector<double> rowcost;  // per row group: sum over source rows of the union width
+    // Work items: one warp per (32 columns x kRows rows) tile; a tile whose source rows cost more
+    // than a fair share is split along the source rows into partial items, longest first.
     const int ngroups = (ny + kRows - 1) / kRows;
-    rowcost.assign(ngroups, 0.0);
+    const int ntx = (nx + 31) / 32;
+    std::vector<std::vector<double>> rowcost(ngroups);  // per group, per source row: union width
+    double total = 0.0;
     for (int g = 0; g < ngroups; ++g) {
       int j0 = g * kRows;
-      double c = 0.0;
       for (int jr = j0 - B.D; jr <= j0 + kRows - 1 + B.D; ++jr) {
-        if (!p->periodic_y && (jr < 0 || jr >= ny)) continue;
-        int A = -1;
-        for (int t = 0; t < kRows; ++t) {
-          int j = j0 + t;
-          if (j >= ny) continue;
-          int dj = jr - j;
-          if (dj < -B.D || dj > B.D) continue;
-          const BandRow& r = B.rows[(sphere ? static_cast<size_t>(j) * W : 0) + (dj + B.D)];
-          A = std::max(A, r.a);
+        double c = 0.0;
+        if (p->periodic_y || (jr >= 0 && jr < ny)) {
+          int A = -1, HI = -1;
+          for (int t = 0; t < kRows; ++t) {
+            int j = j0 + t;
+            if (j >= ny) continue;
+            int dj = jr - j;
+            if (dj < -B.D || dj > B.D) continue;
+            const BandRow& r = B.rows[(sphere ? static_cast<size_t>(j) * W : 0) + (dj + B.D)];
+            A = std::max(A, r.a);
+            HI = std::max(HI, r.hi);
+          }
+          if (A >= 0) c = static_cast<double>(HI + A + 1) + 4.0;  // + per-row overhead
         }
-        if (A >= 0) c += 2.0 * A + 1.0;
+        rowcost[g].push_back(c);
+        total += c * ntx;
       }
-      rowcost[g] = c;
     }
-    const int ntx_wide = (nx + wide - 1) / wide;
-    double total = 0.0;
-    for (int g = 0; g < ngroups; ++g) total += rowcost[g] * ntx_wide * wide;
     int sms = 148;
     {
       int dev = 0;
       cudaDeviceProp prop;
-      if (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
+      if (p->device >= 0 && cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
         sms = prop.multiProcessorCount;
       else
         cudaGetLastError();
     }
-    const double heavy = total / sms / 6.0;
+    const double target = std::max(64.0, total / (sms * 16.0 * 4.0));
+    std::vector<WorkItem> items;
+    std::vector<SplitGroup> groups;
+    int slots = 0;
     for (int g = 0; g < ngroups; ++g) {
-      int j0 = g * kRows;
-      bool split = rowcost[g] * wide > heavy;
-      if (split) {
-        for (int x = 0; x < nx; x += 32)
-          items.push_back(WorkItem{x, j0, 1, static_cast<int32_t>(std::min(rowcost[g] * 32.0, 2e9))});
-      } else {
-        for (int x = 0; x < nx; x += wide)
-          items.push_back(WorkItem{x, j0, 0, static_cast<int32_t>(std::min(rowcost[g] * wide / kWarps, 2e9))});
+      const int j0 = g * kRows;
+      const int jlo = j0 - B.D;
+      double cg = 0.0;
+      for (double c : rowcost[g]) cg += c;
+      if (cg <= 0.0) {
+        for (int x = 0; x < nx; x += 32) items.push_back(WorkItem{x, j0, jlo, jlo, -1, 0});
+        continue;
+      }
+      const int nsplit = std::max(1, std::min(static_cast<int>(rowcost[g].size()), static_cast<int>(std::ceil(cg / target))));
+      // contiguous source-row parts of about equal cost
+      std::vector<int> cut{0};
+      double acc = 0.0;
+      for (int r = 0; r < static_cast<int>(rowcost[g].size()); ++r) {
+        acc += rowcost[g][r];
+        if (static_cast<int>(cut.size()) < nsplit && acc >= cg * cut.size() / nsplit && r + 1 < static_cast<int>(rowcost[g].size()))
+          cut.push_back(r + 1);
+      }
+      cut.push_back(static_cast<int>(rowcost[g].size()));
+      const int parts = static_cast<int>(cut.size()) - 1;
+      for (int x = 0; x < nx; x += 32) {
+        if (parts == 1) {
+          items.push_back(WorkItem{x, j0, jlo, jlo + cut[1], -1, static_cast<int32_t>(std::min(cg, 2e9))});
+          continue;
+        }
+        groups.push_back(SplitGroup{x, j0, slots, parts});
+        for (int q = 0; q < parts; ++q) {
+          double c = 0.0;
+          for (int r = cut[q]; r < cut[q + 1]; ++r) c += rowcost[g][r];
+          items.push_back(WorkItem{x, j0, jlo + cut[q], jlo + cut[q + 1], slots + q, static_cast<int32_t>(std::min(c, 2e9))});
+        }
+        slots += parts;
       }
     }
+    (void)ntx;
     std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
+    p->h_groups = groups;
+    p->nslots = slots;
     p->h_items = items;
     p->H = std::max(B.Amax, 1);
     int rc;
@@ -342,6 +370,7 @@ int build_plan_tables(cgef_plan* p) {
     if ((rc = upload(p, &p->d_w, B.w.data(), B.w.size())) != CGEF_OK) return rc;
     if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
     if ((rc = upload(p, &p->d_items, items.data(), items.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_groups, groups.data(), groups.size())) != CGEF_OK) return rc;
   } else if (p->engine == CGEF_ENGINE_SEPARABLE) {
     // Filtering.jl:1391-1463: square truncation, lim = ceil(rad / step), point-sampled profile.
     p->di_lim = p->dx > 0 ? static_cast<int>(std::ceil(p->rad / p->dx)) : 0;
