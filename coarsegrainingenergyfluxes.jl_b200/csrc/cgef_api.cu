@@ -531,11 +531,18 @@ int32_t cgef_plan_get_info(const cgef_plan* p, cgef_plan_info* info) {
 int32_t cgef_plan_get_footprint(const cgef_plan* p, int32_t* di, int32_t* dj, double* w, int64_t* ptr) {
   if (!p) return fail(CGEF_EINVAL, "plan is NULL");
   if (p->engine != CGEF_ENGINE_BANDED) return fail(CGEF_EINVAL, "plan has no banded footprint");
-  const size_t n = p->h_di.size();
-  if (di) std::memcpy(di, p->h_di.data(), n * sizeof(int32_t));
-  if (dj) std::memcpy(dj, p->h_dj.data(), n * sizeof(int32_t));
-  if (w) std::memcpy(w, p->h_w.data(), n * sizeof(double));
   if (ptr) std::memcpy(ptr, p->h_ptr.data(), p->h_ptr.size() * sizeof(int64_t));
+  if (di || dj || w) {
+    const int nb = static_cast<int>(p->h_ptr.size()) - 1;
+    int64_t k = 0;
+    for (int b = 0; b < nb; ++b)
+      for_each_entry(p, b, [&](int ddi, int ddj, double wv) {
+        if (di) di[k] = ddi;
+        if (dj) dj[k] = ddj;
+        if (w) w[k] = wv;
+        ++k;
+      });
+  }
   return CGEF_OK;
 }
 

@@ -94,9 +94,9 @@ struct cgef_plan {
   double alpha = 0, scale = 0, rad = 0;
   // host tables kept for introspection
   std::vector<double> h_x, h_y;
-  std::vector<int32_t> h_di, h_dj;
-  std::vector<double> h_w;
-  std::vector<int64_t> h_ptr;
+  std::vector<cgef::BandRow> h_rows;  // banded: per (band, row offset) intervals
+  std::vector<double> h_whalf;        // banded: weights by |di|
+  std::vector<int64_t> h_ptr;         // banded: CSR band offsets of the reference's layout
   int64_t nentries = 0;
   int dj_lim = 0, di_max = 0;
   // device geometry tables
@@ -150,6 +150,21 @@ double kernel_radius(int kernel, double alpha, double ell);
 
 // Host plan construction (plan_build.cpp).
 int build_plan_tables(cgef_plan* p);
+
+// Visits band b's footprint entries in the reference's CSR order (row offset ascending, then
+// column offset ascending): f(ddi, ddj, w).
+template <typename F>
+void for_each_entry(const cgef_plan* p, int b, F f) {
+  const int W = 2 * p->D + 1;
+  for (int r = 0; r < W; ++r) {
+    const BandRow& br = p->h_rows[static_cast<size_t>(b) * W + r];
+    if (br.a < 0) continue;
+    for (int di = -br.a; di <= br.hi; ++di) {
+      const double w = p->h_whalf[br.woff + (di < 0 ? -di : di)];
+      if (w != 0.0) f(di, r - p->D, w);
+    }
+  }
+}
 
 // Workspace slot of at least `bytes` bytes.
 int ensure_ws(cgef_plan* p, int slot, size_t bytes, void** out);

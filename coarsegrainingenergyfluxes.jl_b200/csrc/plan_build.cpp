@@ -4,9 +4,11 @@
 // haversine form (Filtering.jl:264-265), cell measure R^2 cos(phi) dlambda dphi
 // (docs/src/theory.md:307), kernel weights and radii of Kernels.jl:318-379.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 #include "cgef_internal.h"
 
@@ -65,6 +67,24 @@ double metric_band(int geometry, double R, double y_t, double y_s, double rad) {
   return std::acos(c);
 }
 
+// Runs body(i) for i in [0, n) on the host's cores (results must not depend on the order).
+template <typename F>
+void parallel_for(int n, F body) {
+  unsigned hw = std::thread::hardware_concurrency();
+  int nt = static_cast<int>(std::min<unsigned>(hw == 0 ? 1 : hw, 32));
+  if (nt <= 1 || n < 64) {
+    for (int i = 0; i < n; ++i) body(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&]() {
+      for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1)) body(i);
+    });
+  for (auto& th : pool) th.join();
+}
+
 template <typename T>
 int upload(const cgef_plan* p, T** dst, const T* src, size_t n) {
   if (n == 0 || p->device < 0) {  // no device: host tables only
@@ -83,9 +103,7 @@ struct Banded {
   int Amax = 0;
   std::vector<BandRow> rows;  // ny * (2D+1) (sphere) or 2D+1 (Cartesian, one band)
   std::vector<double> w;      // half rows
-  std::vector<int32_t> di, dj;
-  std::vector<double> wcsr;
-  std::vector<int64_t> ptr;
+  std::vector<int64_t> ptr;   // CSR band offsets (entry counts of the reference's layout)
 };
 
 // Banded footprint (Filtering.jl:636-732).  Each (band, row offset) holds a contiguous
@@ -103,22 +121,13 @@ void build_banded(const cgef_plan* p, Banded& B) {
     B.D = dj_lim;
     B.rows.assign(2 * dj_lim + 1, BandRow{0, -1, -1, 0});
     B.ptr.push_back(0);
+    int64_t n = 0;
     for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
       int a = -1;
-      std::vector<double> half;
       for (int ddi = 0; ddi <= di_lim; ++ddi) {
         double x = ddi * p->dx, y = ddj * p->dy;
         double d = std::sqrt(x * x + y * y);
         if (d <= rad) a = ddi;
-      }
-      for (int ddi = -di_lim; ddi <= di_lim; ++ddi) {
-        double x = ddi * p->dx, y = ddj * p->dy;
-        double d = std::sqrt(x * x + y * y);
-        if (d <= rad) {
-          B.di.push_back(ddi);
-          B.dj.push_back(ddj);
-          B.wcsr.push_back(kernel_weight(p->kernel, p->alpha, d, p->scale) * A);
-        }
       }
       BandRow& r = B.rows[ddj + dj_lim];
       if (a >= 0) {
@@ -129,19 +138,30 @@ void build_banded(const cgef_plan* p, Banded& B) {
           double x = ddi * p->dx, y = ddj * p->dy;
           double d = std::sqrt(x * x + y * y);
           B.w.push_back(d <= rad ? kernel_weight(p->kernel, p->alpha, d, p->scale) * A : 0.0);
+          if (d <= rad) n += ddi == 0 ? 1 : 2;
         }
         B.Amax = std::max(B.Amax, a);
       }
     }
-    B.ptr.push_back(static_cast<int64_t>(B.di.size()));
+    B.ptr.push_back(n);
     return;
   }
   const int dj_lim = p->dy > 0 ? static_cast<int>(std::ceil(rad / (p->R * p->dy))) : 0;
   const int half = nx / 2;
   B.D = dj_lim;
   B.rows.assign(static_cast<size_t>(ny) * (2 * dj_lim + 1), BandRow{0, -1, -1, 0});
-  B.ptr.push_back(0);
-  for (int j = 0; j < ny; ++j) {
+  // every band is built independently (in parallel), then concatenated in band order
+  struct BandOut {
+    std::vector<double> whalf;
+    std::vector<int32_t> a, hi, off;  // per row offset, off relative to the band's whalf
+    int64_t n = 0;                    // entries (d <= rad) of the band
+  };
+  std::vector<BandOut> outs(ny);
+  parallel_for(ny, [&](int j) {
+    BandOut& o = outs[j];
+    o.a.assign(2 * dj_lim + 1, -1);
+    o.hi.assign(2 * dj_lim + 1, -1);
+    o.off.assign(2 * dj_lim + 1, 0);
     const double phi = coord(p->y0, p->dy, j);
     bool closed = false;
     for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
@@ -163,24 +183,39 @@ void build_banded(const cgef_plan* p, Banded& B) {
       for (int ddi = lo; ddi <= hi; ++ddi) {
         double d = sphere_distance(p->R, 0.0, phi, static_cast<double>(ddi) * p->dx, phi2);
         if (d <= rad) {
-          double wv = kernel_weight(p->kernel, p->alpha, d, p->scale) * A;
-          B.di.push_back(ddi);
-          B.dj.push_back(ddj);
-          B.wcsr.push_back(wv);
-          wabs[std::abs(ddi)] = wv;
+          wabs[std::abs(ddi)] = kernel_weight(p->kernel, p->alpha, d, p->scale) * A;
           amax = std::max(amax, std::abs(ddi));
+          ++o.n;
         }
       }
-      BandRow& r = B.rows[static_cast<size_t>(j) * (2 * dj_lim + 1) + (ddj + dj_lim)];
       if (amax >= 0) {
-        r.woff = static_cast<int32_t>(B.w.size());
-        r.a = amax;
-        r.hi = std::min(amax, hi);
-        for (int k = 0; k <= amax; ++k) B.w.push_back(wabs[k]);
-        B.Amax = std::max(B.Amax, amax);
+        const int r = ddj + dj_lim;
+        o.off[r] = static_cast<int32_t>(o.whalf.size());
+        o.a[r] = amax;
+        o.hi[r] = std::min(amax, hi);
+        for (int k = 0; k <= amax; ++k) o.whalf.push_back(wabs[k]);
       }
     }
-    B.ptr.push_back(static_cast<int64_t>(B.di.size()));
+  });
+  B.ptr.push_back(0);
+  int64_t total = 0;
+  for (int j = 0; j < ny; ++j) total += outs[j].n;
+  (void)total;
+  for (int j = 0; j < ny; ++j) {
+    BandOut& o = outs[j];
+    const int32_t base = static_cast<int32_t>(B.w.size());
+    for (int r = 0; r < 2 * dj_lim + 1; ++r) {
+      BandRow& br = B.rows[static_cast<size_t>(j) * (2 * dj_lim + 1) + r];
+      if (o.a[r] >= 0) {
+        br.woff = base + o.off[r];
+        br.a = o.a[r];
+        br.hi = o.hi[r];
+        B.Amax = std::max(B.Amax, o.a[r]);
+      }
+    }
+    B.w.insert(B.w.end(), o.whalf.begin(), o.whalf.end());
+    B.ptr.push_back(B.ptr.back() + o.n);
+    std::vector<double>().swap(o.whalf);
   }
 }
 
@@ -232,56 +267,52 @@ int build_plan_tables(cgef_plan* p) {
     p->Amax = B.Amax;
     p->dj_lim = B.D;
     p->di_max = B.Amax;
-    p->h_di = B.di;
-    p->h_dj = B.dj;
-    p->h_w = B.wcsr;
+    p->h_rows = B.rows;
+    p->h_whalf = B.w;
     p->h_ptr = B.ptr;
-    p->nentries = static_cast<int64_t>(B.di.size());
-    const int nb = sphere ? ny : 1;
+    p->nentries = B.ptr.back();
     // ZeroFill denominator: the footprint mass over in-domain entries, in CSR order
     // (Filtering.jl:2574-2582 accumulate w for every in-domain entry).
     const int64_t W = 2 * B.D + 1;
-    (void)nb;
     if (p->periodic_x) {
       p->den_zf_2d = 0;
       den_zf.assign(ny, 0.0);
-      for (int j = 0; j < ny; ++j) {
-        int b = sphere ? j : 0;
+      parallel_for(ny, [&](int j) {
         double s = 0.0;
-        for (int64_t k = B.ptr[b]; k < B.ptr[b + 1]; ++k) {
-          int jj = j + B.dj[k];
-          if ((jj < 0 || jj >= ny) && !p->periodic_y) continue;
-          s += B.wcsr[k];
-        }
+        for_each_entry(p, sphere ? j : 0, [&](int, int ddj, double w) {
+          int jj = j + ddj;
+          if ((jj < 0 || jj >= ny) && !p->periodic_y) return;
+          s += w;
+        });
         den_zf[j] = s;
-      }
+      });
     } else {
       p->den_zf_2d = 1;
       den_zf.assign(static_cast<size_t>(ny) * nx, 0.0);
-      for (int j = 0; j < ny; ++j) {
-        int b = sphere ? j : 0;
+      parallel_for(ny, [&](int j) {
+        const int b = sphere ? j : 0;
         // interior columns see every entry; edge columns are summed entry by entry
         double full = 0.0;
-        for (int64_t k = B.ptr[b]; k < B.ptr[b + 1]; ++k) {
-          int jj = j + B.dj[k];
-          if ((jj < 0 || jj >= ny) && !p->periodic_y) continue;
-          full += B.wcsr[k];
-        }
+        for_each_entry(p, b, [&](int, int ddj, double w) {
+          int jj = j + ddj;
+          if ((jj < 0 || jj >= ny) && !p->periodic_y) return;
+          full += w;
+        });
         for (int i = 0; i < nx; ++i) {
           double s = full;
           if (i < B.Amax || i >= nx - B.Amax) {
             s = 0.0;
-            for (int64_t k = B.ptr[b]; k < B.ptr[b + 1]; ++k) {
-              int jj = j + B.dj[k];
-              if ((jj < 0 || jj >= ny) && !p->periodic_y) continue;
-              int ii = i + B.di[k];
-              if (ii < 0 || ii >= nx) continue;
-              s += B.wcsr[k];
-            }
+            for_each_entry(p, b, [&](int ddi, int ddj, double w) {
+              int jj = j + ddj;
+              if ((jj < 0 || jj >= ny) && !p->periodic_y) return;
+              int ii = i + ddi;
+              if (ii < 0 || ii >= nx) return;
+              s += w;
+            });
           }
           den_zf[static_cast<size_t>(j) * nx + i] = s;
         }
-      }
+      });
     }
     (void)W;
     // Work items: one warp per (32 columns x kRows rows) tile; a tile whose source rows cost more
