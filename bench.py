@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--snapshots", type=int, default=1, help="snapshots per step of the sphere1 workload")
+    ap.add_argument("--scale-km", type=float, default=None, help="filter scale of the sphere1 workload (km)")
     return ap.parse_args()
 
 
@@ -53,7 +54,7 @@ def sweep_scales():
     return [50e3 * 40.0 ** (s / 23.0) for s in range(24)]
 
 
-def make_workload(name: str, rank: int, snapshots: int = 1):
+def make_workload(name: str, rank: int, snapshots: int = 1, scale_km=None):
     """Returns dict(grid, u, v, scales, slice_masks, kernel, nslices, desc)."""
     import cgef_b200 as cg
     from cgef_b200 import synthetic as S
@@ -61,9 +62,10 @@ def make_workload(name: str, rank: int, snapshots: int = 1):
         g = S.sphere_grid()
         g = g.with_mask(S.land_mask(g, seed=1))
         us, vs = zip(*[S.sphere_fields(g, seed=100 + snapshots * rank + t) for t in range(snapshots)])
-        return dict(grid=g, u=np.stack(us), v=np.stack(vs), scales=[1e5], slice_masks=None,
+        ell = 1e5 if scale_km is None else 1e3 * scale_km
+        return dict(grid=g, u=np.stack(us), v=np.stack(vs), scales=[ell], slice_masks=None,
                     kernel=cg.GaussianKernel(4.0),
-                    desc="sphere-0.25deg-1440x720-gauss-a4-l100km-zerofill-30pct-land"
+                    desc=f"sphere-0.25deg-1440x720-gauss-a4-l{ell / 1e3:g}km-zerofill-30pct-land"
                          + ("" if snapshots == 1 else f"-x{snapshots}snapshots"),
                     dtype="f64")
     if name == "sweep24x8":
@@ -92,8 +94,7 @@ def algorithmic_flops(plans, grid, nslices, slice_masks) -> float:
     total = 0.0
     for p in plans:
         if p.engine == "banded":
-            _, _, _, ptr = p.footprint()
-            n = np.diff(ptr).astype(np.float64)
+            n = p.band_counts().astype(np.float64)
             if slice_masks is not None:
                 act = slice_masks.reshape(nslices, grid.ny, grid.nx).sum(axis=(0, 2)).astype(np.float64)
             else:
@@ -173,48 +174,79 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------------
 # CPU baseline / reference arm: the FP64 oracle's threaded path
 # ---------------------------------------------------------------------------------------------
-def oracle_rate(wl, budget_s: float, max_steps: int, warmup: int = 1):
+def oracle_rate(wl, budget_s: float):
+    """Rate of the oracle's OpenMP compute_Pi (the restated reference threaded path) on this host.
+
+    A unit is Pi for one (slice, scale).  With one unit it is repeated within the budget; otherwise
+    a bounded subset of units is timed and the whole workload's time is extrapolated linearly in
+    (active targets x footprint entries), the direct sum's cost."""
     import oracle as O
     g = wl["grid"]
     nthreads = O.max_threads()
     nsl = wl["u"].shape[0]
-    scales = wl["scales"]
-    n_units = g.nx * g.ny
-    # one unit of work = Pi for one (slice, scale); run units round-robin until the budget ends
-    units = [(t, s) for s in range(len(scales)) for t in range(nsl)]
+    scales = list(wl["scales"])
+    alpha = wl["kernel"].alpha
+    masks = wl["slice_masks"]
+
+    def ogrid(mask):
+        return O.Grid(O.SPHERE if g.is_spherical else O.CART, g.nx, g.ny, g.x.start, g.x.step, g.y.start, g.y.step,
+                      g.geometry.R if g.is_spherical else 6.371e6, g.periodic[0], g.periodic[1], mask)
+
+    def mask_of(t):
+        return masks[t] if masks is not None else g.mask
+
+    def active(t):
+        m = mask_of(t)
+        return float(g.nx * g.ny if m is None else np.count_nonzero(m))
+
+    entries = [float(O.count_entries(ogrid(None), O.GAUSSIAN, alpha, s)) for s in scales]
+    cost = lambda t, s: active(t) * entries[s]
+    # subset: scales spread over the range whose estimated time fits the budget
+    order = sorted(range(len(scales)), key=lambda s: entries[s])
     plans = {}
 
-    def plan_for(t, s):
-        key = (t if wl["slice_masks"] is not None else -1, s)
+    def run(t, s):
+        key = (t if masks is not None else -1, s)
         if key not in plans:
-            m = wl["slice_masks"][t] if wl["slice_masks"] is not None else g.mask
-            og = O.Grid(O.SPHERE if g.is_spherical else O.CART, g.nx, g.ny, g.x.start, g.x.step, g.y.start,
-                        g.y.step, g.geometry.R if g.is_spherical else 6.371e6, g.periodic[0], g.periodic[1], m)
-            plans[key] = O.Plan(og, O.GAUSSIAN, wl["kernel"].alpha, scales[s], O.ZEROFILL)
-        return plans[key]
-
-    def unit(k):
-        t, s = units[k % len(units)]
-        p = plan_for(t, s)
+            plans[key] = O.Plan(ogrid(mask_of(t)), O.GAUSSIAN, alpha, scales[s], O.ZEROFILL)
+        p = plans[key]
         u = np.asarray(wl["u"][t], dtype=np.float64)
         v = np.asarray(wl["v"][t], dtype=np.float64)
+        t0 = time.perf_counter()
         p.compute_pi(u, v, nthreads)
+        return time.perf_counter() - t0
 
-    # warm-up (also builds the plans), then timed units
-    for k in range(min(warmup, len(units))):
-        plan_for(*units[k])
-    for k in range(warmup):
-        unit(k)
-    done = 0
-    t0 = time.perf_counter()
-    while done < max_steps * len(units):
-        unit(done)
-        done += 1
-        if time.perf_counter() - t0 > budget_s:
-            break
-    el = time.perf_counter() - t0
-    sample = f"{done} x compute_Pi unit(s) of {g.nx}x{g.ny} ({'/'.join(str(int(x)) for x in scales[:1])} m ...)"
-    return n_units * done / el, nthreads, done, el, sample
+    run(0, order[0])  # warm-up
+    timed, spent, ccost = [], 0.0, 0.0
+    t0 = run(0, order[0])
+    timed.append((0, order[0]))
+    spent += t0
+    ccost += cost(0, order[0])
+    per_cost = t0 / cost(0, order[0])
+    picks = [order[len(order) * q // 4] for q in (1, 2, 3)] if len(order) > 1 else []
+    for s in picks:
+        est = per_cost * cost(0, s)
+        if spent + est > budget_s or s in [x[1] for x in timed]:
+            continue
+        dt = run(0, s)
+        timed.append((0, s))
+        spent += dt
+        ccost += cost(0, s)
+    if len(scales) == 1 and nsl == 1:
+        while spent < budget_s * 0.5:
+            spent += run(0, 0)
+            timed.append((0, 0))
+            ccost += cost(0, 0)
+    per_cost = spent / ccost
+    full = sum(cost(t, s) for t in range(nsl) for s in range(len(scales))) * per_cost
+    rate = g.nx * g.ny * nsl * len(scales) / full
+    if len(scales) == 1 and nsl == 1:
+        sample = f"{len(timed)} timed compute_Pi runs of the full {g.nx}x{g.ny} workload ({spent:.1f} s)"
+    else:
+        sample = (f"{len(timed)} timed (slice, scale) units, scales "
+                  f"{sorted({round(scales[s] / 1e3) for _, s in timed})} km of slice 0 ({spent:.1f} s), "
+                  f"extrapolated to all {nsl}x{len(scales)} units linearly in active targets x footprint entries")
+    return rate, nthreads, len(timed), spent, sample
 
 
 def cpu_model() -> str:
@@ -237,9 +269,8 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        wl = make_workload(args.workload, 0, args.snapshots)
-        steps = args.steps if args.steps is not None else 3
-        rate, nth, done, el, sample = oracle_rate(wl, budget_s=150.0, max_steps=steps, warmup=min(args.warmup, 1))
+        wl = make_workload(args.workload, 0, args.snapshots, args.scale_km)
+        rate, nth, done, el, sample = oracle_rate(wl, budget_s=120.0)
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -262,7 +293,7 @@ def main():
     import cgef_b200 as cg
     from cgef_b200 import _lib
 
-    wl = make_workload(args.workload, rank, args.snapshots)
+    wl = make_workload(args.workload, rank, args.snapshots, args.scale_km)
     g = wl["grid"]
     nsl = int(wl["u"].shape[0])
     ns = len(wl["scales"])
@@ -296,7 +327,7 @@ def main():
             step()
         torch.cuda.synchronize()
         per = (time.perf_counter() - t0) / 3
-        steps = int(max(10, min(5000, 5.0 / max(per, 1e-6))))
+        steps = int(max(3, min(5000, 5.0 / max(per, 1e-6))))
     for _ in range(max(args.warmup, 3)):
         flush.fill_(1.0)
         step()
@@ -360,7 +391,9 @@ def main():
             traffic = None
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if peak and peak > 0 else None, "traffic": traffic,
-                "kernel": f"banded_kernel (FP64 FMA footprint gather, {plans[0].engine})",
+                "kernel": {"banded": "banded_kernel + banded_combine_kernel (FP64 FMA footprint gather)",
+                           "separable": "sep_row_kernel + sep_col_kernel (FP64 separable passes)",
+                           "prefixsum": "prefix_scan_kernel + prefix_sweep_kernel"}[plans[0].engine],
                 "per_launch_ms": per_launch_ms, "launches": int(cnt.value),
                 "algorithmic_flops_per_launch": flops_launch,
                 "peak_source": "measured: DFMA loop over all SMs on this GPU (libcgef_peak.so), "
@@ -380,7 +413,8 @@ def main():
                                     None if hm is None else hm.data_ptr(), hPi.data_ptr(), hE.data_ptr()))
 
         host_step()
-        n_e2e = args.e2e_steps if args.e2e_steps is not None else max(3, min(steps, 200))
+        per_step_s = elapsed_ms / 1e3 / steps
+        n_e2e = args.e2e_steps if args.e2e_steps is not None else max(2, min(steps, 200, int(4.0 / per_step_s)))
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
@@ -399,9 +433,9 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, nth, done, el, sample = oracle_rate(wl, budget_s=20.0, max_steps=1, warmup=1)
+        rate, nth, done, el, sample = oracle_rate(wl, budget_s=20.0)
         cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
-               "sample": sample + f", {el:.1f} s; CPU {cpu_model()}; restated reference threaded path (FP64 oracle, OpenMP rows)"}
+               "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path (FP64 oracle, OpenMP rows)"}
 
     if dist is not None:
         dist.barrier()

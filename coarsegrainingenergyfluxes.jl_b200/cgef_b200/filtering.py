@@ -112,6 +112,13 @@ class PhysicalFilterPlan:
                                                        w.ctypes.data, ptr.ctypes.data))
         return di, dj, w, ptr
 
+    def band_counts(self) -> np.ndarray:
+        """Footprint entries per band (banded engine), without materialising the entries."""
+        nb = int(self.info.nbands)
+        ptr = np.zeros(nb + 1, np.int64)
+        _lib.check(_lib.load().cgef_plan_get_footprint(self.handle, None, None, None, ptr.ctypes.data))
+        return np.diff(ptr)
+
     def __repr__(self):
         return (f"PhysicalFilterPlan(engine={self.engine}, kernel={self.kernel!r}, scale={self.scale}, "
                 f"strategy={self.strategy!r})")

@@ -947,3 +947,39 @@ void orc_coords(const orc_plan* p, double* x, double* y) {
   for (int i = 0; i < p->g.nx; ++i) x[i] = gx_coord(&p->g, i);
   for (int j = 0; j < p->g.ny; ++j) y[j] = gy_coord(&p->g, j);
 }
+
+/* Entry count of the banded footprint (the counting pass of footprint_build, rows in parallel):
+ * the benchmark's cost model for extrapolating a timed subset of scales. */
+int64_t orc_count_entries(int geometry, int nx, int ny, double x0, double dx, double y0, double dy, double R,
+                          int periodic_x, int periodic_y, int kernel, double alpha, double ell) {
+  orc_grid g = {geometry, nx, ny, x0, dx, y0, dy, R, periodic_x, periodic_y, NULL};
+  if (geometry == ORC_CART) {
+    orc_footprint fp;
+    footprint_build(&g, kernel, alpha, ell, &fp, 0);
+    return fp.nentries;
+  }
+  double rad = orc_kernel_radius(kernel, alpha, ell);
+  int dj_lim = dy > 0 ? (int)ceil(rad / (R * dy)) : 0;
+  int half = nx / 2;
+  int64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total)
+  for (int j = 0; j < ny; ++j) {
+    double phi = gy_coord(&g, j);
+    int closed = 0;
+    for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
+      int jj = j + ddj;
+      if (jj < 0 || jj >= ny) continue;
+      if (sphere_row_window(&g, phi, gy_coord(&g, jj), rad, half) >= half) closed = 1;
+    }
+    for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
+      int jj = j + ddj;
+      if (jj < 0 || jj >= ny) continue;
+      double phi2 = gy_coord(&g, jj);
+      int win = closed ? half : sphere_row_window(&g, phi, phi2, rad, half);
+      int lo = -win, hi = (closed && 2 * half + 1 > nx) ? half - 1 : win;
+      for (int ddi = lo; ddi <= hi; ++ddi)
+        if (orc_distance(&g, 0.0, phi, (double)ddi * dx, phi2) <= rad) ++total;
+    }
+  }
+  return total;
+}

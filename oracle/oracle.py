@@ -70,6 +70,9 @@ def lib():
         L.orc_kernel_weight.restype = C.c_double
         L.orc_max_threads.restype = C.c_int
         L.orc_coords.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_count_entries.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                        C.c_double, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.orc_count_entries.restype = C.c_int64
         _ = dp
         _lib = L
     return _lib
@@ -219,6 +222,12 @@ def coarse_grain(grid: Grid, u, v, scales, kernel: int = GAUSSIAN, alpha: float 
     E = np.array(E)
     k = L / scales
     return {"Pi": np.stack(Pis), "cumulative_energy": E, "wavenumber": k, "filtering_spectrum": spectral_density(E, k)}
+
+
+def count_entries(grid: Grid, kernel: int, alpha: float, ell: float) -> int:
+    """Entries of the banded footprint (all bands), without building it."""
+    return int(lib().orc_count_entries(grid.geometry, grid.nx, grid.ny, grid.x0, grid.dx, grid.y0, grid.dy, grid.R,
+                                       int(grid.periodic_x), int(grid.periodic_y), kernel, alpha, ell))
 
 
 def max_threads() -> int:
