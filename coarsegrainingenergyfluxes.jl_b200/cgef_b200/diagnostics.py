@@ -49,6 +49,11 @@ class NoSpectrum(AbstractSpectrumPolicy):
 
 
 def gate_spectrum(kernel: AbstractFilterKernel, policy: AbstractSpectrumPolicy) -> bool:
+    """Throw (StrictSpectrum, non-monotone kernel) / warn and compute (ForceSpectrum) / skip
+    (NoSpectrum).  A policy that is not one of the three types is a TypeError, as the reference's
+    typed keyword makes `spectrum = false` or `spectrum = :force` (Diagnostics.jl:17-81)."""
+    if not isinstance(policy, AbstractSpectrumPolicy):
+        raise TypeError(f"spectrum must be StrictSpectrum(), ForceSpectrum() or NoSpectrum(), got {policy!r}")
     if isinstance(policy, StrictSpectrum):
         check_spectrum_kernel(kernel)
         return True
