@@ -32,8 +32,12 @@ EXPORTED = [
     "cgef_cumulative_energy", "cgef_sweep", "cgef_ddx", "cgef_ddy", "cgef_filter_device",
     "cgef_compute_pi_device", "cgef_sweep_device", "cgef_launch_count", "cgef_reset_launch_count",
     "cgef_profile_enable", "cgef_profile_read", "cgef_profile_reset", "cgef_filter_device_noalloc",
+    "cgef_closure_create", "cgef_closure_destroy", "cgef_closure_get_params", "cgef_closure_set_params",
+    "cgef_closure_pairs_device", "cgef_closure_train_device", "cgef_closure_forward_device",
+    "cgef_closure_grad_device", "cgef_closure_pi_device",
 ]
-KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN = 0, 1, 2, 3, 4
+KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE = 0, 1, 2, 3, 4, 5
+CLOSURE_NPARAM = 8899
 
 
 class GridDesc(C.Structure):
@@ -55,6 +59,16 @@ class PlanInfo(C.Structure):
 class PiOutputs(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in
                 ("pi", "ubar", "vbar", "tau_xx", "tau_xy", "tau_yy", "s_xx", "s_xy", "s_yy", "energy")]
+
+
+class AdamW(C.Structure):
+    _fields_ = [("lr", C.c_double), ("beta1", C.c_double), ("beta2", C.c_double), ("eps", C.c_double),
+                ("weight_decay", C.c_double)]
+
+
+class ClosureReport(C.Structure):
+    _fields_ = [("judged_tiles", C.c_int64), ("failed_tiles", C.c_int64), ("est_rel_l2", C.c_double),
+                ("fallbacks", C.c_int32), ("reserved", C.c_int32)]
 
 
 class CgefError(RuntimeError):
@@ -124,6 +138,19 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_profile_read.argtypes = [i32, C.POINTER(dbl), C.POINTER(i64)]
     L.cgef_profile_read.restype = i32
     L.cgef_profile_reset.restype = None
+    L.cgef_closure_create.argtypes = [C.POINTER(vp), C.c_uint64]
+    L.cgef_closure_destroy.argtypes = [vp]
+    L.cgef_closure_get_params.argtypes = [vp, vp]
+    L.cgef_closure_set_params.argtypes = [vp, vp]
+    L.cgef_closure_pairs_device.argtypes = [vp, i32, vp, vp, i64, vp, vp, vp, vp]
+    L.cgef_closure_train_device.argtypes = [vp, vp, vp, i64, i64, i32, C.POINTER(AdamW), vp, vp]
+    L.cgef_closure_forward_device.argtypes = [vp, vp, i64, vp, vp]
+    L.cgef_closure_grad_device.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+    L.cgef_closure_pi_device.argtypes = [vp, vp, i32, vp, vp, i64, vp, dbl, C.c_uint64, dbl, vp,
+                                         C.POINTER(ClosureReport), vp]
+    for n in ("create", "destroy", "get_params", "set_params", "pairs_device", "train_device", "forward_device",
+              "grad_device", "pi_device"):
+        getattr(L, "cgef_closure_" + n).restype = i32
     _lib = L
     return L
 

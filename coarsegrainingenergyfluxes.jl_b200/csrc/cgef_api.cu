@@ -24,8 +24,8 @@ thread_local bool g_prof_suspended = false;
 thread_local std::vector<ProfRec> g_recs;
 thread_local cudaEvent_t g_open = nullptr;
 thread_local int g_open_kind = -1;
-thread_local double g_prof_ms[CGEF_KERNEL_KINDS] = {0, 0, 0, 0, 0};
-thread_local int64_t g_prof_n[CGEF_KERNEL_KINDS] = {0, 0, 0, 0, 0};
+thread_local double g_prof_ms[CGEF_KERNEL_KINDS] = {};
+thread_local int64_t g_prof_n[CGEF_KERNEL_KINDS] = {};
 
 void drain_profile() {
   for (auto& r : g_recs) {
@@ -100,10 +100,7 @@ int ensure_ws(cgef_plan* p, int slot, size_t bytes, void** out) {
 
 using namespace cgef;
 
-namespace {
-
-constexpr int kSlotPlanes = 0, kSlotGather = 1, kSlotPartials = 2, kSlotIn = 3, kSlotOut = 4, kSlotAux = 5,
-              kSlotMask = 6, kSlotSplit = 8;
+namespace cgef {
 
 size_t dsize(int dtype) { return dtype == CGEF_F32 ? sizeof(float) : sizeof(double); }
 
@@ -116,18 +113,6 @@ int check_plan(const cgef_plan* p) {
 int check_dtype(int dtype) {
   return (dtype == CGEF_F64 || dtype == CGEF_F32) ? CGEF_OK : fail(CGEF_EINVAL, "dtype must be CGEF_F64 or CGEF_F32");
 }
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-  }
-};
 
 int pitch_for(const cgef_plan* p, int halo) {
   const int wide = kTileCols;
@@ -247,6 +232,10 @@ int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int
   }
   return launch_strain(p, sa, st);
 }
+
+}  // namespace cgef
+
+namespace {
 
 // Filters nf (<= 4 per pass) fields; outputs FP64 planes (slice stride `ostride`).
 int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int nf, double* const* outs,

@@ -206,6 +206,12 @@ int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, in
                   const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
                   cudaStream_t st);
 
+// The same over a caller-given device list of unsplit work items (slot -1), e.g. a subset of
+// tiles; the plan's own schedule and split groups are not used.
+int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                        const uint8_t* mask, int64_t mask_slice_stride, double* partials, const WorkItem* items,
+                        int nitems, const GatherOut& out, cudaStream_t st);
+
 // Bytes of partial-sum scratch a banded launch of `na` accumulated quantities over `nbatch`
 // slices needs.
 inline size_t banded_partials_bytes(const cgef_plan* p, int na, int nbatch) {
@@ -246,6 +252,14 @@ struct StrainArgs {
   double* partials;  // nbatch * nblocks * 2, or nullptr
   double* energy;    // nullptr = skip
   int64_t energy_stride;
+  // closure features: grad[slice][4][ny*nx] (FP32) = grad_scale * (S_ee, du/dy, dv/dx + u t, S_nn),
+  // and grad_mean[slice] = mean over active cells of their squared norm (grad_partials: scratch of
+  // nbatch * nblocks * 2 doubles).  nullptr = skip.  txx/txy/tyy may be nullptr (read as 0).
+  float* grad;
+  int64_t grad_slice_stride;
+  double grad_scale;
+  double* grad_partials;
+  double* grad_mean;
 };
 
 int launch_strain(const cgef_plan* p, const StrainArgs& a, cudaStream_t st);
@@ -261,5 +275,49 @@ int launch_convert(const double* src, int64_t src_stride, void* dst, int64_t dst
 int launch_energy(const cgef_plan* p, const double* ubar, const double* vbar, int64_t slice_stride,
                   const uint8_t* mask, int64_t mask_slice_stride, int nbatch, double* partials, double* energy,
                   int64_t energy_stride, cudaStream_t st);
+
+
+// ---- shared host helpers (cgef_api.cu) ----
+// Workspace slots of a plan (cgef_plan::ws).
+enum WsSlot {
+  kSlotPlanes = 0,
+  kSlotGather = 1,
+  kSlotPartials = 2,
+  kSlotIn = 3,
+  kSlotOut = 4,
+  kSlotAux = 5,
+  kSlotMask = 6,
+  kSlotDeriv = 7,
+  kSlotSplit = 8,
+  kSlotVel = 9,
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+size_t dsize(int dtype);
+int check_plan(const cgef_plan* p);
+int check_dtype(int dtype);
+// Row pitch (doubles) of the staged planes for a halo of `halo` columns.
+int pitch_for(const cgef_plan* p, int halo);
+// kModePiSphere or kModePiCart.
+int mode_for(const cgef_plan* p);
+// Stages u, v (planetary components on the sphere) into padded planes in slot kSlotPlanes.
+int stage_pi(cgef_plan* p, int dtype, const void* u, const void* v, int nbatch, const uint8_t* mask, int64_t mstride,
+             int halo, double** planes_out, int* pitch_out, int* np_out, cudaStream_t st);
+// Runs the plan's engine in a flux mode: 5 FP64 planes (ubar, vbar, txx, txy, tyy) per slice.
+int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, int nbatch, const uint8_t* mask,
+              int64_t mstride, double* gather, cudaStream_t st);
+int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int64_t nbatch64,
+                      const uint8_t* slice_masks, const cgef_pi_outputs* out, cudaStream_t st);
 
 }  // namespace cgef

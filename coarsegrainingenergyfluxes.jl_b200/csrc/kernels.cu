@@ -695,12 +695,18 @@ struct StrainK {
   void* syy_o;
   int64_t out_stride;
   double* partials;  // [slice][block][2]
+  // velocity-gradient planes (closure features): scale * (S_ee-form du/dx, du/dy, dv/dx + u t, dv/dy)
+  float* grad;       // [slice][4][ny*nx] or nullptr
+  int64_t grad_stride;
+  double grad_scale;
+  double* gpartials;  // [slice][block][2]: sum of |grad|^2 and active count
 };
 
 constexpr int kStrainBX = 32, kStrainBY = 8;
 
 __device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
   // deterministic: warp shuffles in a fixed tree, then warp results in order
+  __syncthreads();  // sh may still be read by a previous call
   for (int off = 16; off > 0; off >>= 1) {
     a += __shfl_down_sync(0xffffffffu, a, off);
     b += __shfl_down_sync(0xffffffffu, b, off);
@@ -728,7 +734,7 @@ __global__ void strain_kernel(StrainK a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int s = blockIdx.z;
-  double e_num = 0.0, e_area = 0.0;
+  double e_num = 0.0, e_area = 0.0, g_sum = 0.0, g_cnt = 0.0;
   if (i < a.nx && j < a.ny) {
     const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
     const int64_t o = s * a.out_stride + pix;
@@ -737,9 +743,11 @@ __global__ void strain_kernel(StrainK a) {
     const double* ub = a.ub + s * a.in_stride;
     const double* vb = a.vb + s * a.in_stride;
     double sxx = 0.0, sxy = 0.0, syy = 0.0, pi = 0.0;
+    double g1 = 0.0, g2 = 0.0;  // du/dy and dv/dx + u t (the two halves of 2 S_en)
     const double u0 = ub[pix], v0 = vb[pix];
-    const double txx = a.txx[s * a.in_stride + pix], txy = a.txy[s * a.in_stride + pix],
-                 tyy = a.tyy[s * a.in_stride + pix];
+    const double txx = a.txx ? a.txx[s * a.in_stride + pix] : 0.0;
+    const double txy = a.txy ? a.txy[s * a.in_stride + pix] : 0.0;
+    const double tyy = a.tyy ? a.tyy[s * a.in_stride + pix] : 0.0;
     if (act) {
       Line Lx{ub + static_cast<int64_t>(j) * a.nx, mk ? mk + static_cast<int64_t>(j) * a.nx : nullptr, 1, a.nx,
               a.periodic_x, a.dx};
@@ -757,8 +765,12 @@ __global__ void strain_kernel(StrainK a) {
         const double tf = a.tanfac[j];
         sxx -= v0 * tf;                          // S_ee = du/dx - v tan(phi)/R
         sxy = 0.5 * (dudy + dvdx + u0 * tf);     // S_en
+        g1 = dudy;
+        g2 = dvdx + u0 * tf;
       } else {
         sxy = 0.5 * (dudy + dvdx);
+        g1 = dudy;
+        g2 = dvdx;
       }
       pi = -(sxx * txx + 2.0 * sxy * txy + syy * tyy);
       const double ar = a.area[j];
@@ -774,6 +786,26 @@ __global__ void strain_kernel(StrainK a) {
     if (a.sxx_o) store_any(a.sxx_o, a.dtype, o, sxx);
     if (a.sxy_o) store_any(a.sxy_o, a.dtype, o, sxy);
     if (a.syy_o) store_any(a.syy_o, a.dtype, o, syy);
+    if (a.grad) {
+      const double g[4] = {a.grad_scale * sxx, a.grad_scale * g1, a.grad_scale * g2, a.grad_scale * syy};
+      float* gp = a.grad + s * a.grad_stride + pix;
+      const int64_t N = static_cast<int64_t>(a.nx) * a.ny;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) gp[k * N] = static_cast<float>(g[k]);
+      if (act) {
+        g_sum = g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + g[3] * g[3];
+        g_cnt = 1.0;
+      }
+    }
+  }
+  if (a.gpartials) {
+    block_sum2(g_sum, g_cnt, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      const int64_t nblk = static_cast<int64_t>(gridDim.x) * gridDim.y;
+      const int64_t b = static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x;
+      a.gpartials[(s * nblk + b) * 2] = g_sum;
+      a.gpartials[(s * nblk + b) * 2 + 1] = g_cnt;
+    }
   }
   if (a.partials) {
     block_sum2(e_num, e_area, sh);
@@ -821,8 +853,10 @@ __global__ void energy_partial_kernel(EnergyK a) {
   }
 }
 
-// One block per slice: sums the block partials in a fixed order; E = 1/2 sum / area.
-__global__ void energy_finish_kernel(const double* partials, int64_t nblk, double* energy, int64_t estride) {
+// One block per slice: sums the block partials in a fixed order; out = factor * sum / weight
+// (E = 1/2 sum / area with factor 1/2).
+__global__ void energy_finish_kernel(const double* partials, int64_t nblk, double* energy, int64_t estride,
+                                     double factor) {
   __shared__ double sa[256], sb[256];
   const int s = blockIdx.x;
   double a = 0.0, b = 0.0;
@@ -840,7 +874,7 @@ __global__ void energy_finish_kernel(const double* partials, int64_t nblk, doubl
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) energy[s * estride] = sb[0] > 0.0 ? 0.5 * sa[0] / sb[0] : 0.0;
+  if (threadIdx.x == 0) energy[s * estride] = sb[0] > 0.0 ? factor * sa[0] / sb[0] : 0.0;
 }
 
 struct DerivK {
@@ -964,6 +998,13 @@ int dispatch_banded(bool def, const BandedK& a, cudaStream_t st) {
 int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                   const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
                   cudaStream_t st) {
+  return launch_banded_items(p, mode, nf, planes, pitch, np, nbatch, mask, mask_slice_stride, partials, nullptr, 0,
+                             out, st);
+}
+
+int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                        const uint8_t* mask, int64_t mask_slice_stride, double* partials, const WorkItem* items,
+                        int nitems, const GatherOut& out, cudaStream_t st) {
   const bool def = p->strategy == CGEF_DEFORMABLE;
   BandedK a{};
   a.planes = planes;
@@ -975,11 +1016,12 @@ int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, in
   a.band_stride = p->geometry == CGEF_SPHERICAL ? 2 * p->D + 1 : 0;
   a.w = p->d_w;
   a.D = p->D;
-  a.items = p->d_items;
-  a.nitems = static_cast<int>(p->h_items.size());
+  a.items = items ? items : p->d_items;
+  a.nitems = items ? nitems : static_cast<int>(p->h_items.size());
   a.nslices = nbatch;
-  a.groups = p->d_groups;
-  a.ngroups = static_cast<int>(p->h_groups.size());
+  a.groups = items ? nullptr : p->d_groups;
+  a.ngroups = items ? 0 : static_cast<int>(p->h_groups.size());
+  if (a.nitems == 0) return CGEF_OK;
   a.partials = partials;
   if (a.ngroups > 0 && partials == nullptr) return fail(CGEF_EINVAL, "banded: split tiles need a partials buffer");
   a.den_zf = p->d_den_zf;
@@ -1169,15 +1211,24 @@ int launch_strain(const cgef_plan* p, const StrainArgs& s, cudaStream_t st) {
   a.syy_o = s.syy_o;
   a.out_stride = s.out_slice_stride;
   a.partials = s.energy ? s.partials : nullptr;
+  a.grad = s.grad;
+  a.grad_stride = s.grad_slice_stride;
+  a.grad_scale = s.grad_scale;
+  a.gpartials = s.grad_mean ? s.grad_partials : nullptr;
   dim3 block(kStrainBX, kStrainBY), grid((p->nx + kStrainBX - 1) / kStrainBX, (p->ny + kStrainBY - 1) / kStrainBY,
                                          s.nbatch);
   prof_begin(CGEF_KERNEL_STRAIN, st);
   strain_kernel<<<grid, block, 0, st>>>(a);
   prof_end(CGEF_KERNEL_STRAIN, st);
   int rc = check_launch("strain_kernel");
-  if (rc || !s.energy) return rc;
+  if (rc) return rc;
   const int64_t nblk = static_cast<int64_t>(grid.x) * grid.y;
-  energy_finish_kernel<<<s.nbatch, 256, 0, st>>>(s.partials, nblk, s.energy, s.energy_stride);
+  if (s.grad_mean) {
+    energy_finish_kernel<<<s.nbatch, 256, 0, st>>>(s.grad_partials, nblk, s.grad_mean, 1, 1.0);
+    if ((rc = check_launch("energy_finish_kernel"))) return rc;
+  }
+  if (!s.energy) return CGEF_OK;
+  energy_finish_kernel<<<s.nbatch, 256, 0, st>>>(s.partials, nblk, s.energy, s.energy_stride, 0.5);
   return check_launch("energy_finish_kernel");
 }
 
@@ -1191,7 +1242,7 @@ int launch_energy(const cgef_plan* p, const double* ubar, const double* vbar, in
   int rc = check_launch("energy_partial_kernel");
   if (rc) return rc;
   const int64_t nblk = static_cast<int64_t>(grid.x) * grid.y;
-  energy_finish_kernel<<<nbatch, 256, 0, st>>>(partials, nblk, energy, energy_stride);
+  energy_finish_kernel<<<nbatch, 256, 0, st>>>(partials, nblk, energy, energy_stride, 0.5);
   return check_launch("energy_finish_kernel");
 }
 

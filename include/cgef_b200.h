@@ -182,6 +182,71 @@ int32_t cgef_sweep_device(cgef_plan* const* plans, int32_t nscales, int32_t dtyp
 int32_t cgef_filter_device_noalloc(cgef_plan* plan, int32_t dtype, const void* field, void* out, int64_t nbatch,
                                    void* stream);
 
+/* ---- Learned closure.  No counterpart in the reference. ----
+ * A pointwise MLP (5 -> 64 -> 64 -> 64 -> 3, GELU) maps the filtered velocity-gradient tensor,
+ * scaled by ell^2, and log ell to the subfilter stress tau; the flux is then -S:tau with S from the
+ * same gradients.  Weights are BF16 operands of tcgen05 tensor-core MMAs with FP32 accumulation
+ * (FP32 master copy, AdamW).  The exact flux path (cgef_compute_pi) generates the training pairs,
+ * judges a seeded fraction of every closure result tile by tile and replaces a slice whose judged
+ * error exceeds the tolerance.
+ *
+ * Per grid point at scale ell (g = ell^2 * (S_ee, du/dy, dv/dx + u t, S_nn) in the local frame, n^2 =
+ * mean over the slice's active points of |g|^2):
+ *   features x = (g / n, (ln ell - ln 223607 m) / 1.4979)         (5 floats)
+ *   targets  y = (tau_ee, tau_en, tau_nn) * ell^2 / n^2            (3 floats)
+ *   closure  tau = MLP(x) * n^2 / ell^2,  Pi = -(S_ee tau_ee + 2 S_en tau_en + S_nn tau_nn).
+ * Parameters (float, CGEF_CLOSURE_NPARAM): W1[64][5] b1[64] W2[64][64] b2[64] W3[64][64] b3[64]
+ * W4[3][64] b4[3]. */
+typedef struct cgef_closure cgef_closure;
+enum { CGEF_CLOSURE_NIN = 5, CGEF_CLOSURE_NHIDDEN = 64, CGEF_CLOSURE_NOUT = 3, CGEF_CLOSURE_NPARAM = 8899 };
+
+typedef struct {
+  double lr, beta1, beta2, eps, weight_decay; /* AdamW; weight decay on the weight matrices only */
+} cgef_adamw;
+
+typedef struct {
+  int64_t judged_tiles; /* 32 x 32 tiles recomputed exactly, summed over slices */
+  int64_t failed_tiles; /* judged tiles whose own Pi error exceeded the tolerance */
+  double est_rel_l2;    /* largest per-slice Pi rel-L2 error of the closure on its judged tiles */
+  int32_t fallbacks;    /* slices recomputed by the exact path */
+  int32_t reserved;
+} cgef_closure_report;
+
+/* Creates a closure on the current device with uniform(+-1/sqrt(fan_in)) weights from `seed`. */
+int32_t cgef_closure_create(cgef_closure** out, uint64_t seed);
+int32_t cgef_closure_destroy(cgef_closure* c);
+/* Host copies of the FP32 master parameters (CGEF_CLOSURE_NPARAM floats). */
+int32_t cgef_closure_get_params(const cgef_closure* c, float* params);
+int32_t cgef_closure_set_params(cgef_closure* c, const float* params);
+
+/* Training pairs from the exact flux path on device buffers: features[nbatch][5][ny*nx] and
+ * targets[nbatch][3][ny*nx] (FP32, planar); masked points hold zeros. */
+int32_t cgef_closure_pairs_device(cgef_plan* plan, int32_t dtype, const void* u, const void* v, int64_t nbatch,
+                                  const uint8_t* slice_masks, float* features, float* targets, void* stream);
+
+/* `nsteps` AdamW steps on device pairs x[npoints][5], t[npoints][3]; step k uses the `batch` points
+ * from (k * batch) mod npoints (shuffle beforehand).  Loss L = sum_o (y_o - t_o)^2 averaged over the
+ * batch; losses[k] receives step k's loss (device buffer, may be NULL). */
+int32_t cgef_closure_train_device(cgef_closure* c, const float* x, const float* t, int64_t npoints, int64_t batch,
+                                  int32_t nsteps, const cgef_adamw* opt, float* losses, void* stream);
+
+/* Network outputs y[npoints][3] for features x[npoints][5] (device). */
+int32_t cgef_closure_forward_device(cgef_closure* c, const float* x, int64_t npoints, float* y, void* stream);
+
+/* Gradient of L over all npoints as one batch, no update: grads[CGEF_CLOSURE_NPARAM] and loss[1]
+ * (device). */
+int32_t cgef_closure_grad_device(cgef_closure* c, const float* x, const float* t, int64_t npoints, float* grads,
+                                 float* loss, void* stream);
+
+/* The flux by the closure at the plan's scale for nbatch slices (device buffers, like
+ * cgef_compute_pi_device's pi output).  A seeded `judge_fraction` of the 32 x 32 tiles (at least one)
+ * is recomputed by the exact path and written exactly; a slice whose closure error on its judged
+ * tiles exceeds `tol` (relative L2) is recomputed entirely by the exact path.  Synchronises
+ * `stream` once to read the judge's sums.  `report` may be NULL. */
+int32_t cgef_closure_pi_device(cgef_closure* c, cgef_plan* plan, int32_t dtype, const void* u, const void* v,
+                               int64_t nbatch, const uint8_t* slice_masks, double judge_fraction,
+                               uint64_t judge_seed, double tol, void* pi, cgef_closure_report* report, void* stream);
+
 /* Tracing (no counterpart in the reference, which has none).  Kernel launches made by this
  * thread's calls since the last reset. */
 int64_t cgef_launch_count(void);
@@ -191,7 +256,7 @@ void cgef_reset_launch_count(void);
  * below with CUDA events on the launch's own stream.  `cgef_profile_read` waits for the recorded
  * events and returns the summed duration (ms) and launch count of one kind since the last reset. */
 enum { CGEF_KERNEL_STAGE = 0, CGEF_KERNEL_BANDED = 1, CGEF_KERNEL_SEPARABLE = 2, CGEF_KERNEL_PREFIX = 3,
-       CGEF_KERNEL_STRAIN = 4, CGEF_KERNEL_KINDS = 5 };
+       CGEF_KERNEL_STRAIN = 4, CGEF_KERNEL_CLOSURE = 5, CGEF_KERNEL_KINDS = 6 };
 void cgef_profile_enable(int32_t enable);
 int32_t cgef_profile_read(int32_t kind, double* total_ms, int64_t* launches);
 void cgef_profile_reset(void);

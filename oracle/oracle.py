@@ -73,6 +73,13 @@ def lib():
         L.orc_count_entries.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]
         L.orc_count_entries.restype = C.c_int64
+        L.orc_closure_nparam.restype = C.c_int
+        L.orc_bf16.argtypes = [C.c_float]
+        L.orc_bf16.restype = C.c_float
+        L.orc_closure_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.orc_closure_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+        L.orc_closure_adamw.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
+                                        C.c_float, C.c_float, C.c_float, C.c_float]
         _ = dp
         _lib = L
     return _lib
@@ -232,3 +239,37 @@ def count_entries(grid: Grid, kernel: int, alpha: float, ell: float) -> int:
 
 def max_threads() -> int:
     return lib().orc_max_threads()
+
+
+# ---- learned closure (closure_oracle.c): the checker of the tensor-core MLP kernels ----
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def closure_nparam() -> int:
+    return int(lib().orc_closure_nparam())
+
+
+def closure_forward(params, x) -> np.ndarray:
+    """y (n, 3) of the MLP with BF16 operands and FP32 sums for features x (n, 5)."""
+    P, X = _f32(params), _f32(x)
+    y = np.empty((X.shape[0], 3), np.float32)
+    lib().orc_closure_forward(_ptr(P), _ptr(X), X.shape[0], _ptr(y))
+    return y
+
+
+def closure_grad(params, x, t):
+    """(gradient (float64, nparam), loss) of mean_i sum_o (y_io - t_io)^2."""
+    P, X, T = _f32(params), _f32(x), _f32(t)
+    g = np.empty(closure_nparam(), np.float64)
+    loss = C.c_double()
+    lib().orc_closure_grad(_ptr(P), _ptr(X), _ptr(T), X.shape[0], _ptr(g), C.byref(loss))
+    return g, loss.value
+
+
+def closure_adamw(params, m, v, g, step, lr, b1=0.9, b2=0.999, eps=1e-8, wd=0.0):
+    """One AdamW step in place on float32 arrays (weight decay on weight matrices only)."""
+    for a in (params, m, v):
+        assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    G = _f32(g)
+    lib().orc_closure_adamw(_ptr(params), _ptr(m), _ptr(v), _ptr(G), int(step), lr, b1, b2, eps, wd)

@@ -1,0 +1,193 @@
+"""The learned closure on the GPU, checked against its CPU oracle (oracle/closure_oracle.c) and
+against the exact flux path: tensor-core forward values, gradients and AdamW step; the training
+pairs; the judge and its fallback."""
+import math
+
+import numpy as np
+import pytest
+
+import cgef_b200 as cg
+from cgef_b200 import closure as CL
+from cgef_b200 import synthetic as S
+import oracle as O
+from helpers import oracle_plan, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+OFF = dict(W1=(0, 320), b1=(320, 384), W2=(384, 4480), b2=(4480, 4544), W3=(4544, 8640), b3=(8640, 8704),
+           W4=(8704, 8896), b4=(8896, 8899))
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+@pytest.fixture(scope="module")
+def data(torch):
+    rng = np.random.default_rng(11)
+    n = 1000  # 7 full tiles and a partial one
+    x = rng.standard_normal((n, 5)).astype(np.float32)
+    t = (0.3 * rng.standard_normal((n, 3))).astype(np.float32)
+    return x, t, torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+
+
+def test_forward_matches_oracle(data):
+    x, _, xd, _ = data
+    c = CL.Closure(seed=3)
+    y = c.forward(xd).cpu().numpy()
+    ref = O.closure_forward(c.get_params(), x)
+    assert rel_l2(y, ref) < 5e-3
+
+
+def test_gradient_matches_oracle(data):
+    x, t, xd, td = data
+    c = CL.Closure(seed=5)
+    g, loss = c.grad(xd, td)
+    gref, lref = O.closure_grad(c.get_params(), x, t)
+    assert abs(loss - lref) / lref < 1e-3
+    for k, (a, b) in OFF.items():
+        assert rel_l2(g[a:b], gref[a:b]) < 2e-2, k
+
+
+def test_adamw_step_matches_oracle(data):
+    _, _, xd, td = data
+    c = CL.Closure(seed=8)
+    p0 = c.get_params()
+    g, _ = c.grad(xd, td)
+    c.train(xd, td, batch=xd.shape[0], steps=1, lr=3e-3, weight_decay=0.05)
+    p1 = c.get_params()
+    p = p0.copy()
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    O.closure_adamw(p, m, v, g, 1, 3e-3, 0.9, 0.999, 1e-8, 0.05)
+    np.testing.assert_allclose(p1, p, rtol=1e-5, atol=1e-7)
+
+
+def test_training_reduces_loss(torch):
+    rng = np.random.default_rng(2)
+    n = 8192
+    x = rng.standard_normal((n, 5)).astype(np.float32)
+    t = np.stack([x[:, 0] * x[:, 1], 0.5 * x[:, 2] ** 2 - 0.5, np.tanh(x[:, 3] + 0.3 * x[:, 4])], 1).astype(np.float32)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    c = CL.Closure(seed=1)
+    losses = c.train(xd, td, batch=1024, steps=400, lr=3e-3, weight_decay=0.0)
+    assert np.all(np.isfinite(losses))
+    assert losses[-20:].mean() < 0.15 * losses[:5].mean()
+
+
+def _sphere_case(nlon=144, nlat=72, seed=4):
+    g = S.sphere_grid(nlon, nlat)
+    g = g.with_mask(S.land_mask(g, seed=seed))
+    u, v = S.sphere_fields(g, seed=seed, lmax=min(nlat - 1, 60))
+    return g, u, v
+
+
+def test_training_pairs_match_oracle(torch):
+    g, u, v = _sphere_case()
+    ell = 8e5
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), ell)
+    feat, targ = CL.training_pairs(plan, torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda())
+    feat, targ = feat.cpu().numpy()[0], targ.cpu().numpy()[0]
+    op = oracle_plan(g, cg.GaussianKernel(4.0), ell)
+    r = op.compute_pi(u, v)
+    dudy = op.ddy(r["ubar"])
+    gs = [r["S_xx"], dudy, 2.0 * r["S_xy"] - dudy, r["S_yy"]]
+    m = g.mask
+    l2 = ell * ell
+    n2 = np.mean(sum((l2 * q[m]) ** 2 for q in gs))
+    ref_f = [np.where(m, l2 * q / math.sqrt(n2), 0.0) for q in gs] + [np.where(m, CL.log_feature(ell), 0.0)]
+    ref_t = [np.where(m, r[k] * l2 / n2, 0.0) for k in ("tau_xx", "tau_xy", "tau_yy")]
+    for k in range(5):
+        assert rel_l2(feat[k].reshape(g.shape), ref_f[k]) < 1e-5, k
+    for k in range(3):
+        assert rel_l2(targ[k].reshape(g.shape), ref_t[k]) < 1e-5, k
+
+
+def _plain_pi(torch, plan, ud, vd):
+    return cg.compute_Pi(None, ud, vd, None, plan.grid, plan.kernel, plan.scale, filter_plan=plan)
+
+
+def test_untrained_closure_falls_back_to_the_exact_flux(torch):
+    g, u, v = _sphere_case(seed=6)
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 6e5)
+    ud = torch.from_numpy(np.stack([u, 0.5 * u])).cuda()
+    vd = torch.from_numpy(np.stack([v, 0.5 * v])).cuda()
+    c = CL.Closure(seed=9)
+    pi, rep = c.pi(plan, ud, vd, judge_fraction=0.1, judge_seed=3, tol=0.05)
+    plain = _plain_pi(torch, plan, ud, vd)
+    assert rep.fallbacks == 2 and rep.est_rel_l2 > 0.05 and rep.judged_tiles > 0
+    assert torch.equal(pi, plain)
+
+
+def test_judged_tiles_are_exact(torch):
+    g, u, v = _sphere_case(seed=7)
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 6e5)
+    ud, vd = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+    c = CL.Closure(seed=10)
+    raw, rep0 = c.pi(plan, ud, vd, judge_fraction=0.0)
+    assert rep0.judged_tiles == 0 and rep0.fallbacks == 0
+    judged, rep = c.pi(plan, ud, vd, judge_fraction=0.25, judge_seed=1, tol=1e30)
+    plain = _plain_pi(torch, plan, ud, vd).cpu().numpy()
+    raw, judged = raw.cpu().numpy(), judged.cpu().numpy()
+    nty, ntx = math.ceil(g.ny / 32), math.ceil(g.nx / 32)
+    assert rep.fallbacks == 0 and rep.judged_tiles == round(0.25 * ntx * nty)
+    changed = 0
+    d2 = e2 = 0.0
+    for ty in range(nty):
+        for tx in range(ntx):
+            sl = (slice(32 * ty, 32 * ty + 32), slice(32 * tx, 32 * tx + 32))
+            if np.array_equal(judged[sl], raw[sl]):
+                continue
+            changed += 1
+            assert rel_l2(judged[sl], plain[sl]) < 1e-6
+            d2 += np.sum((raw[sl] - plain[sl]) ** 2)
+            e2 += np.sum(plain[sl] ** 2)
+    assert 0 < changed <= rep.judged_tiles
+    assert abs(math.sqrt(d2 / e2) - rep.est_rel_l2) < 1e-3 * rep.est_rel_l2
+
+
+def test_cartesian_closure_and_fallback(torch):
+    u, v = S.cartesian_fields(n=128, seed=3)
+    g = S.cartesian_grid(n=128)
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 8e3)
+    assert plan.engine == "separable"
+    ud, vd = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+    c = CL.Closure(seed=2)
+    pi, rep = c.pi(plan, ud, vd, judge_fraction=0.05, tol=1e-6)
+    assert rep.fallbacks == 1
+    assert torch.equal(pi, _plain_pi(torch, plan, ud, vd))
+
+
+def test_trained_closure_beats_the_untrained_one(torch):
+    g, u, v = _sphere_case(nlon=360, nlat=180, seed=12)
+    ud, vd = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+    scales = [3e5, 6e5, 1.2e6]
+    xs, ts = [], []
+    m = torch.from_numpy(g.mask.reshape(-1)).cuda()
+    for ell in scales:
+        plan = cg.plan_filter(g, cg.GaussianKernel(4.0), ell)
+        f, t = CL.training_pairs(plan, ud, vd)
+        xs.append(f[0][:, m].T.contiguous())
+        ts.append(t[0][:, m].T.contiguous())
+    x = torch.cat(xs)
+    t = torch.cat(ts)
+    perm = torch.randperm(x.shape[0], generator=torch.Generator().manual_seed(0)).cuda()
+    x, t = x[perm].contiguous(), t[perm].contiguous()
+    c = CL.Closure(seed=4)
+    errs0, errs1 = [], []
+    for ell in scales:
+        plan = cg.plan_filter(g, cg.GaussianKernel(4.0), ell)
+        plain = _plain_pi(torch, plan, ud, vd)
+        errs0.append(rel_l2(c.pi(plan, ud, vd, judge_fraction=0.0)[0].cpu().numpy(), plain.cpu().numpy()))
+    losses = c.train(x, t, batch=4096, steps=600, lr=2e-3, weight_decay=1e-4)
+    assert losses[-50:].mean() < 0.5 * losses[:5].mean()
+    for ell in scales:
+        plan = cg.plan_filter(g, cg.GaussianKernel(4.0), ell)
+        plain = _plain_pi(torch, plan, ud, vd)
+        errs1.append(rel_l2(c.pi(plan, ud, vd, judge_fraction=0.0)[0].cpu().numpy(), plain.cpu().numpy()))
+    # predicting zero flux has error 1; the trained closure must do clearly better than that and
+    # than its untrained self at every scale
+    assert all(e1 < 0.9 for e1 in errs1), errs1
+    assert all(e1 < e0 for e0, e1 in zip(errs0, errs1)), (errs0, errs1)
