@@ -7,6 +7,10 @@ Gaussian alpha = 4, l = 100 km, ZeroFill, ~30% land -- one scale x one snapshot 
   sweep24x8 : 24 scales (50-2000 km, log-spaced) x 8 snapshots per step, Pi and E(l)
   cart256   : 256^2 doubly periodic Cartesian, dx = 1 km, l = 8 km (separable engine)
   levels40  : regional 400 x 600 x 40 levels, FP32 storage, 6 scales 25-400 km, one mask per level
+  closure8  : the learned closure: trained on exact-path pairs of two snapshots at 8 scales
+              (50-1000 km, 10^7 points), then Pi of a fresh snapshot at the 8 scales by the closure
+              (2% of tiles judged exactly, per-slice fallback above the tolerance) against the plain
+              sweep of the same scales
 
 `value` times the device-resident path (inputs already in HBM, an L2 flush between steps inside
 the timed region); `e2e` times the host C-ABI call (pinned host inputs copied in, Pi copied out)
@@ -39,11 +43,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sphere1", choices=["sphere1", "sweep24x8", "cart256", "levels40"])
+    ap.add_argument("--workload", default="sphere1", choices=["sphere1", "sweep24x8", "cart256", "levels40", "closure8"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--snapshots", type=int, default=1, help="snapshots per step of the sphere1 workload")
     ap.add_argument("--scale-km", type=float, default=None, help="filter scale of the sphere1 workload (km)")
+    ap.add_argument("--closure-tol", type=float, default=0.05,
+                    help="closure8: judged Pi rel-L2 above which a slice falls back to the exact path")
+    ap.add_argument("--closure-epochs", type=float, default=3.0, help="closure8: training epochs over 10^7 points")
     return ap.parse_args()
 
 
@@ -52,6 +59,10 @@ def parse():
 # ---------------------------------------------------------------------------------------------
 def sweep_scales():
     return [50e3 * 40.0 ** (s / 23.0) for s in range(24)]
+
+
+def closure_scales():
+    return [50e3 * 20.0 ** (s / 7.0) for s in range(8)]
 
 
 def make_workload(name: str, rank: int, snapshots: int = 1, scale_km=None):
@@ -81,6 +92,14 @@ def make_workload(name: str, rank: int, snapshots: int = 1, scale_km=None):
         u, v = S.cartesian_fields(seed=rank)
         return dict(grid=g, u=u[None], v=v[None], scales=[8000.0], slice_masks=None, kernel=cg.GaussianKernel(4.0),
                     desc="cartesian-256x256-dx1km-periodic-gauss-a4-l8km-zerofill", dtype="f64")
+    if name == "closure8":
+        g = S.sphere_grid()
+        g = g.with_mask(S.land_mask(g, seed=1))
+        u, v = S.sphere_fields(g, seed=4 + rank)
+        return dict(grid=g, u=u[None], v=v[None], scales=closure_scales(), slice_masks=None,
+                    kernel=cg.GaussianKernel(4.0),
+                    desc="closure-sphere-0.25deg-1440x720-gauss-a4-8scales-50to1000km-zerofill-30pct-land",
+                    dtype="f64")
     grid, U, V, M, _ = S.regional_levels(seed=2 + rank)
     scales = [25e3 * 16.0 ** (s / 5.0) for s in range(6)]
     return dict(grid=grid, u=U, v=V, scales=scales, slice_masks=M, kernel=cg.GaussianKernel(4.0),
@@ -249,6 +268,220 @@ def oracle_rate(wl, budget_s: float):
     return rate, nthreads, len(timed), spent, sample
 
 
+def mlp_flops_per_point() -> float:
+    """Multiply-adds x 2 of the closure MLP per point, unpadded (5-64-64-64-3)."""
+    return 2.0 * (5 * 64 + 64 * 64 + 64 * 64 + 64 * 3)
+
+
+def run_closure(args, rank, world, local, dist):
+    """closure8: train the closure on exact pairs, then time closure vs plain Pi at 8 scales."""
+    import ctypes as C
+
+    import torch
+
+    import cgef_b200 as cg
+    from cgef_b200 import _lib
+    from cgef_b200 import closure as CL
+    from cgef_b200 import synthetic as S
+
+    L = _lib.load()
+    wl = make_workload("closure8", rank)
+    g = wl["grid"]
+    scales = wl["scales"]
+    ns = len(scales)
+    N = g.nx * g.ny
+    plans = [cg.plan_filter(g, wl["kernel"], s) for s in scales]
+    stream = torch.cuda.current_stream()
+
+    # training pairs from two snapshots, 10^7 points sampled (seed 3)
+    t0 = time.perf_counter()
+    m = torch.from_numpy(g.mask.reshape(-1)).cuda()
+    xs, ts = [], []
+    for seed in (300 + 2 * rank, 301 + 2 * rank):
+        u, v = S.sphere_fields(g, seed=seed)
+        du, dv = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+        for p in plans:
+            f, t = CL.training_pairs(p, du, dv)
+            xs.append(f[0][:, m].T.contiguous())
+            ts.append(t[0][:, m].T.contiguous())
+    X = torch.cat(xs)
+    T = torch.cat(ts)
+    del xs, ts
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(3)
+    idx = torch.randperm(X.shape[0], device="cuda", generator=gen)[:10_000_000]
+    X, T = X[idx].contiguous(), T[idx].contiguous()
+    torch.cuda.synchronize()
+    pairs_s = time.perf_counter() - t0
+    c = CL.Closure(seed=3)
+    batch = 8192
+    nsteps = int(args.closure_epochs * X.shape[0] / batch)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    l1 = c.train(X, T, batch=batch, steps=nsteps * 2 // 3, lr=2e-3, weight_decay=1e-4)
+    l2 = c.train(X, T, batch=batch, steps=nsteps - nsteps * 2 // 3, lr=4e-4, weight_decay=1e-4)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    losses = np.concatenate([l1, l2])
+    del X, T
+
+    du = torch.from_numpy(np.ascontiguousarray(wl["u"][0])).cuda()
+    dv = torch.from_numpy(np.ascontiguousarray(wl["v"][0])).cuda()
+    parr = (C.c_void_p * ns)(*[p.handle.value for p in plans])
+    dPi = torch.empty((1, ns) + g.shape, dtype=torch.float64, device="cuda")
+    dE = torch.empty((1, ns), dtype=torch.float64, device="cuda")
+    cPi = torch.empty((ns,) + g.shape, dtype=torch.float64, device="cuda")
+    reports = []
+
+    def plain_step():
+        _lib.check(L.cgef_sweep_device(parr, ns, _lib.F64, du.data_ptr(), dv.data_ptr(), 1, None, dPi.data_ptr(),
+                                       dE.data_ptr(), stream.cuda_stream))
+
+    def closure_step(k, frac=0.02, tol=args.closure_tol):
+        reports.clear()
+        for s, p in enumerate(plans):
+            _, rep = c.pi(p, du, dv, judge_fraction=frac, judge_seed=1000 * k + s, tol=tol, out=cPi[s])
+            reports.append(rep)
+
+    # accuracy: raw closure (no judge) and the judged result against the exact flux
+    plain_step()
+    closure_step(0, frac=0.0, tol=float("inf"))
+    torch.cuda.synchronize()
+    exact = dPi[0].cpu().numpy()
+    msk = g.mask
+    raw_err = [float(np.linalg.norm((cPi[s].cpu().numpy() - exact[s])[msk]) / np.linalg.norm(exact[s][msk]))
+               for s in range(ns)]
+    closure_step(0)
+    torch.cuda.synchronize()
+    judged_err = [float(np.linalg.norm((cPi[s].cpu().numpy() - exact[s])[msk]) / np.linalg.norm(exact[s][msk]))
+                  for s in range(ns)]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed(fn, steps, profile=False):
+        for k in range(max(args.warmup, 3)):
+            flush.fill_(1.0)
+            fn(k)
+        torch.cuda.synchronize()
+        if profile:
+            L.cgef_reset_launch_count()
+            L.cgef_profile_reset()
+            L.cgef_profile_enable(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(steps):
+            flush.fill_(1.0)
+            fn(k + 100)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    steps = args.steps or 3
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ms_open = timed(lambda k: closure_step(k, tol=float("inf")), steps)
+    reports_open = list(reports)
+    ms_closure = timed(closure_step, steps, profile=True)
+    L.cgef_profile_enable(0)
+    launches = int(L.cgef_launch_count())
+    prof = {}
+    for name, kind in (("banded", _lib.KERNEL_BANDED), ("closure_mlp", _lib.KERNEL_CLOSURE),
+                       ("strain", _lib.KERNEL_STRAIN), ("stage", _lib.KERNEL_STAGE)):
+        tot, cnt = C.c_double(), C.c_int64()
+        _lib.check(L.cgef_profile_read(kind, C.byref(tot), C.byref(cnt)))
+        prof[name] = (tot.value, cnt.value)
+    ms_plain = timed(lambda k: plain_step(), steps)
+    clocks = sampler.stop()
+    fallbacks = sum(r.fallbacks for r in reports)
+    units = N * ns
+    value = world * units * steps / (ms_closure / 1e3)
+    plain_value = world * units * steps / (ms_plain / 1e3)
+
+    # roofline of the dominant kernel (the 3-field FP64 velocity gather) and of the tensor-core MLP
+    act = g.mask.sum(axis=1).astype(np.float64)
+    vel_flops = sum(float((act * p.band_counts()).sum()) * 3 * 2 for p in plans)
+    peak = None
+    try:
+        pk = C.CDLL(os.path.join(ROOT, "coarsegrainingenergyfluxes.jl_b200", "cgef_b200", "libcgef_peak.so"))
+        pk.cgef_peak_fp64_tflops.restype = C.c_double
+        pk.cgef_peak_fp64_tflops.argtypes = [C.c_int]
+        peak = float(pk.cgef_peak_fp64_tflops(local))
+    except Exception:
+        peak = None
+    bt, bc = prof["banded"]
+    mt, mc = prof["closure_mlp"]
+    ach = vel_flops * steps / (bt * 1e-3) / 1e12 if bt > 0 else None
+    mlp_ach = N * ns * mlp_flops_per_point() * steps / (mt * 1e-3) / 1e12 if mt > 0 else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        peaks = {}
+    bf16 = peaks.get("bf16_tflops")
+    roofline = {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                "frac": (ach / peak) if (ach and peak) else None, "traffic": None,
+                "kernel": "banded_kernel in fields mode (3 planetary velocity components, FP64 FMA); judged "
+                          "tiles add a 9-field gather over 2% of the tiles",
+                "per_step_ms": bt / steps, "algorithmic_flops_per_step": vel_flops,
+                "mlp": {"bound": "tensor", "achieved": mlp_ach, "peak": bf16, "unit": "TFLOP/s",
+                        "frac": (mlp_ach / bf16) if (mlp_ach and bf16) else None,
+                        "per_step_ms": mt / steps, "flops_per_point": mlp_flops_per_point(),
+                        "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)"}}
+
+    # end to end: pinned host u, v in, Pi of every scale out, each step
+    hu = torch.from_numpy(np.ascontiguousarray(wl["u"][0])).pin_memory()
+    hv = torch.from_numpy(np.ascontiguousarray(wl["v"][0])).pin_memory()
+    hPi = torch.empty((ns,) + g.shape, dtype=torch.float64).pin_memory()
+
+    def e2e_step(k):
+        du.copy_(hu, non_blocking=True)
+        dv.copy_(hv, non_blocking=True)
+        closure_step(k)
+        hPi.copy_(cPi, non_blocking=True)
+        torch.cuda.synchronize()
+
+    e2e_step(0)
+    t0 = time.perf_counter()
+    for k in range(steps):
+        e2e_step(k + 1)
+    el = time.perf_counter() - t0
+    e2e = {"value": world * units * steps / el, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 8,
+           "d2h_bytes_per_step": ns * N * 8, "steps": steps,
+           "timing": "wall clock: pinned H2D of u, v, the closure at 8 scales, D2H of Pi"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, nth, done, el, sample = oracle_rate(wl, budget_s=20.0)
+        cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
+               "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path (plain Pi, FP64 oracle)"}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms_closure / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 flux, bf16 closure (fp32 accumulate)", "data": "synthetic (seeded)",
+            "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": 1,
+                       "judge_fraction": 0.02, "tol": args.closure_tol,
+                       "l2": "flushed between steps (256 MiB write, inside the timed region)",
+                       "parallelism": f"{world} rank(s), independent snapshots per rank"},
+            "closure": {"plain_value": plain_value, "plain_ms_per_step": ms_plain / steps,
+                        "speedup_vs_plain": value / plain_value, "fallback_slices_per_step": fallbacks,
+                        "no_fallback_value": world * units * steps / (ms_open / 1e3),
+                        "no_fallback_ms_per_step": ms_open / steps,
+                        "no_fallback_speedup_vs_plain": (world * units * steps / (ms_open / 1e3)) / plain_value,
+                        "no_fallback_est_rel_l2": [r.est_rel_l2 for r in reports_open],
+                        "pi_rel_l2_raw": raw_err, "pi_rel_l2_judged": judged_err,
+                        "est_rel_l2_judge": [r.est_rel_l2 for r in reports],
+                        "scales_km": [s / 1e3 for s in scales],
+                        "training": {"points": 10_000_000, "batch": batch, "steps": int(nsteps),
+                                     "seconds": train_s, "pairs_seconds": pairs_s,
+                                     "loss_first": float(losses[:10].mean()), "loss_last": float(losses[-50:].mean())}},
+            "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
 def cpu_model() -> str:
     try:
         for line in open("/proc/cpuinfo"):
@@ -293,6 +526,8 @@ def main():
     import cgef_b200 as cg
     from cgef_b200 import _lib
 
+    if args.workload == "closure8":
+        return run_closure(args, rank, world, local, dist)
     wl = make_workload(args.workload, rank, args.snapshots, args.scale_km)
     g = wl["grid"]
     nsl = int(wl["u"].shape[0])

@@ -151,6 +151,20 @@ double kernel_radius(int kernel, double alpha, double ell);
 // Host plan construction (plan_build.cpp).
 int build_plan_tables(cgef_plan* p);
 
+// Banded schedule pieces.  Source-row costs of the kRows-row target group starting at j0: for each
+// source row in [j0 - D, j0 + kRows - 1 + D], the width of the union of the group's intervals plus a
+// per-row overhead (0 where the row is outside a bounded grid or holds no entries).
+std::vector<double> group_row_costs(const cgef_plan* p, int j0);
+// Appends the work items of target group (x0, j0): one item when its cost is within `target`,
+// otherwise contiguous source-row parts of about `target` cost plus their split group (slots
+// numbered from `slots`, which advances).
+void emit_group_items(int x0, int j0, int D, const std::vector<double>& rc, double target,
+                      std::vector<WorkItem>& items, std::vector<SplitGroup>& groups, int& slots);
+// A schedule for the 32 x 32 tiles (tx, ty) only, split so that it fills `sms` SMs in one wave;
+// slots are numbered from 0.
+void subset_schedule(const cgef_plan* p, const std::vector<std::pair<int, int>>& tiles, int sms,
+                     std::vector<WorkItem>& items, std::vector<SplitGroup>& groups, int& slots);
+
 // Visits band b's footprint entries in the reference's CSR order (row offset ascending, then
 // column offset ascending): f(ddi, ddj, w).
 template <typename F>
@@ -206,11 +220,11 @@ int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, in
                   const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
                   cudaStream_t st);
 
-// The same over a caller-given device list of unsplit work items (slot -1), e.g. a subset of
-// tiles; the plan's own schedule and split groups are not used.
+// The same over a caller-given device schedule: work items and the split groups they belong to
+// (e.g. from subset_schedule); `partials` holds the slots that schedule numbers.
 int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                         const uint8_t* mask, int64_t mask_slice_stride, double* partials, const WorkItem* items,
-                        int nitems, const GatherOut& out, cudaStream_t st);
+                        int nitems, const SplitGroup* groups, int ngroups, const GatherOut& out, cudaStream_t st);
 
 // Bytes of partial-sum scratch a banded launch of `na` accumulated quantities over `nbatch`
 // slices needs.

@@ -1147,34 +1147,46 @@ int32_t cgef_closure_pi_device(cgef_closure* c, cgef_plan* p, int32_t dtype, con
     if ((rc = ensure_ws(p, kSlotGather, sizeof(double) * 5 * N * nbatch, &gather))) return rc;
     double* G = static_cast<double*>(gather);
     const int mode = mode_for(p);
+    // a schedule of the judged tiles' work items alone, split finely enough to fill the GPU in
+    // one wave (a few tiles cut at the whole grid's granularity would leave most SMs idle)
     std::vector<WorkItem> items;
+    std::vector<SplitGroup> groups;
+    int jslots = 0;
     const bool banded = p->engine == CGEF_ENGINE_BANDED;
     if (banded) {
-      for (int i = 0; i < nj; ++i)
-        for (int r = 0; r < 32; r += kRows) {
-          const int j0 = tiles[2 * i + 1] * 32 + r;
-          if (j0 >= p->ny) break;
-          items.push_back(WorkItem{tiles[2 * i] * 32, j0, j0 - p->D, j0 + kRows + p->D, -1, 0});
-        }
+      std::vector<std::pair<int, int>> tl(nj);
+      for (int i = 0; i < nj; ++i) tl[i] = {tiles[2 * i], tiles[2 * i + 1]};
+      subset_schedule(p, tl, c->sms, items, groups, jslots);
     }
     const size_t tiles_b = sizeof(int32_t) * 2 * nj, items_b = sizeof(WorkItem) * items.size();
+    const size_t groups_b = sizeof(SplitGroup) * groups.size();
     const size_t sums_b = sizeof(double) * 2 * static_cast<size_t>(nj) * nbatch;
+    auto al = [](size_t b) { return (b + 15) / 16 * 16; };
     void* jw = nullptr;
-    if ((rc = cl_ws(c, 3, sums_b + tiles_b + items_b + 64, &jw))) return rc;
-    double* d_sums = static_cast<double*>(jw);
-    int32_t* d_tiles = reinterpret_cast<int32_t*>(static_cast<char*>(jw) + sums_b);
-    WorkItem* d_items = reinterpret_cast<WorkItem*>(static_cast<char*>(jw) + ((sums_b + tiles_b + 15) / 16) * 16);
+    if ((rc = cl_ws(c, 3, al(sums_b) + al(tiles_b) + al(items_b) + al(groups_b) + 16, &jw))) return rc;
+    char* jb = static_cast<char*>(jw);
+    double* d_sums = reinterpret_cast<double*>(jb);
+    int32_t* d_tiles = reinterpret_cast<int32_t*>(jb + al(sums_b));
+    WorkItem* d_items = reinterpret_cast<WorkItem*>(jb + al(sums_b) + al(tiles_b));
+    SplitGroup* d_groups = reinterpret_cast<SplitGroup*>(jb + al(sums_b) + al(tiles_b) + al(items_b));
     cudaError_t e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles_b, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && !items.empty())
       e = cudaMemcpyAsync(d_items, items.data(), items_b, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !groups.empty())
+      e = cudaMemcpyAsync(d_groups, groups.data(), groups_b, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_fail(e, "judge tiles H2D");
     GatherOut go{};
     for (int m = 0; m < 5; ++m) go.o[m] = G + m * N;
     go.slice_stride = 5 * N;
-    if (banded)
-      rc = launch_banded_items(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, nullptr, d_items,
-                               static_cast<int>(items.size()), go, st);
-    else
+    if (banded) {
+      const int na = (mode == kModePiSphere ? 9 : 5) + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
+      void* part = nullptr;
+      const size_t pb = sizeof(double) * static_cast<size_t>(jslots) * nbatch * kRows * na * 32;
+      if (pb > 0 && (rc = ensure_ws(p, kSlotSplit, pb, &part))) return rc;
+      rc = launch_banded_items(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part),
+                               d_items, static_cast<int>(items.size()), d_groups, static_cast<int>(groups.size()), go,
+                               st);
+    } else
       rc = pi_gather(p, planes, pitch, p->H, np, nbatch, mask, mstride, G, st);
     if (rc) return rc;
     judge_kernel<<<dim3(nj, nbatch), 256, 0, st>>>(d_tiles, nj, G, 5 * N, grad, mask, mstride, p->nx, p->ny,

@@ -999,12 +999,12 @@ int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, in
                   const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
                   cudaStream_t st) {
   return launch_banded_items(p, mode, nf, planes, pitch, np, nbatch, mask, mask_slice_stride, partials, nullptr, 0,
-                             out, st);
+                             nullptr, 0, out, st);
 }
 
 int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                         const uint8_t* mask, int64_t mask_slice_stride, double* partials, const WorkItem* items,
-                        int nitems, const GatherOut& out, cudaStream_t st) {
+                        int nitems, const SplitGroup* groups, int ngroups, const GatherOut& out, cudaStream_t st) {
   const bool def = p->strategy == CGEF_DEFORMABLE;
   BandedK a{};
   a.planes = planes;
@@ -1019,8 +1019,8 @@ int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* plan
   a.items = items ? items : p->d_items;
   a.nitems = items ? nitems : static_cast<int>(p->h_items.size());
   a.nslices = nbatch;
-  a.groups = items ? nullptr : p->d_groups;
-  a.ngroups = items ? 0 : static_cast<int>(p->h_groups.size());
+  a.groups = items ? groups : p->d_groups;
+  a.ngroups = items ? ngroups : static_cast<int>(p->h_groups.size());
   if (a.nitems == 0) return CGEF_OK;
   a.partials = partials;
   if (a.ngroups > 0 && partials == nullptr) return fail(CGEF_EINVAL, "banded: split tiles need a partials buffer");

@@ -221,6 +221,87 @@ void build_banded(const cgef_plan* p, Banded& B) {
 
 }  // namespace
 
+std::vector<double> group_row_costs(const cgef_plan* p, int j0) {
+  const bool sphere = p->geometry == CGEF_SPHERICAL;
+  const int W = 2 * p->D + 1;
+  std::vector<double> rc;
+  rc.reserve(kRows + 2 * p->D);
+  for (int jr = j0 - p->D; jr <= j0 + kRows - 1 + p->D; ++jr) {
+    double c = 0.0;
+    if (p->periodic_y || (jr >= 0 && jr < p->ny)) {
+      int A = -1, HI = -1;
+      for (int t = 0; t < kRows; ++t) {
+        const int j = j0 + t;
+        if (j >= p->ny) continue;
+        const int dj = jr - j;
+        if (dj < -p->D || dj > p->D) continue;
+        const BandRow& r = p->h_rows[(sphere ? static_cast<size_t>(j) * W : 0) + (dj + p->D)];
+        A = std::max(A, r.a);
+        HI = std::max(HI, r.hi);
+      }
+      if (A >= 0) c = static_cast<double>(HI + A + 1) + 4.0;  // + per-row overhead
+    }
+    rc.push_back(c);
+  }
+  return rc;
+}
+
+void emit_group_items(int x0, int j0, int D, const std::vector<double>& rc, double target, std::vector<WorkItem>& items,
+                      std::vector<SplitGroup>& groups, int& slots) {
+  const int jlo = j0 - D;
+  double cg = 0.0;
+  for (double c : rc) cg += c;
+  if (cg <= 0.0) {
+    items.push_back(WorkItem{x0, j0, jlo, jlo, -1, 0});
+    return;
+  }
+  const int nrow = static_cast<int>(rc.size());
+  const int nsplit = std::max(1, std::min(nrow, static_cast<int>(std::ceil(cg / target))));
+  // contiguous source-row parts of about equal cost
+  std::vector<int> cut{0};
+  double acc = 0.0;
+  for (int r = 0; r < nrow; ++r) {
+    acc += rc[r];
+    if (static_cast<int>(cut.size()) < nsplit && acc >= cg * cut.size() / nsplit && r + 1 < nrow) cut.push_back(r + 1);
+  }
+  cut.push_back(nrow);
+  const int parts = static_cast<int>(cut.size()) - 1;
+  if (parts == 1) {
+    items.push_back(WorkItem{x0, j0, jlo, jlo + cut[1], -1, static_cast<int32_t>(std::min(cg, 2e9))});
+    return;
+  }
+  groups.push_back(SplitGroup{x0, j0, slots, parts});
+  for (int q = 0; q < parts; ++q) {
+    double c = 0.0;
+    for (int r = cut[q]; r < cut[q + 1]; ++r) c += rc[r];
+    items.push_back(WorkItem{x0, j0, jlo + cut[q], jlo + cut[q + 1], slots + q, static_cast<int32_t>(std::min(c, 2e9))});
+  }
+  slots += parts;
+}
+
+void subset_schedule(const cgef_plan* p, const std::vector<std::pair<int, int>>& tiles, int sms,
+                     std::vector<WorkItem>& items, std::vector<SplitGroup>& groups, int& slots) {
+  struct G {
+    int x0, j0;
+    std::vector<double> rc;
+  };
+  std::vector<G> gs;
+  double total = 0.0;
+  for (const auto& t : tiles)
+    for (int r = 0; r < 32; r += kRows) {
+      const int j0 = t.second * 32 + r;
+      if (j0 >= p->ny) break;
+      gs.push_back(G{t.first * 32, j0, group_row_costs(p, j0)});
+      for (double c : gs.back().rc) total += c;
+    }
+  const double target = std::max(64.0, total / (sms * 16.0));
+  items.clear();
+  groups.clear();
+  slots = 0;
+  for (const G& g : gs) emit_group_items(g.x0, g.j0, p->D, g.rc, target, items, groups, slots);
+  std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
+}
+
 int build_plan_tables(cgef_plan* p) {
   const int nx = p->nx, ny = p->ny;
   const bool sphere = p->geometry == CGEF_SPHERICAL;
@@ -321,27 +402,9 @@ int build_plan_tables(cgef_plan* p) {
     const int ntx = (nx + 31) / 32;
     std::vector<std::vector<double>> rowcost(ngroups);  // per group, per source row: union width
     double total = 0.0;
-    for (int g = 0; g < ngroups; ++g) {
-      int j0 = g * kRows;
-      for (int jr = j0 - B.D; jr <= j0 + kRows - 1 + B.D; ++jr) {
-        double c = 0.0;
-        if (p->periodic_y || (jr >= 0 && jr < ny)) {
-          int A = -1, HI = -1;
-          for (int t = 0; t < kRows; ++t) {
-            int j = j0 + t;
-            if (j >= ny) continue;
-            int dj = jr - j;
-            if (dj < -B.D || dj > B.D) continue;
-            const BandRow& r = B.rows[(sphere ? static_cast<size_t>(j) * W : 0) + (dj + B.D)];
-            A = std::max(A, r.a);
-            HI = std::max(HI, r.hi);
-          }
-          if (A >= 0) c = static_cast<double>(HI + A + 1) + 4.0;  // + per-row overhead
-        }
-        rowcost[g].push_back(c);
-        total += c * ntx;
-      }
-    }
+    parallel_for(ngroups, [&](int g) { rowcost[g] = group_row_costs(p, g * kRows); });
+    for (int g = 0; g < ngroups; ++g)
+      for (double c : rowcost[g]) total += c * ntx;
     int sms = 148;
     {
       int dev = 0;
@@ -355,41 +418,8 @@ int build_plan_tables(cgef_plan* p) {
     std::vector<WorkItem> items;
     std::vector<SplitGroup> groups;
     int slots = 0;
-    for (int g = 0; g < ngroups; ++g) {
-      const int j0 = g * kRows;
-      const int jlo = j0 - B.D;
-      double cg = 0.0;
-      for (double c : rowcost[g]) cg += c;
-      if (cg <= 0.0) {
-        for (int x = 0; x < nx; x += 32) items.push_back(WorkItem{x, j0, jlo, jlo, -1, 0});
-        continue;
-      }
-      const int nsplit = std::max(1, std::min(static_cast<int>(rowcost[g].size()), static_cast<int>(std::ceil(cg / target))));
-      // contiguous source-row parts of about equal cost
-      std::vector<int> cut{0};
-      double acc = 0.0;
-      for (int r = 0; r < static_cast<int>(rowcost[g].size()); ++r) {
-        acc += rowcost[g][r];
-        if (static_cast<int>(cut.size()) < nsplit && acc >= cg * cut.size() / nsplit && r + 1 < static_cast<int>(rowcost[g].size()))
-          cut.push_back(r + 1);
-      }
-      cut.push_back(static_cast<int>(rowcost[g].size()));
-      const int parts = static_cast<int>(cut.size()) - 1;
-      for (int x = 0; x < nx; x += 32) {
-        if (parts == 1) {
-          items.push_back(WorkItem{x, j0, jlo, jlo + cut[1], -1, static_cast<int32_t>(std::min(cg, 2e9))});
-          continue;
-        }
-        groups.push_back(SplitGroup{x, j0, slots, parts});
-        for (int q = 0; q < parts; ++q) {
-          double c = 0.0;
-          for (int r = cut[q]; r < cut[q + 1]; ++r) c += rowcost[g][r];
-          items.push_back(WorkItem{x, j0, jlo + cut[q], jlo + cut[q + 1], slots + q, static_cast<int32_t>(std::min(c, 2e9))});
-        }
-        slots += parts;
-      }
-    }
-    (void)ntx;
+    for (int g = 0; g < ngroups; ++g)
+      for (int x = 0; x < nx; x += 32) emit_group_items(x, g * kRows, B.D, rowcost[g], target, items, groups, slots);
     std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
     p->h_groups = groups;
     p->nslots = slots;
