@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--closure-tol", type=float, default=0.05,
                     help="closure8: judged Pi rel-L2 above which a slice falls back to the exact path")
     ap.add_argument("--closure-epochs", type=float, default=3.0, help="closure8: training epochs over 10^7 points")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default banded schedules")
     return ap.parse_args()
 
 
@@ -291,6 +292,7 @@ def run_closure(args, rank, world, local, dist):
     ns = len(scales)
     N = g.nx * g.ny
     plans = [cg.plan_filter(g, wl["kernel"], s) for s in scales]
+    waves = [p.autotune(1) if not args.no_autotune else 4.0 for p in plans]
     stream = torch.cuda.current_stream()
 
     # training pairs from two snapshots, 10^7 points sampled (seed 3)
@@ -462,7 +464,7 @@ def run_closure(args, rank, world, local, dist):
             "warmup": args.warmup, "ms_per_step": ms_closure / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 flux, bf16 closure (fp32 accumulate)", "data": "synthetic (seeded)",
             "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": 1,
-                       "judge_fraction": 0.02, "tol": args.closure_tol,
+                       "judge_fraction": 0.02, "tol": args.closure_tol, "schedule_split_waves": waves,
                        "l2": "flushed between steps (256 MiB write, inside the timed region)",
                        "parallelism": f"{world} rank(s), independent snapshots per rank"},
             "closure": {"plain_value": plain_value, "plain_ms_per_step": ms_plain / steps,
@@ -534,6 +536,8 @@ def main():
     ns = len(wl["scales"])
     plans = [cg.plan_filter(g.with_mask(None) if wl["slice_masks"] is not None else g, wl["kernel"], s)
              for s in wl["scales"]]
+    # schedule autotuning is plan setup, like building the footprint: outside the timed region
+    waves = [p.autotune(nsl) if not args.no_autotune else 4.0 for p in plans]
     L = _lib.load()
     tdt = torch.float32 if wl["dtype"] == "f32" else torch.float64
     du = torch.from_numpy(np.ascontiguousarray(wl["u"])).to(device="cuda", dtype=tdt)
@@ -683,7 +687,8 @@ def main():
             "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": nsl,
                        "active_fraction": float(1.0 if g.mask is None else g.mask.mean()),
                        "l2": "flushed between steps (256 MiB write, inside the timed region)",
-                       "parallelism": f"{world} rank(s), independent snapshots per rank"},
+                       "parallelism": f"{world} rank(s), independent snapshots per rank",
+                       "schedule_split_waves": waves},
             "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}
     print(json.dumps(line))
     return 0

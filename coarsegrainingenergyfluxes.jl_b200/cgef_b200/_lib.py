@@ -34,7 +34,7 @@ EXPORTED = [
     "cgef_profile_enable", "cgef_profile_read", "cgef_profile_reset", "cgef_filter_device_noalloc",
     "cgef_closure_create", "cgef_closure_destroy", "cgef_closure_get_params", "cgef_closure_set_params",
     "cgef_closure_pairs_device", "cgef_closure_train_device", "cgef_closure_forward_device",
-    "cgef_closure_grad_device", "cgef_closure_pi_device",
+    "cgef_closure_grad_device", "cgef_closure_pi_device", "cgef_plan_autotune", "cgef_plan_set_split_waves",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE = 0, 1, 2, 3, 4, 5
 CLOSURE_NPARAM = 8899
@@ -138,6 +138,10 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_profile_read.argtypes = [i32, C.POINTER(dbl), C.POINTER(i64)]
     L.cgef_profile_read.restype = i32
     L.cgef_profile_reset.restype = None
+    L.cgef_plan_autotune.argtypes = [vp, i32, C.POINTER(dbl)]
+    L.cgef_plan_autotune.restype = i32
+    L.cgef_plan_set_split_waves.argtypes = [vp, dbl]
+    L.cgef_plan_set_split_waves.restype = i32
     L.cgef_closure_create.argtypes = [C.POINTER(vp), C.c_uint64]
     L.cgef_closure_destroy.argtypes = [vp]
     L.cgef_closure_get_params.argtypes = [vp, vp]

@@ -100,6 +100,19 @@ class PhysicalFilterPlan:
         except Exception:
             pass
 
+    def autotune(self, nbatch: int = 1) -> float:
+        """Times the banded engine's candidate schedules on this plan's grid and keeps the fastest;
+        returns the chosen split granularity (0 for the separable and prefix engines)."""
+        w = C.c_double()
+        _lib.check(_lib.load().cgef_plan_autotune(self.handle, int(nbatch), C.byref(w)))
+        self.split_waves = w.value
+        return w.value
+
+    def set_split_waves(self, waves: float) -> None:
+        """Sets the banded schedule's split granularity (rounds of resident warps per SM)."""
+        _lib.check(_lib.load().cgef_plan_set_split_waves(self.handle, float(waves)))
+        self.split_waves = float(waves)
+
     def footprint(self):
         """The banded footprint in the reference's CSR form (di, dj, w, ptr), 0-based."""
         n = int(self.info.nentries)

@@ -517,6 +517,81 @@ int32_t cgef_plan_get_info(const cgef_plan* p, cgef_plan_info* info) {
   return CGEF_OK;
 }
 
+int32_t cgef_plan_set_split_waves(cgef_plan* p, double waves) {
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (!(waves > 0.0 && waves <= 1024.0)) return fail(CGEF_EINVAL, "waves must be in (0, 1024]");
+  if (p->engine != CGEF_ENGINE_BANDED) return CGEF_OK;
+  DeviceGuard dg(p->device);
+  return rebuild_schedule(p, waves);
+}
+
+int32_t cgef_plan_autotune(cgef_plan* p, int32_t nbatch, double* chosen) {
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (nbatch < 1 || nbatch > 65535) return fail(CGEF_EINVAL, "nbatch must be in 1..65535");
+  if (p->engine != CGEF_ENGINE_BANDED) {
+    if (chosen) *chosen = 0.0;
+    return CGEF_OK;
+  }
+  DeviceGuard dg(p->device);
+  cudaStream_t st = p->stream;
+  const int64_t N = static_cast<int64_t>(p->nx) * p->ny;
+  void* zin = nullptr;
+  if ((rc = ensure_ws(p, kSlotIn, sizeof(double) * 2 * N * nbatch, &zin))) return rc;
+  cudaError_t e = cudaMemsetAsync(zin, 0, sizeof(double) * 2 * N * nbatch, st);
+  if (e != cudaSuccess) return cuda_fail(e, "autotune inputs");
+  double* planes = nullptr;
+  int pitch = 0, np = 0;
+  if ((rc = stage_pi(p, CGEF_F64, zin, static_cast<double*>(zin) + N * nbatch, nbatch, p->d_mask, 0, p->H, &planes,
+                     &pitch, &np, st)))
+    return rc;
+  void* gather = nullptr;
+  if ((rc = ensure_ws(p, kSlotGather, sizeof(double) * 5 * N * nbatch, &gather))) return rc;
+  cudaEvent_t e0, e1;
+  if ((e = cudaEventCreate(&e0)) != cudaSuccess) return cuda_fail(e, "autotune events");
+  if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_fail(e, "autotune events");
+  }
+  const double cand[4] = {2.0, 4.0, 8.0, 16.0};
+  double best = p->split_waves, best_ms = 1e300;
+  for (double w : cand) {
+    if ((rc = rebuild_schedule(p, w))) break;
+    // one untimed pass (partials workspace, caches), then the timed passes
+    if ((rc = pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0, static_cast<double*>(gather), st))) break;
+    // timed passes: three, or one when a pass takes more than 20 ms
+    double ms = 0.0;
+    int done = 0;
+    while (done < 3) {
+      cudaEventRecord(e0, st);
+      rc = pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0, static_cast<double*>(gather), st);
+      cudaEventRecord(e1, st);
+      if (rc) break;
+      float one = 0.f;
+      if ((e = cudaEventSynchronize(e1)) != cudaSuccess || (e = cudaEventElapsedTime(&one, e0, e1)) != cudaSuccess) {
+        rc = cuda_fail(e, "autotune timing");
+        break;
+      }
+      ms += one;
+      ++done;
+      if (one > 20.0f) break;
+    }
+    if (rc) break;
+    ms /= done;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = w;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if ((rc = rebuild_schedule(p, best))) return rc;
+  if (chosen) *chosen = best;
+  return CGEF_OK;
+}
+
 int32_t cgef_plan_get_footprint(const cgef_plan* p, int32_t* di, int32_t* dj, double* w, int64_t* ptr) {
   if (!p) return fail(CGEF_EINVAL, "plan is NULL");
   if (p->engine != CGEF_ENGINE_BANDED) return fail(CGEF_EINVAL, "plan has no banded footprint");

@@ -117,6 +117,8 @@ struct cgef_plan {
   double* d_w = nullptr;            // weights, half rows
   double* d_den_zf = nullptr;       // ZeroFill denominator: ny (periodic x) or ny*nx
   int den_zf_2d = 0;
+  std::vector<std::vector<double>> h_rowcost;  // per target group, per source row (schedule cost model)
+  double split_waves = 4.0;                    // schedule granularity (rounds of resident warps)
   std::vector<cgef::WorkItem> h_items;
   cgef::WorkItem* d_items = nullptr;
   std::vector<cgef::SplitGroup> h_groups;
@@ -160,6 +162,9 @@ std::vector<double> group_row_costs(const cgef_plan* p, int j0);
 // numbered from `slots`, which advances).
 void emit_group_items(int x0, int j0, int D, const std::vector<double>& rc, double target,
                       std::vector<WorkItem>& items, std::vector<SplitGroup>& groups, int& slots);
+// Rebuilds and uploads the plan's work-item schedule, split so that the banded gather runs in
+// about `waves` rounds of 16 resident warps per SM (the autotuner's knob).
+int rebuild_schedule(cgef_plan* p, double waves);
 // A schedule for the 32 x 32 tiles (tx, ty) only, split so that it fills `sms` SMs in one wave;
 // slots are numbered from 0.
 void subset_schedule(const cgef_plan* p, const std::vector<std::pair<int, int>>& tiles, int sms,

@@ -221,6 +221,10 @@ void build_banded(const cgef_plan* p, Banded& B) {
 
 }  // namespace
 
+#ifndef CGEF_SPLIT_WAVES
+#define CGEF_SPLIT_WAVES 4.0
+#endif
+
 std::vector<double> group_row_costs(const cgef_plan* p, int j0) {
   const bool sphere = p->geometry == CGEF_SPHERICAL;
   const int W = 2 * p->D + 1;
@@ -300,6 +304,43 @@ void subset_schedule(const cgef_plan* p, const std::vector<std::pair<int, int>>&
   slots = 0;
   for (const G& g : gs) emit_group_items(g.x0, g.j0, p->D, g.rc, target, items, groups, slots);
   std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
+}
+
+int rebuild_schedule(cgef_plan* p, double waves) {
+  if (!(waves > 0.0)) return fail(CGEF_EINVAL, "split waves must be positive");
+  const int ngroups = static_cast<int>(p->h_rowcost.size());
+  double total = 0.0;
+  const int ntx = (p->nx + 31) / 32;
+  for (int g = 0; g < ngroups; ++g)
+    for (double c : p->h_rowcost[g]) total += c * ntx;
+  int sms = 148;
+  {
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (p->device >= 0 && cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
+      sms = prop.multiProcessorCount;
+    else
+      cudaGetLastError();
+  }
+  // about `waves` rounds of 16 resident warps per SM
+  const double target = std::max(64.0, total / (sms * 16.0 * waves));
+  std::vector<WorkItem> items;
+  std::vector<SplitGroup> groups;
+  int slots = 0;
+  for (int g = 0; g < ngroups; ++g)
+    for (int x = 0; x < p->nx; x += 32) emit_group_items(x, g * kRows, p->D, p->h_rowcost[g], target, items, groups, slots);
+  std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
+  if (p->d_items) cudaFree(p->d_items);
+  if (p->d_groups) cudaFree(p->d_groups);
+  p->d_items = nullptr;
+  p->d_groups = nullptr;
+  p->h_items = std::move(items);
+  p->h_groups = std::move(groups);
+  p->nslots = slots;
+  p->split_waves = waves;
+  int rc;
+  if ((rc = upload(p, &p->d_items, p->h_items.data(), p->h_items.size())) != CGEF_OK) return rc;
+  return upload(p, &p->d_groups, p->h_groups.data(), p->h_groups.size());
 }
 
 int build_plan_tables(cgef_plan* p) {
@@ -399,39 +440,15 @@ int build_plan_tables(cgef_plan* p) {
     // Work items: one warp per (32 columns x kRows rows) tile; a tile whose source rows cost more
     // than a fair share is split along the source rows into partial items, longest first.
     const int ngroups = (ny + kRows - 1) / kRows;
-    const int ntx = (nx + 31) / 32;
-    std::vector<std::vector<double>> rowcost(ngroups);  // per group, per source row: union width
-    double total = 0.0;
-    parallel_for(ngroups, [&](int g) { rowcost[g] = group_row_costs(p, g * kRows); });
-    for (int g = 0; g < ngroups; ++g)
-      for (double c : rowcost[g]) total += c * ntx;
-    int sms = 148;
-    {
-      int dev = 0;
-      cudaDeviceProp prop;
-      if (p->device >= 0 && cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
-        sms = prop.multiProcessorCount;
-      else
-        cudaGetLastError();
-    }
-    const double target = std::max(64.0, total / (sms * 16.0 * 4.0));
-    std::vector<WorkItem> items;
-    std::vector<SplitGroup> groups;
-    int slots = 0;
-    for (int g = 0; g < ngroups; ++g)
-      for (int x = 0; x < nx; x += 32) emit_group_items(x, g * kRows, B.D, rowcost[g], target, items, groups, slots);
-    std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
-    p->h_groups = groups;
-    p->nslots = slots;
-    p->h_items = items;
+    p->h_rowcost.assign(ngroups, {});
+    parallel_for(ngroups, [&](int g) { p->h_rowcost[g] = group_row_costs(p, g * kRows); });
     p->H = std::max(B.Amax, 1);
     int rc;
     if ((rc = upload(p, &p->d_rows, B.rows.data(), B.rows.size())) != CGEF_OK) return rc;
     if (B.w.empty()) B.w.push_back(0.0);
     if ((rc = upload(p, &p->d_w, B.w.data(), B.w.size())) != CGEF_OK) return rc;
     if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
-    if ((rc = upload(p, &p->d_items, items.data(), items.size())) != CGEF_OK) return rc;
-    if ((rc = upload(p, &p->d_groups, groups.data(), groups.size())) != CGEF_OK) return rc;
+    if ((rc = rebuild_schedule(p, CGEF_SPLIT_WAVES)) != CGEF_OK) return rc;
   } else if (p->engine == CGEF_ENGINE_SEPARABLE) {
     // Filtering.jl:1391-1463: square truncation, lim = ceil(rad / step), point-sampled profile.
     p->di_lim = p->dx > 0 ? static_cast<int>(std::ceil(p->rad / p->dx)) : 0;

@@ -123,6 +123,17 @@ int32_t cgef_plan_destroy(cgef_plan* plan);
 /* Plan statistics. */
 int32_t cgef_plan_get_info(const cgef_plan* plan, cgef_plan_info* info);
 
+/* Schedule autotuner of the banded engine (no counterpart in the reference, whose loops have no
+ * schedule).  Times the flux gather on this plan's grid and mask (zero-valued inputs; the gather's
+ * cost depends on the footprint and the mask, not on the values) for each candidate split
+ * granularity -- the work-item schedule cut into about 2, 4, 8 or 16 rounds of resident warps per
+ * SM -- and keeps the fastest; `chosen` (may be NULL) receives it.  A no-op for the separable and
+ * prefix engines.  Results stay within FP64 rounding of each other across schedules: only the
+ * order in which a split tile's partial sums are added changes. */
+int32_t cgef_plan_autotune(cgef_plan* plan, int32_t nbatch, double* chosen);
+/* Sets the split granularity directly (rounds of resident warps per SM, > 0; the default is 4). */
+int32_t cgef_plan_set_split_waves(cgef_plan* plan, double waves);
+
 /* Banded footprint of the plan in the reference's CSR form (FilterFootprint, Filtering.jl:327-336):
  * di/dj/w have nentries entries, ptr has nbands+1 (0-based offsets).  Any pointer may be NULL. */
 int32_t cgef_plan_get_footprint(const cgef_plan* plan, int32_t* di, int32_t* dj, double* w, int64_t* ptr);

@@ -1,0 +1,48 @@
+"""The banded engine's schedule autotuner: it picks one of its candidate split granularities, and
+the flux computed under any schedule stays the oracle's to FP64 rounding."""
+import numpy as np
+import pytest
+
+import cgef_b200 as cg
+from cgef_b200 import synthetic as S
+from helpers import oracle_plan, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    g = S.sphere_grid(360, 180)
+    g = g.with_mask(S.land_mask(g, seed=2))
+    u, v = S.sphere_fields(g, seed=8, lmax=120)
+    return g, u, v
+
+
+def test_autotune_picks_a_candidate_and_keeps_parity(case):
+    g, u, v = case
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 7e5)
+    w = plan.autotune(nbatch=1)
+    assert w in (2.0, 4.0, 8.0, 16.0)
+    Pi = cg.compute_Pi(None, u, v, None, g, plan.kernel, plan.scale, filter_plan=plan)
+    ref = oracle_plan(g, cg.GaussianKernel(4.0), 7e5).compute_pi(u, v)["Pi"]
+    assert rel_l2(Pi, ref) < 1e-9
+    again = cg.compute_Pi(None, u, v, None, g, plan.kernel, plan.scale, filter_plan=plan)
+    assert np.array_equal(Pi, again)
+
+
+def test_every_schedule_gives_the_same_flux(case):
+    g, u, v = case
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 1.2e6)
+    out = []
+    for w in (1.0, 2.0, 16.0, 64.0):
+        plan.set_split_waves(w)
+        out.append(cg.compute_Pi(None, u, v, None, g, plan.kernel, plan.scale, filter_plan=plan))
+    for o in out[1:]:
+        assert rel_l2(o, out[0]) < 1e-13
+
+
+def test_autotune_is_a_no_op_off_the_banded_engine():
+    g = S.cartesian_grid(n=64)
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 8e3)
+    assert plan.engine == "separable"
+    assert plan.autotune() == 0.0
