@@ -35,6 +35,7 @@ EXPORTED = [
     "cgef_closure_create", "cgef_closure_destroy", "cgef_closure_get_params", "cgef_closure_set_params",
     "cgef_closure_pairs_device", "cgef_closure_train_device", "cgef_closure_forward_device",
     "cgef_closure_grad_device", "cgef_closure_pi_device", "cgef_plan_autotune", "cgef_plan_set_split_waves",
+    "cgef_sweep_graph_create", "cgef_graph_launch", "cgef_graph_destroy",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE = 0, 1, 2, 3, 4, 5
 CLOSURE_NPARAM = 8899
@@ -138,6 +139,12 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_profile_read.argtypes = [i32, C.POINTER(dbl), C.POINTER(i64)]
     L.cgef_profile_read.restype = i32
     L.cgef_profile_reset.restype = None
+    L.cgef_sweep_graph_create.argtypes = [C.POINTER(vp), vp, i32, i32, vp, vp, i64, vp, vp, vp, vp]
+    L.cgef_sweep_graph_create.restype = i32
+    L.cgef_graph_launch.argtypes = [vp, vp]
+    L.cgef_graph_launch.restype = i32
+    L.cgef_graph_destroy.argtypes = [vp]
+    L.cgef_graph_destroy.restype = i32
     L.cgef_plan_autotune.argtypes = [vp, i32, C.POINTER(dbl)]
     L.cgef_plan_autotune.restype = i32
     L.cgef_plan_set_split_waves.argtypes = [vp, dbl]

@@ -734,6 +734,76 @@ int32_t cgef_sweep_device(cgef_plan* const* plans, int32_t nscales, int32_t dtyp
   return sweep_device(plans, nscales, dtype, u, v, nbatch, slice_masks, pi, energy, static_cast<cudaStream_t>(stream));
 }
 
+}  // extern "C"
+
+struct cgef_graph {
+  int device = -1;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t kernels = 0;
+};
+
+extern "C" {
+
+int32_t cgef_sweep_graph_create(cgef_graph** out, cgef_plan* const* plans, int32_t nscales, int32_t dtype,
+                                const void* u, const void* v, int64_t nbatch, const uint8_t* slice_masks, void* pi,
+                                double* energy, void* stream) {
+  if (!out) return fail(CGEF_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!plans || nscales < 1 || !plans[0]) return fail(CGEF_EINVAL, "need at least one plan");
+  int rc = check_plan(plans[0]);
+  if (rc) return rc;
+  DeviceGuard dg(plans[0]->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (st == nullptr) return fail(CGEF_EINVAL, "capture needs a created stream, not the legacy default stream");
+  // a first run sizes every workspace, so the captured call allocates nothing
+  if ((rc = sweep_device(plans, nscales, dtype, u, v, nbatch, slice_masks, pi, energy, st))) return rc;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "sweep before capture");
+  cgef_graph* g = new (std::nothrow) cgef_graph();
+  if (!g) return fail(CGEF_ENOMEM, "graph allocation failed");
+  g->device = plans[0]->device;
+  prof_suspend(true);
+  const int64_t before = g_launches;
+  e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = sweep_device(plans, nscales, dtype, u, v, nbatch, slice_masks, pi, energy, st);
+    cudaError_t e2 = cudaStreamEndCapture(st, &g->graph);
+    if (rc == CGEF_OK && e2 != cudaSuccess) rc = cuda_fail(e2, "cudaStreamEndCapture");
+  } else {
+    rc = cuda_fail(e, "cudaStreamBeginCapture");
+  }
+  prof_suspend(false);
+  g->kernels = g_launches - before;
+  g_launches = before;
+  if (rc == CGEF_OK && (e = cudaGraphInstantiate(&g->exec, g->graph, 0)) != cudaSuccess)
+    rc = cuda_fail(e, "cudaGraphInstantiate");
+  if (rc) {
+    cgef_graph_destroy(g);
+    return rc;
+  }
+  *out = g;
+  return CGEF_OK;
+}
+
+int32_t cgef_graph_launch(cgef_graph* g, void* stream) {
+  if (!g || !g->exec) return fail(CGEF_EINVAL, "graph is NULL");
+  DeviceGuard dg(g->device);
+  cudaError_t e = cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+  count_launch(g->kernels);
+  return CGEF_OK;
+}
+
+int32_t cgef_graph_destroy(cgef_graph* g) {
+  if (!g) return CGEF_OK;
+  DeviceGuard dg(g->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return CGEF_OK;
+}
+
 int32_t cgef_sweep(cgef_plan* const* plans, int32_t nscales, int32_t dtype, const void* u, const void* v,
                    int64_t nbatch, const uint8_t* slice_masks, void* pi, double* energy) {
   if (!plans || nscales < 1 || !plans[0]) return fail(CGEF_EINVAL, "need at least one plan");

@@ -180,6 +180,20 @@ int32_t cgef_compute_pi_device(cgef_plan* plan, int32_t dtype, const void* u, co
 int32_t cgef_sweep_device(cgef_plan* const* plans, int32_t nscales, int32_t dtype, const void* u, const void* v,
                           int64_t nbatch, const uint8_t* slice_masks, void* pi, double* energy, void* stream);
 
+/* A captured sweep: one cgef_sweep_device call recorded as a CUDA graph and replayed.  No
+ * counterpart in the reference (its GPU driver launches per scale).  `create` runs the sweep once on
+ * `stream` (sizing every workspace), then captures the same call; each `launch` replays it on the
+ * given stream, reading u, v and the masks and writing pi and energy at the captured addresses.  The
+ * plans' device tables and workspaces are baked into the graph: keep the plans alive, unchanged
+ * (no autotune or other calls on them in between) and unused by other streams while the graph is
+ * replayed. */
+typedef struct cgef_graph cgef_graph;
+int32_t cgef_sweep_graph_create(cgef_graph** out, cgef_plan* const* plans, int32_t nscales, int32_t dtype,
+                                const void* u, const void* v, int64_t nbatch, const uint8_t* slice_masks, void* pi,
+                                double* energy, void* stream);
+int32_t cgef_graph_launch(cgef_graph* graph, void* stream);
+int32_t cgef_graph_destroy(cgef_graph* graph);
+
 /* cgef_filter_device without any device allocation.  No counterpart in the reference.
  * For callers that cannot let a library allocate device memory during a call: a host whose device
  * memory is owned by its own pool allocator (a Julia or PyTorch caching allocator, which a library

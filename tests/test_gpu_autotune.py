@@ -46,3 +46,42 @@ def test_autotune_is_a_no_op_off_the_banded_engine():
     plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 8e3)
     assert plan.engine == "separable"
     assert plan.autotune() == 0.0
+
+
+def test_captured_sweep_graph_replays_the_eager_sweep_exactly(case):
+    import ctypes as C
+
+    import torch
+
+    from cgef_b200 import _lib
+    g, u, v = case
+    L = _lib.load()
+    plans = [cg.plan_filter(g, cg.GaussianKernel(4.0), s) for s in (2e5, 6e5)]
+    du = torch.from_numpy(np.stack([u, -u])).cuda()
+    dv = torch.from_numpy(np.stack([v, 0.5 * v])).cuda()
+    parr = (C.c_void_p * 2)(*[p.handle.value for p in plans])
+    st = torch.cuda.Stream()
+    Pi = torch.empty((2, 2) + g.shape, dtype=torch.float64, device="cuda")
+    E = torch.empty((2, 2), dtype=torch.float64, device="cuda")
+    _lib.check(L.cgef_sweep_device(parr, 2, _lib.F64, du.data_ptr(), dv.data_ptr(), 2, None, Pi.data_ptr(),
+                                   E.data_ptr(), st.cuda_stream))
+    torch.cuda.synchronize()
+    eager_pi, eager_e = Pi.clone(), E.clone()
+    Pi.zero_()
+    E.zero_()
+    gh = C.c_void_p()
+    _lib.check(L.cgef_sweep_graph_create(C.byref(gh), parr, 2, _lib.F64, du.data_ptr(), dv.data_ptr(), 2, None,
+                                         Pi.data_ptr(), E.data_ptr(), st.cuda_stream))
+    Pi.zero_()
+    E.zero_()
+    torch.cuda.synchronize()
+    L.cgef_reset_launch_count()
+    _lib.check(L.cgef_graph_launch(gh, st.cuda_stream))
+    torch.cuda.synchronize()
+    assert L.cgef_launch_count() > 0
+    _lib.check(L.cgef_graph_destroy(gh))
+    assert torch.equal(Pi, eager_pi) and torch.equal(E, eager_e)
+    # the null (legacy) stream cannot be captured: refused, not attempted
+    with pytest.raises(cg.CgefError):
+        _lib.check(L.cgef_sweep_graph_create(C.byref(gh), parr, 2, _lib.F64, du.data_ptr(), dv.data_ptr(), 2, None,
+                                             Pi.data_ptr(), E.data_ptr(), None))
