@@ -7,8 +7,9 @@ shape (ny, nx) -- the reference's column-major (Nx, Ny) -- or CUDA tensors of th
 """
 from ._lib import CgefError, device_count, library_path, load
 from .diagnostics import (AbstractSpectrumPolicy, ForceSpectrum, NoSpectrum, StrictSpectrum, active_area,
-                          compute_Pi, compute_Pi_fields, compute_Π, cumulative_energy, ddx, ddy,
-                          filtering_spectrum, gate_spectrum, spectral_density)
+                          compute_Pi, compute_Pi_fields, compute_Pi_strain_convergence, compute_Π,
+                          compute_Π_strain_convergence, cumulative_energy, ddx, ddy, filtering_spectrum,
+                          gate_spectrum, spectral_density, tau_decomposition)
 from .errors import ArgumentError, DimensionMismatch
 from .filtering import (AbstractMaskStrategy, Deformable, PhysicalFilterPlan, ZeroFill, filter_apply,
                         filter_apply_batch, filter_apply_batched, filter_field, filter_fields, plan_filter)

@@ -35,7 +35,8 @@ EXPORTED = [
     "cgef_closure_create", "cgef_closure_destroy", "cgef_closure_get_params", "cgef_closure_set_params",
     "cgef_closure_pairs_device", "cgef_closure_train_device", "cgef_closure_forward_device",
     "cgef_closure_grad_device", "cgef_closure_pi_device", "cgef_plan_autotune", "cgef_plan_set_split_waves",
-    "cgef_sweep_graph_create", "cgef_graph_launch", "cgef_graph_destroy",
+    "cgef_sweep_graph_create", "cgef_graph_launch", "cgef_graph_destroy", "cgef_tau_decomposition",
+    "cgef_tau_decomposition_device", "cgef_pi_strain_convergence", "cgef_pi_strain_convergence_device",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE = 0, 1, 2, 3, 4, 5
 CLOSURE_NPARAM = 8899
@@ -70,6 +71,14 @@ class AdamW(C.Structure):
 class ClosureReport(C.Structure):
     _fields_ = [("judged_tiles", C.c_int64), ("failed_tiles", C.c_int64), ("est_rel_l2", C.c_double),
                 ("fallbacks", C.c_int32), ("reserved", C.c_int32)]
+
+
+class TauParts(C.Structure):
+    _fields_ = [("leonard", C.c_void_p * 3), ("cross", C.c_void_p * 3), ("reynolds", C.c_void_p * 3)]
+
+
+class StrainConvOutputs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("total", "strain", "convergence", "divergence", "strain_magnitude")]
 
 
 class CgefError(RuntimeError):
@@ -139,6 +148,14 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_profile_read.argtypes = [i32, C.POINTER(dbl), C.POINTER(i64)]
     L.cgef_profile_read.restype = i32
     L.cgef_profile_reset.restype = None
+    L.cgef_tau_decomposition.argtypes = [vp, i32, vp, vp, C.POINTER(TauParts)]
+    L.cgef_tau_decomposition.restype = i32
+    L.cgef_tau_decomposition_device.argtypes = [vp, i32, vp, vp, C.POINTER(TauParts), vp]
+    L.cgef_tau_decomposition_device.restype = i32
+    L.cgef_pi_strain_convergence.argtypes = [vp, i32, vp, vp, i64, C.POINTER(StrainConvOutputs)]
+    L.cgef_pi_strain_convergence.restype = i32
+    L.cgef_pi_strain_convergence_device.argtypes = [vp, i32, vp, vp, i64, vp, C.POINTER(StrainConvOutputs), vp]
+    L.cgef_pi_strain_convergence_device.restype = i32
     L.cgef_sweep_graph_create.argtypes = [C.POINTER(vp), vp, i32, i32, vp, vp, i64, vp, vp, vp, vp]
     L.cgef_sweep_graph_create.restype = i32
     L.cgef_graph_launch.argtypes = [vp, vp]

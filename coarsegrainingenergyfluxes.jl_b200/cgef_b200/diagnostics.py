@@ -226,6 +226,70 @@ def filtering_spectrum(u, v, w, grid: StructuredGrid, kernel: AbstractFilterKern
 
 
 # ------------------------------------------------------------------------------------------
+# Decompositions (Diagnostics.jl:1350-1527, 1724-1852)
+# ------------------------------------------------------------------------------------------
+def tau_decomposition(u, v, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
+                      mask_strategy: AbstractMaskStrategy = ZeroFill(),
+                      filter_plan: Optional[PhysicalFilterPlan] = None) -> Dict[str, Dict[str, object]]:
+    """Diagnostics.tau_decomposition (Diagnostics.jl:1350-1527): tau = Leonard + Cross + Reynolds with
+    generalized central moments (Germano 1992).  Returns {"L": {"xx", "xy", "yy"}, "C": ..., "R": ...};
+    on the sphere the components are east-east, east-north, north-north."""
+    if tuple(u.shape) != grid.shape or tuple(v.shape) != grid.shape:
+        raise DimensionMismatch(f"u and v must have the grid's shape {grid.shape}")
+    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy)
+    dt = A.dtype_code(u)
+    if A.dtype_code(v) != dt:
+        raise ArgumentError("u and v must share a dtype")
+    outs = {part: {c: A.empty_like(u) for c in ("xx", "xy", "yy")} for part in ("L", "C", "R")}
+    tp = _lib.TauParts()
+    for field, part in (("leonard", "L"), ("cross", "C"), ("reynolds", "R")):
+        arr = getattr(tp, field)
+        for k, c in enumerate(("xx", "xy", "yy")):
+            arr[k] = A.ptr(outs[part][c])
+    L = _lib.load()
+    if A.is_device(u):
+        _lib.check(L.cgef_tau_decomposition_device(plan.handle, dt, A.ptr(u.contiguous()), A.ptr(v.contiguous()),
+                                                   C.byref(tp), A.stream_of(u)))
+    else:
+        _lib.check(L.cgef_tau_decomposition(plan.handle, dt, A.ptr(np.ascontiguousarray(u)),
+                                            A.ptr(np.ascontiguousarray(v)), C.byref(tp)))
+    return outs
+
+
+def compute_Pi_strain_convergence(u, v, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
+                                  mask_strategy: AbstractMaskStrategy = ZeroFill(),
+                                  filter_plan: Optional[PhysicalFilterPlan] = None) -> Dict[str, object]:
+    """Diagnostics.compute_Π_strain_convergence (Diagnostics.jl:1724-1852): the flux split into
+    deformation (`strain`) and convergence production, Pi = strain - convergence, with the two
+    rotation invariants `divergence` and `strain_magnitude`.  Cartesian grids only, as in the
+    reference; u, v may carry leading batch axes."""
+    if grid.is_spherical:
+        raise ArgumentError("compute_Pi_strain_convergence is defined for Cartesian grids only")
+    bs = _batch_shape(u, grid, "u")
+    if _batch_shape(v, grid, "v") != bs:
+        raise DimensionMismatch("v's batch axes do not match u's")
+    nb = _nbatch(bs)
+    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy)
+    dt = A.dtype_code(u)
+    if A.dtype_code(v) != dt:
+        raise ArgumentError("u and v must share a dtype")
+    names = ("total", "strain", "convergence", "divergence", "strain_magnitude")
+    outs = {n: A.empty_like(u) for n in names}
+    so = _lib.StrainConvOutputs(*[A.ptr(outs[n]) for n in names])
+    L = _lib.load()
+    if A.is_device(u):
+        _lib.check(L.cgef_pi_strain_convergence_device(plan.handle, dt, A.ptr(u.contiguous()), A.ptr(v.contiguous()),
+                                                       nb, None, C.byref(so), A.stream_of(u)))
+    else:
+        _lib.check(L.cgef_pi_strain_convergence(plan.handle, dt, A.ptr(np.ascontiguousarray(u)),
+                                                A.ptr(np.ascontiguousarray(v)), nb, C.byref(so)))
+    return outs
+
+
+compute_Π_strain_convergence = compute_Pi_strain_convergence
+
+
+# ------------------------------------------------------------------------------------------
 # Derivatives.jl
 # ------------------------------------------------------------------------------------------
 def _deriv(axis_fn: str, out, f, grid_or_plan):

@@ -233,10 +233,6 @@ int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int
   return launch_strain(p, sa, st);
 }
 
-}  // namespace cgef
-
-namespace {
-
 // Filters nf (<= 4 per pass) fields; outputs FP64 planes (slice stride `ostride`).
 int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int nf, double* const* outs,
                          int64_t ostride, int nbatch, const uint8_t* mask, int64_t mstride, cudaStream_t st) {
@@ -276,6 +272,10 @@ int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int
     return rc;
   return launch_prefix(p, kModeFields, nf, pl, pitch, np, nbatch, mask, mstride, static_cast<double*>(pre), go, st);
 }
+
+}  // namespace cgef
+
+namespace {
 
 // One field with a trailing batch axis: device in/out of the caller's dtype.
 int filter_device(cgef_plan* p, int dtype, const void* field, void* out, int64_t nbatch64, cudaStream_t st) {

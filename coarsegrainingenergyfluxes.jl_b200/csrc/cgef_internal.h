@@ -138,7 +138,7 @@ struct cgef_plan {
   cgef::PrefixRow* d_prows = nullptr;  // ny * nb
   // execution
   cudaStream_t stream = nullptr;
-  cgef::DeviceBuffer ws[10];  // workspace slots, grown on demand
+  cgef::DeviceBuffer ws[12];  // workspace slots (cgef::WsSlot), grown on demand
 };
 
 namespace cgef {
@@ -279,6 +279,9 @@ struct StrainArgs {
   double grad_scale;
   double* grad_partials;
   double* grad_mean;
+  // strain / convergence split (plane; outputs of dtype, out_slice_stride): total, strain,
+  // convergence, divergence, strain magnitude.  nullptr = skip.
+  void* sc[5];
 };
 
 int launch_strain(const cgef_plan* p, const StrainArgs& a, cudaStream_t st);
@@ -309,6 +312,8 @@ enum WsSlot {
   kSlotDeriv = 7,
   kSlotSplit = 8,
   kSlotVel = 9,
+  kSlotDecomp = 10,
+  kNumSlots = 12,
 };
 
 struct DeviceGuard {
@@ -338,5 +343,9 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
               int64_t mstride, double* gather, cudaStream_t st);
 int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int64_t nbatch64,
                       const uint8_t* slice_masks, const cgef_pi_outputs* out, cudaStream_t st);
+// Filters nf (<= 4) fields of dtype through the plan's engine into FP64 planes outs[m] (slice stride
+// `ostride`).
+int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int nf, double* const* outs,
+                         int64_t ostride, int nbatch, const uint8_t* mask, int64_t mstride, cudaStream_t st);
 
 }  // namespace cgef

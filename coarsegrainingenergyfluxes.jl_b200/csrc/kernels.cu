@@ -700,6 +700,8 @@ struct StrainK {
   int64_t grad_stride;
   double grad_scale;
   double* gpartials;  // [slice][block][2]: sum of |grad|^2 and active count
+  // strain / convergence split of the flux (plane): total, strain, convergence, divergence, |strain|
+  void* sc[5];
 };
 
 constexpr int kStrainBX = 32, kStrainBY = 8;
@@ -786,6 +788,21 @@ __global__ void strain_kernel(StrainK a) {
     if (a.sxx_o) store_any(a.sxx_o, a.dtype, o, sxx);
     if (a.sxy_o) store_any(a.sxy_o, a.dtype, o, sxy);
     if (a.syy_o) store_any(a.syy_o, a.dtype, o, syy);
+    if (a.sc[0] || a.sc[1] || a.sc[2] || a.sc[3] || a.sc[4]) {
+      // Diagnostics.jl:1757-1769 (Srinivasan, Barkan & McWilliams 2023, eq. 10)
+      double d = 0.0, al = 0.0, pa = 0.0, pd = 0.0;
+      if (act) {
+        const double ux = sxx, vy = syy, uy = g1, vx = g2;
+        d = ux + vy;
+        al = sqrt((ux - vy) * (ux - vy) + (uy + vx) * (uy + vx));
+        pa = (tyy - txx) * (ux - vy) / 2.0 - txy * (uy + vx);
+        pd = (tyy + txx) * (ux + vy) / 2.0;
+      }
+      const double vals[5] = {pa - pd, pa, pd, d, al};
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        if (a.sc[k]) store_any(a.sc[k], a.dtype, o, vals[k]);
+    }
     if (a.grad) {
       const double g[4] = {a.grad_scale * sxx, a.grad_scale * g1, a.grad_scale * g2, a.grad_scale * syy};
       float* gp = a.grad + s * a.grad_stride + pix;
@@ -1215,6 +1232,7 @@ int launch_strain(const cgef_plan* p, const StrainArgs& s, cudaStream_t st) {
   a.grad_stride = s.grad_slice_stride;
   a.grad_scale = s.grad_scale;
   a.gpartials = s.grad_mean ? s.grad_partials : nullptr;
+  for (int k = 0; k < 5; ++k) a.sc[k] = s.sc[k];
   dim3 block(kStrainBX, kStrainBY), grid((p->nx + kStrainBX - 1) / kStrainBX, (p->ny + kStrainBY - 1) / kStrainBY,
                                          s.nbatch);
   prof_begin(CGEF_KERNEL_STRAIN, st);

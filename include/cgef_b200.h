@@ -207,6 +207,40 @@ int32_t cgef_graph_destroy(cgef_graph* graph);
 int32_t cgef_filter_device_noalloc(cgef_plan* plan, int32_t dtype, const void* field, void* out, int64_t nbatch,
                                    void* stream);
 
+/* Diagnostics.tau_decomposition (Diagnostics.jl:1350-1527): tau = Leonard + Cross + Reynolds with
+ * generalized central moments M(f, g) = (fg)bar - fbar gbar of ubar and u' = u - ubar (Germano 1992);
+ * on the sphere the moments are formed from planetary Cartesian components and each part is rotated
+ * to east/north.  One (ny, nx) field pair; each part has xx, xy, yy outputs (ny*nx values of dtype;
+ * NULL skips one).  Masked cells give 0. */
+typedef struct cgef_tau_parts {
+  void* leonard[3];
+  void* cross[3];
+  void* reynolds[3];
+} cgef_tau_parts;
+int32_t cgef_tau_decomposition(cgef_plan* plan, int32_t dtype, const void* u, const void* v,
+                               const cgef_tau_parts* out);
+int32_t cgef_tau_decomposition_device(cgef_plan* plan, int32_t dtype, const void* u, const void* v,
+                                      const cgef_tau_parts* out, void* stream);
+
+/* Diagnostics.compute_Π_strain_convergence! (Diagnostics.jl:1724-1852; Srinivasan, Barkan &
+ * McWilliams 2023, eq. 10), Cartesian grids: with delta = u_x + v_y, sigma_n = u_x - v_y,
+ * sigma_s = u_y + v_x of the filtered velocity, Pi_alpha = (tau_vv - tau_uu) sigma_n / 2 - tau_uv sigma_s,
+ * Pi_delta = (tau_vv + tau_uu) delta / 2, total = Pi_alpha - Pi_delta (= compute_Π!'s Pi),
+ * strain_magnitude = sqrt(sigma_n^2 + sigma_s^2).  Batched like cgef_compute_pi; NULL skips an
+ * output.  CGEF_EUNSUPPORTED on the sphere (the reference defines it on the plane only). */
+typedef struct cgef_strain_conv_outputs {
+  void* total;
+  void* strain;
+  void* convergence;
+  void* divergence;
+  void* strain_magnitude;
+} cgef_strain_conv_outputs;
+int32_t cgef_pi_strain_convergence(cgef_plan* plan, int32_t dtype, const void* u, const void* v, int64_t nbatch,
+                                   const cgef_strain_conv_outputs* out);
+int32_t cgef_pi_strain_convergence_device(cgef_plan* plan, int32_t dtype, const void* u, const void* v,
+                                          int64_t nbatch, const uint8_t* slice_masks,
+                                          const cgef_strain_conv_outputs* out, void* stream);
+
 /* ---- Learned closure.  No counterpart in the reference. ----
  * A pointwise MLP (5 -> 64 -> 64 -> 64 -> 3, GELU) maps the filtered velocity-gradient tensor,
  * scaled by ell^2, and log ell to the subfilter stress tau; the flux is then -S:tau with S from the
