@@ -123,6 +123,35 @@ def test_compute_pi_sphere_banded_matches_oracle(strat):
     _pi_parity(g, cg.GaussianKernel(4.0), 5e5, u, v, strat)
 
 
+@pytest.mark.parametrize("strat", [cg.ZeroFill(), cg.Deformable()])
+def test_compute_pi_sphere_banded_alpha6_matches_oracle(strat):
+    # the narrower Gaussian (Kernels.jl:59-62, radius 1.959 l)
+    g = sphere2(seed=6)
+    u, v = S.sphere_fields(g, seed=17, lmax=89)
+    _pi_parity(g, cg.GaussianKernel(6.0), 7e5, u, v, strat)
+
+
+@pytest.mark.parametrize("strat", [cg.ZeroFill(), cg.Deformable()])
+def test_compute_pi_cartesian_alpha6_matches_oracle(strat):
+    n = 96
+    u, v = S.cartesian_fields(n=n, seed=4)
+    m = np.ones((n, n), bool)
+    m[20:40, 30:70] = False
+    g = S.cartesian_grid(n, 1000.0, (True, False), m)
+    _pi_parity(g, cg.GaussianKernel(6.0), 7000.0, u, v, strat)
+
+
+def test_filter_alpha6_batched_matches_oracle():
+    g = sphere2(seed=9)
+    rng = np.random.default_rng(6)
+    f = rng.standard_normal((3,) + g.shape)
+    p = cg.plan_filter(g, cg.GaussianKernel(6.0), 9e5)
+    got = cg.filter_apply_batched(None, f, p)
+    op = oracle_plan(g, cg.GaussianKernel(6.0), 9e5)
+    for t in range(3):
+        assert max_rel(got[t], op.filter(f[t])) < FIELD_TOL
+
+
 def test_compute_pi_sphere_tophat_matches_oracle():
     g = sphere2()
     u, v = S.sphere_fields(g, seed=8, lmax=89)
