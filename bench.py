@@ -353,6 +353,26 @@ def run_closure(args, rank, world, local, dist):
     msk = g.mask
     raw_err = [float(np.linalg.norm((cPi[s].cpu().numpy() - exact[s])[msk]) / np.linalg.norm(exact[s][msk]))
                for s in range(ns)]
+    # the classical nonlinear gradient model on the same snapshot, for comparison: for a Gaussian of
+    # second moment l^2 / (2 alpha), tau_ij = l^2 / (2 alpha) A_ik A_jk with A the filtered velocity
+    # gradient (curvature terms included); in the closure's normalised units y = x x^T / (2 alpha).
+    # Also with its coefficient fitted by least squares to this snapshot's exact tau (an upper bound
+    # on what the model can do).
+    ngm_err, ngm_fit_err = [], []
+    mflat = torch.from_numpy(msk.reshape(-1)).cuda()
+    for s_, p in enumerate(plans):
+        f, t = CL.training_pairs(p, du, dv)
+        x, y = f[0].double(), t[0].double()
+        yn = torch.stack([x[0] ** 2 + x[1] ** 2, x[0] * x[2] + x[1] * x[3], x[2] ** 2 + x[3] ** 2])
+        # Pi from normalised quantities: S = (x0, (x1 + x2)/2, x3) n / l^2, tau = y n^2 / l^2, so
+        # Pi is proportional to -(x0 y0 + (x1 + x2) y1 + x3 y2) with one positive factor per slice
+        pi_of = lambda yy: -(x[0] * yy[0] + (x[1] + x[2]) * yy[1] + x[3] * yy[2])
+        ex = pi_of(y)[mflat]
+        ng = pi_of(yn)[mflat]
+        c_th = 1.0 / (2.0 * wl["kernel"].alpha)
+        c_fit = float((ng * ex).sum() / (ng * ng).sum())
+        ngm_err.append(float(torch.linalg.norm(c_th * ng - ex) / torch.linalg.norm(ex)))
+        ngm_fit_err.append(float(torch.linalg.norm(c_fit * ng - ex) / torch.linalg.norm(ex)))
     closure_step(0)
     torch.cuda.synchronize()
     judged_err = [float(np.linalg.norm((cPi[s].cpu().numpy() - exact[s])[msk]) / np.linalg.norm(exact[s][msk]))
@@ -474,6 +494,7 @@ def run_closure(args, rank, world, local, dist):
                         "no_fallback_speedup_vs_plain": (world * units * steps / (ms_open / 1e3)) / plain_value,
                         "no_fallback_est_rel_l2": [r.est_rel_l2 for r in reports_open],
                         "pi_rel_l2_raw": raw_err, "pi_rel_l2_judged": judged_err,
+                        "gradient_model_pi_rel_l2": ngm_err, "gradient_model_fitted_pi_rel_l2": ngm_fit_err,
                         "est_rel_l2_judge": [r.est_rel_l2 for r in reports],
                         "scales_km": [s / 1e3 for s in scales],
                         "training": {"points": 10_000_000, "batch": batch, "steps": int(nsteps),
