@@ -335,10 +335,8 @@ int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u,
     // the sweep's planes carry the widest halo; run each plan against them
     const int saveH = q->H;
     q->H = halo;
-    if (q->engine != CGEF_ENGINE_BANDED && q != p0) {
-      // separable/prefix scratch of the plan itself
-    }
-    rc = pi_gather(q == p0 ? p0 : q, planes, pitch, halo, np, nbatch, mask, mstride, g, st);
+    // each plan runs its engine with its own scratch (split partials, separable rows, prefix sums)
+    rc = pi_gather(q, planes, pitch, halo, np, nbatch, mask, mstride, g, st);
     q->H = saveH;
     if (rc) return rc;
     StrainArgs sa{};
