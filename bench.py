@@ -269,6 +269,20 @@ def oracle_rate(wl, budget_s: float):
     return rate, nthreads, len(timed), spent, sample
 
 
+def device_steps_ms(run, steps, stream, flush) -> float:
+    """Device time of `steps` steps: an L2 flush (a write larger than L2) before each step, and a pair of
+    CUDA events on the launch stream around each step alone; returns the summed milliseconds."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.fill_(1.0)
+        ev[k][0].record(stream)
+        run(k)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return float(sum(a.elapsed_time(b) for a, b in ev))
+
+
 def mlp_flops_per_point() -> float:
     """Multiply-adds x 2 of the closure MLP per point, unpadded (5-64-64-64-3)."""
     return 2.0 * (5 * 64 + 64 * 64 + 64 * 64 + 64 * 3)
@@ -388,14 +402,7 @@ def run_closure(args, rank, world, local, dist):
             L.cgef_reset_launch_count()
             L.cgef_profile_reset()
             L.cgef_profile_enable(1)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for k in range(steps):
-            flush.fill_(1.0)
-            fn(k + 100)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
+        return device_steps_ms(lambda k: fn(k + 100), steps, stream, flush)
 
     steps = args.steps or 3
     sampler = ClockSampler(local)
@@ -485,7 +492,7 @@ def run_closure(args, rank, world, local, dist):
             "vs_baseline": None, "dtype": "f64 flux, bf16 closure (fp32 accumulate)", "data": "synthetic (seeded)",
             "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": 1,
                        "judge_fraction": 0.02, "tol": args.closure_tol, "schedule_split_waves": waves,
-                       "l2": "flushed between steps (256 MiB write, inside the timed region)",
+                       "l2": "flushed between steps (a 256 MiB write before every step, outside the step's own events)",
                        "parallelism": f"{world} rank(s), independent snapshots per rank"},
             "closure": {"plain_value": plain_value, "plain_ms_per_step": ms_plain / steps,
                         "speedup_vs_plain": value / plain_value, "fallback_slices_per_step": fallbacks,
@@ -602,19 +609,11 @@ def main():
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        flush.fill_(1.0)
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
+    elapsed_ms = device_steps_ms(lambda k: step(), steps, stream, flush)
     if dist is not None:
         dist.barrier()
     L.cgef_profile_enable(0)
     launches = int(L.cgef_launch_count())
-    elapsed_ms = e0.elapsed_time(e1)
 
     # the same step replayed from a captured CUDA graph (cgef_sweep_graph_create / cgef_graph_launch)
     graph_line = None
@@ -632,16 +631,8 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     L.cgef_reset_launch_count()
-    g0 = torch.cuda.Event(enable_timing=True)
-    g1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(gs):
-        g0.record(gs)
-        for _ in range(steps):
-            flush.fill_(1.0)
-            _lib.check(L.cgef_graph_launch(gh, gs.cuda_stream))
-        g1.record(gs)
-    torch.cuda.synchronize()
-    graph_ms = g0.elapsed_time(g1)
+        graph_ms = device_steps_ms(lambda k: _lib.check(L.cgef_graph_launch(gh, gs.cuda_stream)), steps, gs, flush)
     graph_launches = int(L.cgef_launch_count())
     _lib.check(L.cgef_graph_destroy(gh))
     if dist is not None:
@@ -722,10 +713,45 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             el = float(t.item())
         bsz = 4 if tdt == torch.float32 else 8
+        e2e_sync = {"value": world * units_per_step * n_e2e / el, "unit": UNIT,
+                    "h2d_bytes_per_step": int(2 * nsl * g.nx * g.ny * bsz + (0 if hm is None else hm.numel())),
+                    "d2h_bytes_per_step": int(nsl * ns * g.nx * g.ny * bsz + nsl * ns * 8), "steps": n_e2e,
+                    "timing": "wall clock around synchronous cgef_sweep calls (host buffers, pinned)"}
+
+        # the same steps streamed through cgef_pipeline_*: every step still copies its u, v in and its Pi
+        # and E out, but a step's copies overlap its neighbours' sweeps (double-buffered device memory)
+        ph = C.c_void_p()
+        _lib.check(L.cgef_pipeline_create(C.byref(ph), parr, ns, dt_code, nsl, None if hm is None else hm.data_ptr(),
+                                          1))
+        outs = [(torch.empty_like(hPi).pin_memory(), torch.empty_like(hE).pin_memory()) for _ in range(2)]
+
+        def submit(k):
+            pi_k, e_k = outs[k % 2]
+            _lib.check(L.cgef_pipeline_submit(ph, hu.data_ptr(), hv.data_ptr(), pi_k.data_ptr(), e_k.data_ptr()))
+
+        submit(0)
+        submit(1)
+        _lib.check(L.cgef_pipeline_drain(ph))
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for k in range(n_e2e):
+            submit(k)
+        _lib.check(L.cgef_pipeline_drain(ph))
+        el = time.perf_counter() - t0
+        _lib.check(L.cgef_pipeline_destroy(ph))
+        if dist is not None:
+            t = torch.tensor([el], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
         e2e = {"value": world * units_per_step * n_e2e / el, "unit": UNIT,
-               "h2d_bytes_per_step": int(2 * nsl * g.nx * g.ny * bsz + (0 if hm is None else hm.numel())),
+               "h2d_bytes_per_step": int(2 * nsl * g.nx * g.ny * bsz),
                "d2h_bytes_per_step": int(nsl * ns * g.nx * g.ny * bsz + nsl * ns * 8), "steps": n_e2e,
-               "timing": "wall clock around synchronous cgef_sweep calls (host buffers, pinned)"}
+               "timing": "wall clock from the first cgef_pipeline_submit to cgef_pipeline_drain: pinned u, v "
+                         "copied in and Pi, E copied out for every step, overlapping the neighbouring steps' "
+                         "sweeps (the per-level masks, if any, are copied once at create); no L2 flush: "
+                         "each step's inputs arrive by H2D",
+               "synchronous": e2e_sync}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -743,7 +769,7 @@ def main():
             "dtype": "f64" if wl["dtype"] == "f64" else "f64 (f32 storage)", "data": "synthetic (seeded)",
             "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": nsl,
                        "active_fraction": float(1.0 if g.mask is None else g.mask.mean()),
-                       "l2": "flushed between steps (256 MiB write, inside the timed region)",
+                       "l2": "flushed between steps (a 256 MiB write before every step, outside the step's own events)",
                        "parallelism": f"{world} rank(s), independent snapshots per rank",
                        "schedule_split_waves": waves},
             "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,

@@ -17,6 +17,6 @@ from .grids import Axis, CartesianGeometry, SphericalGeometry, StructuredGrid, a
 from .kernels import (GaussianKernel, TopHatKernel, check_spectrum_kernel, kernel_radius, kernel_weight,
                       transfer_monotone)
 from .pipeline import (CoarseGrainBatchResult, CoarseGrainResult, coarse_grain, coarse_grain_batch,
-                       coarse_grain_profile, coarse_grain_slices)
+                       coarse_grain_profile, coarse_grain_slices, SnapshotStream)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

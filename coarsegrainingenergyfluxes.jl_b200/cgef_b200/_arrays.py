@@ -26,9 +26,9 @@ def dtype_code(a) -> int:
 
 
 def ptr(a) -> int:
-    if is_device(a):
+    if is_device(a) or hasattr(a, "data_ptr"):  # CUDA tensors, and host (e.g. pinned) torch tensors
         if not a.is_contiguous():
-            raise ValueError("device tensors must be contiguous")
+            raise ValueError("tensors must be contiguous")
         return a.data_ptr()
     if not a.flags["C_CONTIGUOUS"]:
         raise ValueError("host arrays must be C-contiguous ((ny, nx) with x fastest)")

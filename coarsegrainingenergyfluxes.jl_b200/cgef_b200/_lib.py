@@ -37,6 +37,7 @@ EXPORTED = [
     "cgef_closure_grad_device", "cgef_closure_pi_device", "cgef_plan_autotune", "cgef_plan_set_split_waves",
     "cgef_sweep_graph_create", "cgef_graph_launch", "cgef_graph_destroy", "cgef_tau_decomposition",
     "cgef_tau_decomposition_device", "cgef_pi_strain_convergence", "cgef_pi_strain_convergence_device",
+    "cgef_pipeline_create", "cgef_pipeline_submit", "cgef_pipeline_drain", "cgef_pipeline_destroy",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE = 0, 1, 2, 3, 4, 5
 CLOSURE_NPARAM = 8899
@@ -148,6 +149,12 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_profile_read.argtypes = [i32, C.POINTER(dbl), C.POINTER(i64)]
     L.cgef_profile_read.restype = i32
     L.cgef_profile_reset.restype = None
+    L.cgef_pipeline_create.argtypes = [C.POINTER(vp), vp, i32, i32, i64, vp, i32]
+    L.cgef_pipeline_submit.argtypes = [vp, vp, vp, vp, vp]
+    L.cgef_pipeline_drain.argtypes = [vp]
+    L.cgef_pipeline_destroy.argtypes = [vp]
+    for n in ("create", "submit", "drain", "destroy"):
+        getattr(L, "cgef_pipeline_" + n).restype = i32
     L.cgef_tau_decomposition.argtypes = [vp, i32, vp, vp, C.POINTER(TauParts)]
     L.cgef_tau_decomposition.restype = i32
     L.cgef_tau_decomposition_device.argtypes = [vp, i32, vp, vp, C.POINTER(TauParts), vp]

@@ -187,3 +187,71 @@ def coarse_grain_slices(us: Sequence, vs: Sequence, grids: Sequence[StructuredGr
         for q, t in enumerate(g):
             results[t] = CoarseGrainResult(scales.copy(), Pi[q], E[q], k, _spectrum(E[q], k, spectrum))
     return results  # type: ignore[return-value]
+
+
+class SnapshotStream:
+    """A time series of snapshots streamed through a sweep (`cgef_pipeline_*`): every `submit` copies
+    one snapshot's u, v in, sweeps it over the plans' scales and copies its Pi (nbatch, nscales, ny, nx)
+    and E (nbatch, nscales) out, while neighbouring snapshots' copies and sweeps overlap on the GPU.
+    Host buffers must stay alive and untouched until `drain()`; they overlap the GPU's work only when
+    pinned (e.g. torch tensors from `.pin_memory()`)."""
+
+    def __init__(self, plans: Sequence[PhysicalFilterPlan], *, nbatch: int = 1, dtype=np.float64,
+                 slice_masks=None, want_pi: bool = True):
+        if not plans:
+            raise ArgumentError("need at least one plan")
+        self.plans = list(plans)
+        self.grid = plans[0].grid
+        self.nbatch = int(nbatch)
+        self.dtype = np.dtype(dtype)
+        self.want_pi = bool(want_pi)
+        code = _lib.F32 if self.dtype == np.float32 else _lib.F64
+        if self.dtype not in (np.float32, np.float64):
+            raise ArgumentError("dtype must be float32 or float64")
+        m = None if slice_masks is None else np.ascontiguousarray(slice_masks, dtype=np.uint8)
+        if m is not None and m.size != self.nbatch * self.grid.nx * self.grid.ny:
+            raise DimensionMismatch("slice_masks must hold one (ny, nx) mask per slice")
+        self._keep = []
+        arr = (C.c_void_p * len(self.plans))(*[p.handle.value for p in self.plans])
+        self._h = C.c_void_p()
+        _lib.check(_lib.load().cgef_pipeline_create(C.byref(self._h), arr, len(self.plans), code, self.nbatch,
+                                                    None if m is None else m.ctypes.data, int(self.want_pi)))
+
+    def _shape_ok(self, a, shape, name, itemsize=None):
+        if tuple(a.shape) != shape:
+            raise DimensionMismatch(f"{name} must have shape {shape}")
+        if A.is_device(a):
+            raise ArgumentError(f"{name} must be host memory")
+        size = a.element_size() if hasattr(a, "element_size") else a.itemsize
+        if size != (self.dtype.itemsize if itemsize is None else itemsize):
+            raise ArgumentError(f"{name} has the wrong element type")
+
+    def submit(self, u, v, pi=None, energy=None) -> None:
+        ny, nx = self.grid.shape
+        fs = (self.nbatch, ny, nx)
+        self._shape_ok(u, fs, "u")
+        self._shape_ok(v, fs, "v")
+        if self.want_pi:
+            if pi is None:
+                raise ArgumentError("this stream returns Pi: pass a (nbatch, nscales, ny, nx) buffer")
+            self._shape_ok(pi, (self.nbatch, len(self.plans), ny, nx), "pi")
+        if energy is not None:
+            self._shape_ok(energy, (self.nbatch, len(self.plans)), "energy", itemsize=8)
+        self._keep.append((u, v, pi, energy))
+        _lib.check(_lib.load().cgef_pipeline_submit(self._h, A.ptr(u), A.ptr(v), None if pi is None else A.ptr(pi),
+                                                    None if energy is None else A.ptr(energy)))
+
+    def drain(self) -> None:
+        _lib.check(_lib.load().cgef_pipeline_drain(self._h))
+        self._keep.clear()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value and _lib._lib is not None:
+            _lib._lib.cgef_pipeline_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -300,6 +300,10 @@ int filter_device(cgef_plan* p, int dtype, const void* field, void* out, int64_t
   return CGEF_OK;
 }
 
+}  // namespace
+
+namespace cgef {
+
 int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u, const void* v, int64_t nbatch64,
                  const uint8_t* slice_masks, void* pi, double* energy, cudaStream_t st) {
   int rc;
@@ -361,6 +365,10 @@ int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u,
   }
   return CGEF_OK;
 }
+
+}  // namespace cgef
+
+namespace {
 
 int h2d(cgef_plan* p, int slot, const void* src, size_t bytes, void** dst) {
   int rc = ensure_ws(p, slot, bytes, dst);

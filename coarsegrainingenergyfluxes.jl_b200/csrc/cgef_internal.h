@@ -343,6 +343,10 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
               int64_t mstride, double* gather, cudaStream_t st);
 int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int64_t nbatch64,
                       const uint8_t* slice_masks, const cgef_pi_outputs* out, cudaStream_t st);
+// The sweep over plans (one grid) for nbatch slices on stream st: Pi [nbatch][nscales][N] (dtype) and
+// E [nbatch][nscales], either may be nullptr.
+int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u, const void* v, int64_t nbatch64,
+                 const uint8_t* slice_masks, void* pi, double* energy, cudaStream_t st);
 // Filters nf (<= 4) fields of dtype through the plan's engine into FP64 planes outs[m] (slice stride
 // `ostride`).
 int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int nf, double* const* outs,

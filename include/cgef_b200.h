@@ -194,6 +194,23 @@ int32_t cgef_sweep_graph_create(cgef_graph** out, cgef_plan* const* plans, int32
 int32_t cgef_graph_launch(cgef_graph* graph, void* stream);
 int32_t cgef_graph_destroy(cgef_graph* graph);
 
+/* Streaming sweep: the snapshots of a time series submitted one after another from host memory,
+ * each copied in, swept over the plans (as cgef_sweep) and its Pi and E copied out, with a
+ * snapshot's copies overlapping its neighbours' sweeps (double-buffered device memory, three
+ * streams).  The synchronous reference driver loops over snapshots one call at a time
+ * (Pipeline.jl:519-563, 686-717); this is that loop with the transfers off the critical path.
+ * `submit` returns once the step is queued: u, v (nbatch*ny*nx of dtype), pi (nbatch*nscales*ny*nx,
+ * required when the pipeline was created with want_pi) and energy (nbatch*nscales doubles, may be
+ * NULL) must stay valid and untouched until `drain` returns; they overlap the GPU's work only when
+ * they are pinned host memory.  slice_masks (host, copied at create) as in cgef_sweep.  The plans
+ * are used by the pipeline's streams: make no other call on them before `drain`. */
+typedef struct cgef_pipeline cgef_pipeline;
+int32_t cgef_pipeline_create(cgef_pipeline** out, cgef_plan* const* plans, int32_t nscales, int32_t dtype,
+                             int64_t nbatch, const uint8_t* slice_masks, int32_t want_pi);
+int32_t cgef_pipeline_submit(cgef_pipeline* pipeline, const void* u, const void* v, void* pi, double* energy);
+int32_t cgef_pipeline_drain(cgef_pipeline* pipeline);
+int32_t cgef_pipeline_destroy(cgef_pipeline* pipeline);
+
 /* cgef_filter_device without any device allocation.  No counterpart in the reference.
  * For callers that cannot let a library allocate device memory during a call: a host whose device
  * memory is owned by its own pool allocator (a Julia or PyTorch caching allocator, which a library
