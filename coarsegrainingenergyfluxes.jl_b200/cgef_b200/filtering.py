@@ -108,6 +108,16 @@ class PhysicalFilterPlan:
         self.split_waves = w.value
         return w.value
 
+    def set_filter_rows(self, rows: int) -> None:
+        """Tile height (4 or 8 target rows per thread) of the banded engine's filter passes."""
+        _lib.check(_lib.load().cgef_plan_set_filter_rows(self.handle, int(rows)))
+
+    def schedule(self):
+        """(split granularity of the flux gather, tile height of the filter passes)."""
+        w, r = C.c_double(), C.c_int32()
+        _lib.check(_lib.load().cgef_plan_get_schedule(self.handle, C.byref(w), C.byref(r)))
+        return w.value, r.value
+
     def set_split_waves(self, waves: float) -> None:
         """Sets the banded schedule's split granularity (rounds of resident warps per SM)."""
         _lib.check(_lib.load().cgef_plan_set_split_waves(self.handle, float(waves)))

@@ -136,7 +136,7 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
   if (p->engine == CGEF_ENGINE_BANDED) {
     const int na = (mode == kModePiSphere ? 9 : 5) + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
     void* part = nullptr;
-    const size_t pb = banded_partials_bytes(p, na, nbatch);
+    const size_t pb = banded_partials_bytes(p, na, nbatch, mode);
     if (pb > 0) {
       int rc = ensure_ws(p, kSlotSplit, pb, &part);
       if (rc) return rc;
@@ -257,7 +257,7 @@ int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int
   double* pl = static_cast<double*>(planes);
   if (p->engine == CGEF_ENGINE_BANDED) {
     void* part = nullptr;
-    const size_t pb = banded_partials_bytes(p, nf + (def ? 1 : 0), nbatch);
+    const size_t pb = banded_partials_bytes(p, nf + (def ? 1 : 0), nbatch, kModeFields);
     if (pb > 0 && (rc = ensure_ws(p, kSlotSplit, pb, &part))) return rc;
     return launch_banded(p, kModeFields, nf, pl, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st);
   }
@@ -499,8 +499,9 @@ int32_t cgef_plan_destroy(cgef_plan* p) {
   if (p->device >= 0) {
     DeviceGuard dg(p->device);
     void* ptrs[] = {p->d_mask, p->d_x, p->d_sinlam, p->d_coslam, p->d_sinphi, p->d_cosphi, p->d_area, p->d_xscale,
-                    p->d_tanfac, p->d_rows, p->d_w, p->d_den_zf, p->d_items, p->d_groups, p->d_gx, p->d_gy, p->d_px,
-                    p->d_py, p->d_xe, p->d_prefix_wx, p->d_prows};
+                    p->d_tanfac, p->d_rows, p->d_w, p->d_den_zf, p->sched[0].d_items, p->sched[0].d_groups,
+                    p->sched[1].d_items, p->sched[1].d_groups, p->d_gx, p->d_gy, p->d_px, p->d_py, p->d_xe,
+                    p->d_prefix_wx, p->d_prows};
     for (void* q : ptrs)
       if (q) cudaFree(q);
     for (auto& b : p->ws)
@@ -529,7 +530,27 @@ int32_t cgef_plan_set_split_waves(cgef_plan* p, double waves) {
   if (!(waves > 0.0 && waves <= 1024.0)) return fail(CGEF_EINVAL, "waves must be in (0, 1024]");
   if (p->engine != CGEF_ENGINE_BANDED) return CGEF_OK;
   DeviceGuard dg(p->device);
-  return rebuild_schedule(p, waves);
+  int rc2 = rebuild_schedule(p, waves, 0);
+  if (rc2 == CGEF_OK && p->sched[1].rows) rc2 = rebuild_schedule(p, waves, 1);
+  return rc2;
+}
+
+int32_t cgef_plan_set_filter_rows(cgef_plan* p, int32_t rows) {
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (rows != kRows && rows != kRowsTall) return fail(CGEF_EINVAL, "filter tile height must be 4 or 8 rows");
+  if (p->engine != CGEF_ENGINE_BANDED) return CGEF_OK;
+  DeviceGuard dg(p->device);
+  if (rows == kRowsTall && p->sched[1].rows == 0 && (rc = rebuild_schedule(p, p->sched[0].waves, 1))) return rc;
+  p->filter_rows = rows;
+  return CGEF_OK;
+}
+
+int32_t cgef_plan_get_schedule(const cgef_plan* p, double* waves, int32_t* filter_rows) {
+  if (!p) return fail(CGEF_EINVAL, "plan is NULL");
+  if (waves) *waves = p->engine == CGEF_ENGINE_BANDED ? p->sched[0].waves : 0.0;
+  if (filter_rows) *filter_rows = p->engine == CGEF_ENGINE_BANDED ? p->filter_rows : 0;
+  return CGEF_OK;
 }
 
 int32_t cgef_plan_autotune(cgef_plan* p, int32_t nbatch, double* chosen) {
@@ -560,40 +581,62 @@ int32_t cgef_plan_autotune(cgef_plan* p, int32_t nbatch, double* chosen) {
     cudaEventDestroy(e0);
     return cuda_fail(e, "autotune events");
   }
-  const double cand[4] = {2.0, 4.0, 8.0, 16.0};
-  double best = p->split_waves, best_ms = 1e300;
-  for (double w : cand) {
-    if ((rc = rebuild_schedule(p, w))) break;
-    // one untimed pass (partials workspace, caches), then the timed passes
-    if ((rc = pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0, static_cast<double*>(gather), st))) break;
-    // timed passes: three, or one when a pass takes more than 20 ms
+  // mean device time of `pass`: one untimed pass (workspaces, caches), then three timed ones, or one
+  // when a pass takes more than 20 ms
+  auto time_pass = [&](auto pass, double* ms_out) -> int {
+    int r = pass();
+    if (r) return r;
     double ms = 0.0;
     int done = 0;
     while (done < 3) {
       cudaEventRecord(e0, st);
-      rc = pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0, static_cast<double*>(gather), st);
+      if ((r = pass())) return r;
       cudaEventRecord(e1, st);
-      if (rc) break;
       float one = 0.f;
-      if ((e = cudaEventSynchronize(e1)) != cudaSuccess || (e = cudaEventElapsedTime(&one, e0, e1)) != cudaSuccess) {
-        rc = cuda_fail(e, "autotune timing");
-        break;
-      }
+      cudaError_t ee;
+      if ((ee = cudaEventSynchronize(e1)) != cudaSuccess || (ee = cudaEventElapsedTime(&one, e0, e1)) != cudaSuccess)
+        return cuda_fail(ee, "autotune timing");
       ms += one;
       ++done;
       if (one > 20.0f) break;
     }
-    if (rc) break;
-    ms /= done;
+    *ms_out = ms / done;
+    return CGEF_OK;
+  };
+  // 1. split granularity of the flux gather's schedule
+  const double cand[4] = {2.0, 4.0, 8.0, 16.0};
+  double best = p->sched[0].waves, best_ms = 1e300;
+  for (double w : cand) {
+    double ms = 0.0;
+    if ((rc = rebuild_schedule(p, w, 0))) break;
+    if ((rc = time_pass([&] { return pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0,
+                                               static_cast<double*>(gather), st); },
+                        &ms)))
+      break;
     if (ms < best_ms) {
       best_ms = ms;
       best = w;
     }
   }
+  if (rc == CGEF_OK) rc = rebuild_schedule(p, best, 0);
+  // 2. tile height of the filter passes (timed on a three-field pass: the velocity gather)
+  if (rc == CGEF_OK) rc = rebuild_schedule(p, best, 1);
+  if (rc == CGEF_OK) {
+    const void* f[3] = {zin, zin, zin};
+    double* G = static_cast<double*>(gather);
+    double* o[3] = {G, G + N, G + 2 * N};
+    double ms_r[2] = {0.0, 0.0};
+    const int heights[2] = {kRows, kRowsTall};
+    for (int k = 0; k < 2 && rc == CGEF_OK; ++k) {
+      p->filter_rows = heights[k];
+      rc = time_pass([&] { return filter_fields_device(p, CGEF_F64, f, 3, o, 5 * N, nbatch, p->d_mask, 0, st); },
+                     &ms_r[k]);
+    }
+    p->filter_rows = (rc == CGEF_OK && ms_r[1] < ms_r[0]) ? kRowsTall : kRows;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  if ((rc = rebuild_schedule(p, best))) return rc;
   if (chosen) *chosen = best;
   return CGEF_OK;
 }

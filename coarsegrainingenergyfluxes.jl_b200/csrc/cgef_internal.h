@@ -22,8 +22,10 @@ constexpr double kGaussianTruncationTol = 1e-10;
 #ifndef CGEF_WARPS
 #define CGEF_WARPS 4
 #endif
-// Target rows carried by one thread of the banded gather (register tile height).
+// Target rows carried by one thread of the banded gather (register tile height): the flux's, and
+// the taller tile the schedule autotuner may choose for filters of up to four fields.
 constexpr int kRows = CGEF_ROWS;
+constexpr int kRowsTall = 2 * CGEF_ROWS;
 // Warps per CTA of the banded gather; every warp works on its own item.
 constexpr int kWarps = CGEF_WARPS;
 // Width of the staged planes' column tiling (the pitch is padded to a multiple of this).
@@ -60,6 +62,18 @@ struct SplitGroup {
   int32_t j0;
   int32_t slot0;
   int32_t nslots;
+};
+
+// A work-item schedule of the banded gather for one tile height `rows` (rows == 0: not built).
+struct Schedule {
+  int rows = 0;
+  std::vector<std::vector<double>> rowcost;  // per target group, per source row (cost model)
+  double waves = 4.0;                        // split granularity (rounds of resident warps)
+  std::vector<WorkItem> h_items;
+  WorkItem* d_items = nullptr;
+  std::vector<SplitGroup> h_groups;
+  SplitGroup* d_groups = nullptr;
+  int nslots = 0;
 };
 
 // Per (target row j, source row slot b) of the prefix-sum top-hat sweep (Filtering.jl:974-1097).
@@ -117,13 +131,8 @@ struct cgef_plan {
   double* d_w = nullptr;            // weights, half rows
   double* d_den_zf = nullptr;       // ZeroFill denominator: ny (periodic x) or ny*nx
   int den_zf_2d = 0;
-  std::vector<std::vector<double>> h_rowcost;  // per target group, per source row (schedule cost model)
-  double split_waves = 4.0;                    // schedule granularity (rounds of resident warps)
-  std::vector<cgef::WorkItem> h_items;
-  cgef::WorkItem* d_items = nullptr;
-  std::vector<cgef::SplitGroup> h_groups;
-  cgef::SplitGroup* d_groups = nullptr;
-  int nslots = 0;
+  cgef::Schedule sched[2];  // [0]: kRows-row tiles (every mode), [1]: kRowsTall rows (filters, when built)
+  int filter_rows = CGEF_ROWS;  // tile height of the filter passes (kModeFields)
   // separable engine
   int di_lim = 0, sep_dj_lim = 0;
   double* d_gx = nullptr;
@@ -153,18 +162,24 @@ double kernel_radius(int kernel, double alpha, double ell);
 // Host plan construction (plan_build.cpp).
 int build_plan_tables(cgef_plan* p);
 
-// Banded schedule pieces.  Source-row costs of the kRows-row target group starting at j0: for each
-// source row in [j0 - D, j0 + kRows - 1 + D], the width of the union of the group's intervals plus a
+// Banded schedule pieces.  Source-row costs of the R-row target group starting at j0: for each
+// source row in [j0 - D, j0 + R - 1 + D], the width of the union of the group's intervals plus a
 // per-row overhead (0 where the row is outside a bounded grid or holds no entries).
-std::vector<double> group_row_costs(const cgef_plan* p, int j0);
+std::vector<double> group_row_costs(const cgef_plan* p, int j0, int R = kRows);
 // Appends the work items of target group (x0, j0): one item when its cost is within `target`,
 // otherwise contiguous source-row parts of about `target` cost plus their split group (slots
 // numbered from `slots`, which advances).
 void emit_group_items(int x0, int j0, int D, const std::vector<double>& rc, double target,
                       std::vector<WorkItem>& items, std::vector<SplitGroup>& groups, int& slots);
-// Rebuilds and uploads the plan's work-item schedule, split so that the banded gather runs in
-// about `waves` rounds of 16 resident warps per SM (the autotuner's knob).
-int rebuild_schedule(cgef_plan* p, double waves);
+// Builds (or rebuilds) and uploads schedule `which` of the plan (0: kRows rows, 1: kRowsTall rows),
+// split so that the banded gather runs in about `waves` rounds of 16 resident warps per SM.
+int rebuild_schedule(cgef_plan* p, double waves, int which = 0);
+// Accumulated quantities up to which the taller tile keeps its accumulators in registers.
+constexpr int kTallMaxQuantities = 3;
+// The schedule a launch of `mode` with `na` accumulated quantities uses: the flux modes always the
+// kRows one; a filter pass of at most kTallMaxQuantities quantities the taller one when the plan
+// chose it and it is built.
+inline const Schedule& schedule_for(const cgef_plan* p, int mode, int na);
 // A schedule for the 32 x 32 tiles (tx, ty) only, split so that it fills `sms` SMs in one wave;
 // slots are numbered from 0.
 void subset_schedule(const cgef_plan* p, const std::vector<std::pair<int, int>>& tiles, int sms,
@@ -231,10 +246,11 @@ int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* plan
                         const uint8_t* mask, int64_t mask_slice_stride, double* partials, const WorkItem* items,
                         int nitems, const SplitGroup* groups, int ngroups, const GatherOut& out, cudaStream_t st);
 
-// Bytes of partial-sum scratch a banded launch of `na` accumulated quantities over `nbatch`
-// slices needs.
-inline size_t banded_partials_bytes(const cgef_plan* p, int na, int nbatch) {
-  return sizeof(double) * static_cast<size_t>(p->nslots) * nbatch * kRows * na * 32;
+// Bytes of partial-sum scratch a banded launch of `mode` with `na` accumulated quantities over
+// `nbatch` slices needs.
+inline size_t banded_partials_bytes(const cgef_plan* p, int na, int nbatch, int mode) {
+  const Schedule& s = schedule_for(p, mode, na);
+  return sizeof(double) * static_cast<size_t>(s.nslots) * nbatch * s.rows * na * 32;
 }
 
 int launch_separable(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
@@ -351,5 +367,11 @@ int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u,
 // `ostride`).
 int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int nf, double* const* outs,
                          int64_t ostride, int nbatch, const uint8_t* mask, int64_t mstride, cudaStream_t st);
+
+inline const Schedule& schedule_for(const cgef_plan* p, int mode, int na) {
+  if (mode == kModeFields && na <= kTallMaxQuantities && p->filter_rows == kRowsTall && p->sched[1].rows == kRowsTall)
+    return p->sched[1];
+  return p->sched[0];
+}
 
 }  // namespace cgef

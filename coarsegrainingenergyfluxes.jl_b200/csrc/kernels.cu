@@ -255,11 +255,11 @@ __device__ __forceinline__ void finish_target(const BandedK& a, const double (&a
 // the kRows rows' weights (zero outside each row's own interval) in its own shared-memory slab,
 // then every lane streams its three (or K) staged values along the row and applies the kRows
 // weights to all accumulated quantities with FP64 FMA.  Warps never wait for one another.
-template <int MODE, int NF, bool DEF>
+template <int MODE, int NF, bool DEF, int R>
 __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(BandedK a) {
   using C = Cfg<MODE, NF, DEF>;
-  __shared__ double wbuf[kWarps][kRows][32];
-  __shared__ int rint[kWarps][3][kRows];  // per warp: a, hi, woff of the kRows rows for the current source row
+  __shared__ double wbuf[kWarps][R][32];
+  __shared__ int rint[kWarps][3][R];  // per warp: a, hi, woff of the R rows for the current source row
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int64_t gid = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
@@ -270,9 +270,9 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
   const int col = it.x0 + lane;
   const int j0 = it.j0;
 
-  double acc[kRows][C::NA];
+  double acc[R][C::NA];
 #pragma unroll
-  for (int t = 0; t < kRows; ++t)
+  for (int t = 0; t < R; ++t)
 #pragma unroll
     for (int m = 0; m < C::NA; ++m) acc[t][m] = 0.0;
 
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
   bool any_act = false;
   if (col < a.nx) {
 #pragma unroll
-    for (int t = 0; t < kRows; ++t) {
+    for (int t = 0; t < R; ++t) {
       const int j = j0 + t;
       if (j < a.ny)
         any_act |= a.mask == nullptr || a.mask[slice * a.mask_stride + static_cast<int64_t>(j) * a.nx + col] != 0;
@@ -296,8 +296,8 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
       if (!a.periodic_y) continue;
       jj = wrap(jr, a.ny);
     }
-    // lanes 0..kRows-1 fetch the rows' intervals into the warp's slab
-    if (lane < kRows) {
+    // lanes 0..R-1 fetch the rows' intervals into the warp's slab
+    if (lane < R) {
       int ra = -1, rhi = -1, roff = 0;
       const int j = j0 + lane;
       const int dj = jr - j;
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
     __syncwarp();
     int A = -1, HI = -1;
 #pragma unroll
-    for (int t = 0; t < kRows; ++t) {
+    for (int t = 0; t < R; ++t) {
       A = max(A, rint[warp][0][t]);
       HI = max(HI, rint[warp][1][t]);
     }
@@ -325,15 +325,15 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
     const double* src = base + static_cast<int64_t>(jj) * a.pitch;
     for (int c0 = -A; c0 <= HI; c0 += 32) {
       const int k = c0 + lane;
-      double wv[kRows];
+      double wv[R];
 #pragma unroll
-      for (int t = 0; t < kRows; ++t) {
+      for (int t = 0; t < R; ++t) {
         const int at = rint[warp][0][t];
         wv[t] = (at >= 0 && k >= -at && k <= rint[warp][1][t]) ? __ldg(a.w + rint[warp][2][t] + abs(k)) : 0.0;
       }
       __syncwarp();
 #pragma unroll
-      for (int t = 0; t < kRows; ++t) wb[t * 32 + lane] = wv[t];
+      for (int t = 0; t < R; ++t) wb[t * 32 + lane] = wv[t];
       __syncwarp();
       const int cn = min(32, HI - c0 + 1);
       const double* s = src + c0;
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
         double q[C::NA];
         expand<MODE, NF, DEF>(v, q);
 #pragma unroll
-        for (int t = 0; t < kRows; ++t) {
+        for (int t = 0; t < R; ++t) {
           const double wt = wb[t * 32 + kk];
 #pragma unroll
           for (int m = 0; m < C::NA; ++m) acc[t][m] = fma(wt, q[m], acc[t][m]);
@@ -357,16 +357,16 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
 
   if (it.slot >= 0) {
     // partial sums of a split tile: [slot][slice][t][m][lane]
-    double* pp = a.partials + ((static_cast<int64_t>(it.slot) * a.nslices + slice) * kRows * C::NA) * 32 + lane;
+    double* pp = a.partials + ((static_cast<int64_t>(it.slot) * a.nslices + slice) * R * C::NA) * 32 + lane;
 #pragma unroll
-    for (int t = 0; t < kRows; ++t)
+    for (int t = 0; t < R; ++t)
 #pragma unroll
       for (int m = 0; m < C::NA; ++m) pp[(t * C::NA + m) * 32] = acc[t][m];
     return;
   }
   if (col >= a.nx) return;
 #pragma unroll
-  for (int t = 0; t < kRows; ++t) {
+  for (int t = 0; t < R; ++t) {
     const int j = j0 + t;
     if (j >= a.ny) break;
     finish_target<MODE, NF, DEF>(a, acc[t], slice, j, col);
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
 }
 
 // Adds the partial slots of every split tile in slot order (deterministic) and finishes it.
-template <int MODE, int NF, bool DEF>
+template <int MODE, int NF, bool DEF, int R>
 __global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
   using C = Cfg<MODE, NF, DEF>;
   const int lane = threadIdx.x & 31;
@@ -386,14 +386,14 @@ __global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
   const int col = g.x0 + lane;
   if (col >= a.nx) return;
   double acc[C::NA];
-  for (int t = 0; t < kRows; ++t) {
+  for (int t = 0; t < R; ++t) {
     const int j = g.j0 + t;
     if (j >= a.ny) break;
 #pragma unroll
     for (int m = 0; m < C::NA; ++m) acc[m] = 0.0;
     for (int q = 0; q < g.nslots; ++q) {
       const double* pp =
-          a.partials + ((static_cast<int64_t>(g.slot0 + q) * a.nslices + slice) * kRows * C::NA + t * C::NA) * 32 + lane;
+          a.partials + ((static_cast<int64_t>(g.slot0 + q) * a.nslices + slice) * R * C::NA + t * C::NA) * 32 + lane;
 #pragma unroll
       for (int m = 0; m < C::NA; ++m) acc[m] += pp[m * 32];
     }
@@ -989,25 +989,33 @@ int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* plane
 
 namespace {
 
-template <int MODE, int NF, bool DEF>
+template <int MODE, int NF, bool DEF, int R>
 int run_banded(const BandedK& a, cudaStream_t st) {
   const int64_t warps = static_cast<int64_t>(a.nitems) * a.nslices;
   const unsigned blocks = static_cast<unsigned>((warps + kWarps - 1) / kWarps);
   prof_begin(CGEF_KERNEL_BANDED, st);
-  banded_kernel<MODE, NF, DEF><<<blocks, 32 * kWarps, 0, st>>>(a);
+  banded_kernel<MODE, NF, DEF, R><<<blocks, 32 * kWarps, 0, st>>>(a);
   int rc = check_launch("banded_kernel");
   if (rc == CGEF_OK && a.ngroups > 0) {
     const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices;
-    banded_combine_kernel<MODE, NF, DEF><<<static_cast<unsigned>((cw + 3) / 4), 128, 0, st>>>(a);
+    banded_combine_kernel<MODE, NF, DEF, R><<<static_cast<unsigned>((cw + 3) / 4), 128, 0, st>>>(a);
     rc = check_launch("banded_combine_kernel");
   }
   prof_end(CGEF_KERNEL_BANDED, st);
   return rc;
 }
 
+// The flux modes run kRows-row tiles only (taller tiles spill their accumulators); the filter
+// passes also have kRowsTall-row tiles.
 template <int MODE, int NF>
-int dispatch_banded(bool def, const BandedK& a, cudaStream_t st) {
-  return def ? run_banded<MODE, NF, true>(a, st) : run_banded<MODE, NF, false>(a, st);
+int dispatch_banded(bool def, int R, const BandedK& a, cudaStream_t st) {
+  if constexpr (MODE == kModeFields && NF + 1 <= kTallMaxQuantities) {
+    if (R == kRowsTall)
+      return def ? run_banded<MODE, NF, true, kRowsTall>(a, st) : run_banded<MODE, NF, false, kRowsTall>(a, st);
+  } else if constexpr (MODE == kModeFields && NF <= kTallMaxQuantities) {
+    if (R == kRowsTall && !def) return run_banded<MODE, NF, false, kRowsTall>(a, st);
+  }
+  return def ? run_banded<MODE, NF, true, kRows>(a, st) : run_banded<MODE, NF, false, kRows>(a, st);
 }
 
 }  // namespace
@@ -1033,11 +1041,14 @@ int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* plan
   a.band_stride = p->geometry == CGEF_SPHERICAL ? 2 * p->D + 1 : 0;
   a.w = p->d_w;
   a.D = p->D;
-  a.items = items ? items : p->d_items;
-  a.nitems = items ? nitems : static_cast<int>(p->h_items.size());
+  const int na = (mode == kModePiSphere ? 9 : (mode == kModePiCart ? 5 : nf)) + (def ? 1 : 0);
+  const Schedule& S = schedule_for(p, mode, na);
+  const int R = items ? kRows : S.rows;
+  a.items = items ? items : S.d_items;
+  a.nitems = items ? nitems : static_cast<int>(S.h_items.size());
   a.nslices = nbatch;
-  a.groups = items ? groups : p->d_groups;
-  a.ngroups = items ? ngroups : static_cast<int>(p->h_groups.size());
+  a.groups = items ? groups : S.d_groups;
+  a.ngroups = items ? ngroups : static_cast<int>(S.h_groups.size());
   if (a.nitems == 0) return CGEF_OK;
   a.partials = partials;
   if (a.ngroups > 0 && partials == nullptr) return fail(CGEF_EINVAL, "banded: split tiles need a partials buffer");
@@ -1055,13 +1066,13 @@ int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* plan
   a.cosphi = sph ? p->d_cosphi : nullptr;
   for (int m = 0; m < 9; ++m) a.out[m] = out.o[m];
   a.out_stride = out.slice_stride;
-  if (mode == kModePiSphere) return dispatch_banded<kModePiSphere, 1>(def, a, st);
-  if (mode == kModePiCart) return dispatch_banded<kModePiCart, 1>(def, a, st);
+  if (mode == kModePiSphere) return dispatch_banded<kModePiSphere, 1>(def, R, a, st);
+  if (mode == kModePiCart) return dispatch_banded<kModePiCart, 1>(def, R, a, st);
   switch (nf) {
-    case 1: return dispatch_banded<kModeFields, 1>(def, a, st);
-    case 2: return dispatch_banded<kModeFields, 2>(def, a, st);
-    case 3: return dispatch_banded<kModeFields, 3>(def, a, st);
-    case 4: return dispatch_banded<kModeFields, 4>(def, a, st);
+    case 1: return dispatch_banded<kModeFields, 1>(def, R, a, st);
+    case 2: return dispatch_banded<kModeFields, 2>(def, R, a, st);
+    case 3: return dispatch_banded<kModeFields, 3>(def, R, a, st);
+    case 4: return dispatch_banded<kModeFields, 4>(def, R, a, st);
     default: return fail(CGEF_EINVAL, "banded: 1..4 fields per pass");
   }
 }

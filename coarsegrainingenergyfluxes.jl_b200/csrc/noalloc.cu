@@ -67,7 +67,7 @@ extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const
   if (p->engine == CGEF_ENGINE_SEPARABLE) engine_b = round256(sizeof(double) * 2 * static_cast<size_t>(N) * nbatch);
   if (p->engine == CGEF_ENGINE_PREFIXSUM)
     engine_b = round256(sizeof(double) * 2 * static_cast<size_t>(p->ny) * (p->pre_ne + 1) * nbatch);
-  if (p->engine == CGEF_ENGINE_BANDED) engine_b = round256(banded_partials_bytes(p, np, nbatch));
+  if (p->engine == CGEF_ENGINE_BANDED) engine_b = round256(banded_partials_bytes(p, np, nbatch, kModeFields));
   const size_t result_b = dtype == CGEF_F64 ? 0 : round256(sizeof(double) * static_cast<size_t>(N) * nbatch);
   const size_t need = planes_b + engine_b + result_b;
   if (need > kNoallocScratchBytes)

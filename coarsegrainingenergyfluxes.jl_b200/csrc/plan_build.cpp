@@ -225,16 +225,16 @@ void build_banded(const cgef_plan* p, Banded& B) {
 #define CGEF_SPLIT_WAVES 4.0
 #endif
 
-std::vector<double> group_row_costs(const cgef_plan* p, int j0) {
+std::vector<double> group_row_costs(const cgef_plan* p, int j0, int R) {
   const bool sphere = p->geometry == CGEF_SPHERICAL;
   const int W = 2 * p->D + 1;
   std::vector<double> rc;
-  rc.reserve(kRows + 2 * p->D);
-  for (int jr = j0 - p->D; jr <= j0 + kRows - 1 + p->D; ++jr) {
+  rc.reserve(R + 2 * p->D);
+  for (int jr = j0 - p->D; jr <= j0 + R - 1 + p->D; ++jr) {
     double c = 0.0;
     if (p->periodic_y || (jr >= 0 && jr < p->ny)) {
       int A = -1, HI = -1;
-      for (int t = 0; t < kRows; ++t) {
+      for (int t = 0; t < R; ++t) {
         const int j = j0 + t;
         if (j >= p->ny) continue;
         const int dj = jr - j;
@@ -306,13 +306,21 @@ void subset_schedule(const cgef_plan* p, const std::vector<std::pair<int, int>>&
   std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
 }
 
-int rebuild_schedule(cgef_plan* p, double waves) {
+int rebuild_schedule(cgef_plan* p, double waves, int which) {
   if (!(waves > 0.0)) return fail(CGEF_EINVAL, "split waves must be positive");
-  const int ngroups = static_cast<int>(p->h_rowcost.size());
+  if (which < 0 || which > 1) return fail(CGEF_EINVAL, "schedule index must be 0 or 1");
+  Schedule& S = p->sched[which];
+  const int R = which == 0 ? kRows : kRowsTall;
+  if (S.rowcost.empty()) {
+    const int ngroups = (p->ny + R - 1) / R;
+    S.rowcost.assign(ngroups, {});
+    parallel_for(ngroups, [&](int g) { S.rowcost[g] = group_row_costs(p, g * R, R); });
+  }
+  const int ngroups = static_cast<int>(S.rowcost.size());
   double total = 0.0;
   const int ntx = (p->nx + 31) / 32;
   for (int g = 0; g < ngroups; ++g)
-    for (double c : p->h_rowcost[g]) total += c * ntx;
+    for (double c : S.rowcost[g]) total += c * ntx;
   int sms = 148;
   {
     int dev = 0;
@@ -328,19 +336,20 @@ int rebuild_schedule(cgef_plan* p, double waves) {
   std::vector<SplitGroup> groups;
   int slots = 0;
   for (int g = 0; g < ngroups; ++g)
-    for (int x = 0; x < p->nx; x += 32) emit_group_items(x, g * kRows, p->D, p->h_rowcost[g], target, items, groups, slots);
+    for (int x = 0; x < p->nx; x += 32) emit_group_items(x, g * R, p->D, S.rowcost[g], target, items, groups, slots);
   std::stable_sort(items.begin(), items.end(), [](const WorkItem& a, const WorkItem& b) { return a.cost > b.cost; });
-  if (p->d_items) cudaFree(p->d_items);
-  if (p->d_groups) cudaFree(p->d_groups);
-  p->d_items = nullptr;
-  p->d_groups = nullptr;
-  p->h_items = std::move(items);
-  p->h_groups = std::move(groups);
-  p->nslots = slots;
-  p->split_waves = waves;
+  if (S.d_items) cudaFree(S.d_items);
+  if (S.d_groups) cudaFree(S.d_groups);
+  S.d_items = nullptr;
+  S.d_groups = nullptr;
+  S.h_items = std::move(items);
+  S.h_groups = std::move(groups);
+  S.nslots = slots;
+  S.waves = waves;
+  S.rows = R;
   int rc;
-  if ((rc = upload(p, &p->d_items, p->h_items.data(), p->h_items.size())) != CGEF_OK) return rc;
-  return upload(p, &p->d_groups, p->h_groups.data(), p->h_groups.size());
+  if ((rc = upload(p, &S.d_items, S.h_items.data(), S.h_items.size())) != CGEF_OK) return rc;
+  return upload(p, &S.d_groups, S.h_groups.data(), S.h_groups.size());
 }
 
 int build_plan_tables(cgef_plan* p) {
@@ -439,16 +448,13 @@ int build_plan_tables(cgef_plan* p) {
     (void)W;
     // Work items: one warp per (32 columns x kRows rows) tile; a tile whose source rows cost more
     // than a fair share is split along the source rows into partial items, longest first.
-    const int ngroups = (ny + kRows - 1) / kRows;
-    p->h_rowcost.assign(ngroups, {});
-    parallel_for(ngroups, [&](int g) { p->h_rowcost[g] = group_row_costs(p, g * kRows); });
     p->H = std::max(B.Amax, 1);
     int rc;
     if ((rc = upload(p, &p->d_rows, B.rows.data(), B.rows.size())) != CGEF_OK) return rc;
     if (B.w.empty()) B.w.push_back(0.0);
     if ((rc = upload(p, &p->d_w, B.w.data(), B.w.size())) != CGEF_OK) return rc;
     if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
-    if ((rc = rebuild_schedule(p, CGEF_SPLIT_WAVES)) != CGEF_OK) return rc;
+    if ((rc = rebuild_schedule(p, CGEF_SPLIT_WAVES, 0)) != CGEF_OK) return rc;
   } else if (p->engine == CGEF_ENGINE_SEPARABLE) {
     // Filtering.jl:1391-1463: square truncation, lim = ceil(rad / step), point-sampled profile.
     p->di_lim = p->dx > 0 ? static_cast<int>(std::ceil(p->rad / p->dx)) : 0;

@@ -127,12 +127,21 @@ int32_t cgef_plan_get_info(const cgef_plan* plan, cgef_plan_info* info);
  * schedule).  Times the flux gather on this plan's grid and mask (zero-valued inputs; the gather's
  * cost depends on the footprint and the mask, not on the values) for each candidate split
  * granularity -- the work-item schedule cut into about 2, 4, 8 or 16 rounds of resident warps per
- * SM -- and keeps the fastest; `chosen` (may be NULL) receives it.  A no-op for the separable and
+ * SM -- and keeps the fastest; `chosen` (may be NULL) receives it.  It then times a three-field
+ * filter pass with 4- and 8-row tiles and keeps the faster for the filter passes.  A no-op for the separable and
  * prefix engines.  Results stay within FP64 rounding of each other across schedules: only the
  * order in which a split tile's partial sums are added changes. */
 int32_t cgef_plan_autotune(cgef_plan* plan, int32_t nbatch, double* chosen);
 /* Sets the split granularity directly (rounds of resident warps per SM, > 0; the default is 4). */
 int32_t cgef_plan_set_split_waves(cgef_plan* plan, double waves);
+/* Tile height of the banded engine's filter passes (cgef_filter*, cumulative energy, the closure's and
+ * the decompositions' gathers): 4 or 8 target rows per thread (the flux always uses 4).  The autotuner
+ * also chooses it, timing a three-field pass.  Results are identical either way up to FP64 rounding of
+ * split tiles' partial sums. */
+int32_t cgef_plan_set_filter_rows(cgef_plan* plan, int32_t rows);
+/* The plan's current schedule: split granularity of the flux gather and the filters' tile height
+ * (both 0 off the banded engine). */
+int32_t cgef_plan_get_schedule(const cgef_plan* plan, double* waves, int32_t* filter_rows);
 
 /* Banded footprint of the plan in the reference's CSR form (FilterFootprint, Filtering.jl:327-336):
  * di/dj/w have nentries entries, ptr has nbands+1 (0-based offsets).  Any pointer may be NULL. */

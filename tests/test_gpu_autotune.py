@@ -85,3 +85,32 @@ def test_captured_sweep_graph_replays_the_eager_sweep_exactly(case):
     with pytest.raises(cg.CgefError):
         _lib.check(L.cgef_sweep_graph_create(C.byref(gh), parr, 2, _lib.F64, du.data_ptr(), dv.data_ptr(), 2, None,
                                              Pi.data_ptr(), E.data_ptr(), None))
+
+
+@pytest.mark.parametrize("strat", [cg.ZeroFill(), cg.Deformable()])
+def test_tall_filter_tiles_match_the_oracle(case, strat):
+    g, u, v = case
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 9e5, mask_strategy=strat)
+    op = oracle_plan(g, cg.GaussianKernel(4.0), 9e5, strat)
+    rng = np.random.default_rng(3)
+    fields = [rng.standard_normal(g.shape) for _ in range(4)]
+    ref = [op.filter(f) for f in fields]
+    for rows in (8, 4):
+        plan.set_filter_rows(rows)
+        assert plan.schedule()[1] == rows
+        # 1, 2, 3 and 4 fields per pass (3 with the mask and 4 fall back to 4-row tiles)
+        for k in (1, 2, 3, 4):
+            outs = cg.filter_apply_batch(None, fields[:k], plan)
+            for o, r in zip(outs, ref):
+                assert rel_l2(o, r) < 1e-10, (rows, k)
+        got = cg.filter_apply_batched(None, np.stack(fields[:3]), plan)
+        for t in range(3):
+            assert rel_l2(got[t], ref[t]) < 1e-10
+
+
+def test_autotune_reports_a_filter_tile_height(case):
+    g, _, _ = case
+    plan = cg.plan_filter(g, cg.GaussianKernel(4.0), 1.5e6)
+    plan.autotune()
+    w, rows = plan.schedule()
+    assert w in (2.0, 4.0, 8.0, 16.0) and rows in (4, 8)
