@@ -41,3 +41,18 @@ def test_stream_equals_the_synchronous_sweep():
     with pytest.raises(cg.ArgumentError):
         st.submit(u[None].astype(np.float32), v[None].astype(np.float32), pi)
     st.close()
+
+
+def test_sharded_sweep_on_one_rank_equals_the_batch_sweep():
+    """coarse_grain_sharded with no process group (one rank, one GPU) runs every unit itself and
+    assembles exactly the batch sweep's E and Pi."""
+    from cgef_b200 import sharding as SH
+    g = S.sphere_grid(144, 72)
+    g = g.with_mask(S.land_mask(g, seed=6))
+    scales = [3e5, 6e5, 1.2e6]
+    U, V = zip(*[S.sphere_fields(g, seed=60 + k, lmax=50) for k in range(3)])
+    U, V = np.stack(U), np.stack(V)
+    E, Pi = SH.coarse_grain_sharded(U, V, g, scales=scales, kernel=cg.GaussianKernel(4.0))
+    ref = cg.coarse_grain_batch(U, V, g, scales=scales, kernel=cg.GaussianKernel(4.0))
+    assert np.array_equal(E, ref.cumulative_energy)
+    assert np.array_equal(Pi, ref.Pi)
