@@ -191,3 +191,24 @@ def test_trained_closure_beats_the_untrained_one(torch):
     # than its untrained self at every scale
     assert all(e1 < 0.9 for e1 in errs1), errs1
     assert all(e1 < e0 for e0, e1 in zip(errs0, errs1)), (errs0, errs1)
+
+
+@pytest.mark.parametrize("case", ["sphere-tophat", "sphere-deformable", "plane-tophat"])
+def test_closure_paths_of_every_engine_fall_back_exactly(torch, case):
+    if case.startswith("sphere"):
+        g, u, v = _sphere_case(seed=13)
+        kern = cg.TopHatKernel() if case == "sphere-tophat" else cg.GaussianKernel(4.0)
+        strat = cg.Deformable() if case == "sphere-deformable" else cg.ZeroFill()
+        plan = cg.plan_filter(g, kern, 7e5, mask_strategy=strat)
+    else:
+        u, v = S.cartesian_fields(n=96, seed=5)
+        g = S.cartesian_grid(n=96)
+        plan = cg.plan_filter(g, cg.TopHatKernel(), 9e3)
+    assert plan.engine == ("prefixsum" if "tophat" in case else "banded")
+    ud, vd = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+    c = CL.Closure(seed=6)
+    raw, _ = c.pi(plan, ud, vd, judge_fraction=0.0)
+    assert torch.isfinite(raw).all()
+    pi, rep = c.pi(plan, ud, vd, judge_fraction=0.1, tol=1e-9)
+    assert rep.fallbacks == 1
+    assert torch.equal(pi, _plain_pi(torch, plan, ud, vd))
