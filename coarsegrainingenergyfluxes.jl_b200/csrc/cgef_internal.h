@@ -133,6 +133,7 @@ struct cgef_plan {
   int den_zf_2d = 0;
   cgef::Schedule sched[2];  // [0]: kRows-row tiles (every mode), [1]: kRowsTall rows (filters, when built)
   int filter_rows = CGEF_ROWS;  // tile height of the filter passes (kModeFields)
+  bool paired = false;          // the gather adds mirrored columns first (weights even in the offset)
   // separable engine
   int di_lim = 0, sep_dj_lim = 0;
   double* d_gx = nullptr;

@@ -255,7 +255,13 @@ __device__ __forceinline__ void finish_target(const BandedK& a, const double (&a
 // the kRows rows' weights (zero outside each row's own interval) in its own shared-memory slab,
 // then every lane streams its three (or K) staged values along the row and applies the kRows
 // weights to all accumulated quantities with FP64 FMA.  Warps never wait for one another.
-template <int MODE, int NF, bool DEF, int R>
+//
+// PAIR: the weights of every row are even in the longitude offset (w(-d) = w(d)), so each lane adds
+// the quantities of the mirrored source columns c + d and c - d first and applies each row's weight
+// once per pair: per pair of columns 12 DMUL + NA DADD + R*NA DFMA instead of 12 DMUL + 2*R*NA DFMA.
+// The centre column (d = 0) is its own mirror and a ring-closing row's +a column is its -a column on a
+// periodic ring (the reference visits [-a, a-1]); both carry half weight, which is exact in FP64.
+template <int MODE, int NF, bool DEF, int R, bool PAIR>
 __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(BandedK a) {
   using C = Cfg<MODE, NF, DEF>;
   __shared__ double wbuf[kWarps][R][32];
@@ -323,32 +329,74 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
       continue;
     }
     const double* src = base + static_cast<int64_t>(jj) * a.pitch;
-    for (int c0 = -A; c0 <= HI; c0 += 32) {
-      const int k = c0 + lane;
-      double wv[R];
-#pragma unroll
-      for (int t = 0; t < R; ++t) {
-        const int at = rint[warp][0][t];
-        wv[t] = (at >= 0 && k >= -at && k <= rint[warp][1][t]) ? __ldg(a.w + rint[warp][2][t] + abs(k)) : 0.0;
-      }
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < R; ++t) wb[t * 32 + lane] = wv[t];
-      __syncwarp();
-      const int cn = min(32, HI - c0 + 1);
-      const double* s = src + c0;
-#pragma unroll kBandedUnroll
-      for (int kk = 0; kk < cn; ++kk) {
-        double v[C::NP];
-#pragma unroll
-        for (int pl = 0; pl < C::NP; ++pl) v[pl] = __ldg(s + pl * a.plane_stride + kk);
-        double q[C::NA];
-        expand<MODE, NF, DEF>(v, q);
+    if constexpr (PAIR) {
+      // offsets d = 0 .. A, the pair (c + d, c - d) per step
+      for (int d0 = 0; d0 <= A; d0 += 32) {
+        const int d = d0 + lane;
+        double wv[R];
 #pragma unroll
         for (int t = 0; t < R; ++t) {
-          const double wt = wb[t * 32 + kk];
+          const int at = rint[warp][0][t];
+          double w = (at >= 0 && d <= at) ? __ldg(a.w + rint[warp][2][t] + d) : 0.0;
+          if (d == 0 || (d == at && rint[warp][1][t] < at)) w *= 0.5;
+          wv[t] = w;
+        }
+        __syncwarp();
 #pragma unroll
-          for (int m = 0; m < C::NA; ++m) acc[t][m] = fma(wt, q[m], acc[t][m]);
+        for (int t = 0; t < R; ++t) wb[t * 32 + lane] = wv[t];
+        __syncwarp();
+        const int cn = min(32, A - d0 + 1);
+        const double* sp = src + d0;
+        const double* sm = src - d0;
+#pragma unroll kBandedUnroll
+        for (int kk = 0; kk < cn; ++kk) {
+          double v1[C::NP], v2[C::NP];
+#pragma unroll
+          for (int pl = 0; pl < C::NP; ++pl) {
+            v1[pl] = __ldg(sp + pl * a.plane_stride + kk);
+            v2[pl] = __ldg(sm + pl * a.plane_stride - kk);
+          }
+          double q[C::NA], q2[C::NA];
+          expand<MODE, NF, DEF>(v1, q);
+          expand<MODE, NF, DEF>(v2, q2);
+#pragma unroll
+          for (int m = 0; m < C::NA; ++m) q[m] += q2[m];
+#pragma unroll
+          for (int t = 0; t < R; ++t) {
+            const double wt = wb[t * 32 + kk];
+#pragma unroll
+            for (int m = 0; m < C::NA; ++m) acc[t][m] = fma(wt, q[m], acc[t][m]);
+          }
+        }
+      }
+    } else {
+      for (int c0 = -A; c0 <= HI; c0 += 32) {
+        const int k = c0 + lane;
+        double wv[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          const int at = rint[warp][0][t];
+          wv[t] = (at >= 0 && k >= -at && k <= rint[warp][1][t]) ? __ldg(a.w + rint[warp][2][t] + abs(k)) : 0.0;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < R; ++t) wb[t * 32 + lane] = wv[t];
+        __syncwarp();
+        const int cn = min(32, HI - c0 + 1);
+        const double* s = src + c0;
+#pragma unroll kBandedUnroll
+        for (int kk = 0; kk < cn; ++kk) {
+          double v[C::NP];
+#pragma unroll
+          for (int pl = 0; pl < C::NP; ++pl) v[pl] = __ldg(s + pl * a.plane_stride + kk);
+          double q[C::NA];
+          expand<MODE, NF, DEF>(v, q);
+#pragma unroll
+          for (int t = 0; t < R; ++t) {
+            const double wt = wb[t * 32 + kk];
+#pragma unroll
+            for (int m = 0; m < C::NA; ++m) acc[t][m] = fma(wt, q[m], acc[t][m]);
+          }
         }
       }
     }
@@ -990,11 +1038,14 @@ int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* plane
 namespace {
 
 template <int MODE, int NF, bool DEF, int R>
-int run_banded(const BandedK& a, cudaStream_t st) {
+int run_banded(const BandedK& a, bool pair, cudaStream_t st) {
   const int64_t warps = static_cast<int64_t>(a.nitems) * a.nslices;
   const unsigned blocks = static_cast<unsigned>((warps + kWarps - 1) / kWarps);
   prof_begin(CGEF_KERNEL_BANDED, st);
-  banded_kernel<MODE, NF, DEF, R><<<blocks, 32 * kWarps, 0, st>>>(a);
+  if (pair)
+    banded_kernel<MODE, NF, DEF, R, true><<<blocks, 32 * kWarps, 0, st>>>(a);
+  else
+    banded_kernel<MODE, NF, DEF, R, false><<<blocks, 32 * kWarps, 0, st>>>(a);
   int rc = check_launch("banded_kernel");
   if (rc == CGEF_OK && a.ngroups > 0) {
     const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices;
@@ -1008,14 +1059,15 @@ int run_banded(const BandedK& a, cudaStream_t st) {
 // The flux modes run kRows-row tiles only (taller tiles spill their accumulators); the filter
 // passes also have kRowsTall-row tiles.
 template <int MODE, int NF>
-int dispatch_banded(bool def, int R, const BandedK& a, cudaStream_t st) {
+int dispatch_banded(bool def, int R, bool pair, const BandedK& a, cudaStream_t st) {
   if constexpr (MODE == kModeFields && NF + 1 <= kTallMaxQuantities) {
     if (R == kRowsTall)
-      return def ? run_banded<MODE, NF, true, kRowsTall>(a, st) : run_banded<MODE, NF, false, kRowsTall>(a, st);
+      return def ? run_banded<MODE, NF, true, kRowsTall>(a, pair, st)
+                 : run_banded<MODE, NF, false, kRowsTall>(a, pair, st);
   } else if constexpr (MODE == kModeFields && NF <= kTallMaxQuantities) {
-    if (R == kRowsTall && !def) return run_banded<MODE, NF, false, kRowsTall>(a, st);
+    if (R == kRowsTall && !def) return run_banded<MODE, NF, false, kRowsTall>(a, pair, st);
   }
-  return def ? run_banded<MODE, NF, true, kRows>(a, st) : run_banded<MODE, NF, false, kRows>(a, st);
+  return def ? run_banded<MODE, NF, true, kRows>(a, pair, st) : run_banded<MODE, NF, false, kRows>(a, pair, st);
 }
 
 }  // namespace
@@ -1066,13 +1118,14 @@ int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* plan
   a.cosphi = sph ? p->d_cosphi : nullptr;
   for (int m = 0; m < 9; ++m) a.out[m] = out.o[m];
   a.out_stride = out.slice_stride;
-  if (mode == kModePiSphere) return dispatch_banded<kModePiSphere, 1>(def, R, a, st);
-  if (mode == kModePiCart) return dispatch_banded<kModePiCart, 1>(def, R, a, st);
+  const bool pair = p->paired;
+  if (mode == kModePiSphere) return dispatch_banded<kModePiSphere, 1>(def, R, pair, a, st);
+  if (mode == kModePiCart) return dispatch_banded<kModePiCart, 1>(def, R, pair, a, st);
   switch (nf) {
-    case 1: return dispatch_banded<kModeFields, 1>(def, R, a, st);
-    case 2: return dispatch_banded<kModeFields, 2>(def, R, a, st);
-    case 3: return dispatch_banded<kModeFields, 3>(def, R, a, st);
-    case 4: return dispatch_banded<kModeFields, 4>(def, R, a, st);
+    case 1: return dispatch_banded<kModeFields, 1>(def, R, pair, a, st);
+    case 2: return dispatch_banded<kModeFields, 2>(def, R, pair, a, st);
+    case 3: return dispatch_banded<kModeFields, 3>(def, R, pair, a, st);
+    case 4: return dispatch_banded<kModeFields, 4>(def, R, pair, a, st);
     default: return fail(CGEF_EINVAL, "banded: 1..4 fields per pass");
   }
 }

@@ -221,6 +221,9 @@ void build_banded(const cgef_plan* p, Banded& B) {
 
 }  // namespace
 
+#ifndef CGEF_PAIRED
+#define CGEF_PAIRED 1
+#endif
 #ifndef CGEF_SPLIT_WAVES
 #define CGEF_SPLIT_WAVES 4.0
 #endif
@@ -455,6 +458,12 @@ int build_plan_tables(cgef_plan* p) {
     if ((rc = upload(p, &p->d_w, B.w.data(), B.w.size())) != CGEF_OK) return rc;
     if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
     if ((rc = rebuild_schedule(p, CGEF_SPLIT_WAVES, 0)) != CGEF_OK) return rc;
+    // Mirrored columns may be paired when every row's interval is symmetric, or when the only
+    // asymmetric rows close a periodic ring (their +a column is their -a column).
+    bool symmetric = true;
+    for (const BandRow& r : B.rows)
+      if (r.a >= 0 && r.hi != r.a) symmetric = false;
+    p->paired = CGEF_PAIRED && (symmetric || p->periodic_x);
   } else if (p->engine == CGEF_ENGINE_SEPARABLE) {
     // Filtering.jl:1391-1463: square truncation, lim = ceil(rad / step), point-sampled profile.
     p->di_lim = p->dx > 0 ? static_cast<int>(std::ceil(p->rad / p->dx)) : 0;
