@@ -421,32 +421,46 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
   }
 }
 
-// Adds the partial slots of every split tile in slot order (deterministic) and finishes it.
+// Adds the partial slots of every split tile in slot order (deterministic) and finishes it: one warp
+// per (tile, slice, target row).  The loads of four slots are in flight together; the additions stay
+// in slot order.
 template <int MODE, int NF, bool DEF, int R>
 __global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
   using C = Cfg<MODE, NF, DEF>;
+  constexpr int kAhead = 4;
   const int lane = threadIdx.x & 31;
   const int64_t gid = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  if (gid >= static_cast<int64_t>(a.ngroups) * a.nslices) return;
-  const int gi = static_cast<int>(gid / a.nslices);
-  const int slice = static_cast<int>(gid - static_cast<int64_t>(gi) * a.nslices);
+  if (gid >= static_cast<int64_t>(a.ngroups) * a.nslices * R) return;
+  const int t = static_cast<int>(gid % R);
+  const int64_t gs = gid / R;
+  const int gi = static_cast<int>(gs / a.nslices);
+  const int slice = static_cast<int>(gs - static_cast<int64_t>(gi) * a.nslices);
   const SplitGroup g = a.groups[gi];
   const int col = g.x0 + lane;
-  if (col >= a.nx) return;
+  const int j = g.j0 + t;
+  if (col >= a.nx || j >= a.ny) return;
   double acc[C::NA];
-  for (int t = 0; t < R; ++t) {
-    const int j = g.j0 + t;
-    if (j >= a.ny) break;
 #pragma unroll
-    for (int m = 0; m < C::NA; ++m) acc[m] = 0.0;
-    for (int q = 0; q < g.nslots; ++q) {
-      const double* pp =
-          a.partials + ((static_cast<int64_t>(g.slot0 + q) * a.nslices + slice) * R * C::NA + t * C::NA) * 32 + lane;
+  for (int m = 0; m < C::NA; ++m) acc[m] = 0.0;
+  const int64_t slot_stride = static_cast<int64_t>(a.nslices) * R * C::NA * 32;
+  const double* p0 =
+      a.partials + ((static_cast<int64_t>(g.slot0) * a.nslices + slice) * R * C::NA + t * C::NA) * 32 + lane;
+  int q = 0;
+  for (; q + kAhead <= g.nslots; q += kAhead) {
+    double v[kAhead][C::NA];
 #pragma unroll
-      for (int m = 0; m < C::NA; ++m) acc[m] += pp[m * 32];
-    }
-    finish_target<MODE, NF, DEF>(a, acc, slice, j, col);
+    for (int u = 0; u < kAhead; ++u)
+#pragma unroll
+      for (int m = 0; m < C::NA; ++m) v[u][m] = p0[(q + u) * slot_stride + m * 32];
+#pragma unroll
+    for (int u = 0; u < kAhead; ++u)
+#pragma unroll
+      for (int m = 0; m < C::NA; ++m) acc[m] += v[u][m];
   }
+  for (; q < g.nslots; ++q)
+#pragma unroll
+    for (int m = 0; m < C::NA; ++m) acc[m] += p0[q * slot_stride + m * 32];
+  finish_target<MODE, NF, DEF>(a, acc, slice, j, col);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1048,7 +1062,7 @@ int run_banded(const BandedK& a, bool pair, cudaStream_t st) {
     banded_kernel<MODE, NF, DEF, R, false><<<blocks, 32 * kWarps, 0, st>>>(a);
   int rc = check_launch("banded_kernel");
   if (rc == CGEF_OK && a.ngroups > 0) {
-    const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices;
+    const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices * R;
     banded_combine_kernel<MODE, NF, DEF, R><<<static_cast<unsigned>((cw + 3) / 4), 128, 0, st>>>(a);
     rc = check_launch("banded_combine_kernel");
   }
