@@ -149,6 +149,7 @@ struct cgef_plan {
   // execution
   cudaStream_t stream = nullptr;
   cgef::DeviceBuffer ws[12];  // workspace slots (cgef::WsSlot), grown on demand
+  unsigned long long* d_queue = nullptr;  // banded work queue: [next unit, warps finished], zero between launches
 };
 
 namespace cgef {

@@ -15,6 +15,7 @@
 //
 // This file is compiled with --fmad=false: every product and sum outside the explicit fma()
 // accumulations is rounded separately, as in the reference's Julia code.
+#include <algorithm>
 #include <cstdint>
 
 #include "cgef_internal.h"
@@ -149,6 +150,7 @@ struct BandedK {
   const double* cosphi;
   double* out[9];
   int64_t out_stride;
+  unsigned long long* queue;  // [next unit, warps finished]; zero when a launch starts
 };
 
 // Expands the staged values of one source cell into the accumulated quantities: the fields
@@ -177,6 +179,36 @@ __device__ __forceinline__ void expand(const double (&v)[Cfg<MODE, NF, DEF>::NP]
     for (int m = 0; m < NF; ++m) q[m] = v[m];
   }
   if (DEF) q[C::NA - 1] = v[C::NP - 1];
+}
+
+// The quantities of two mirrored source cells added together: sums of the fields, and each product
+// of the first cell fused onto the rounded product of the second (one DMUL + one DFMA per product).
+template <int MODE, int NF, bool DEF>
+__device__ __forceinline__ void expand_pair(const double (&v)[Cfg<MODE, NF, DEF>::NP],
+                                            const double (&u)[Cfg<MODE, NF, DEF>::NP],
+                                            double (&q)[Cfg<MODE, NF, DEF>::NA]) {
+  using C = Cfg<MODE, NF, DEF>;
+  if (MODE == kModePiSphere) {
+    q[0] = v[0] + u[0];
+    q[1] = v[1] + u[1];
+    q[2] = v[2] + u[2];
+    q[3] = fma(v[0], v[0], u[0] * u[0]);
+    q[4] = fma(v[0], v[1], u[0] * u[1]);
+    q[5] = fma(v[0], v[2], u[0] * u[2]);
+    q[6] = fma(v[1], v[1], u[1] * u[1]);
+    q[7] = fma(v[1], v[2], u[1] * u[2]);
+    q[8] = fma(v[2], v[2], u[2] * u[2]);
+  } else if (MODE == kModePiCart) {
+    q[0] = v[0] + u[0];
+    q[1] = v[1] + u[1];
+    q[2] = fma(v[0], v[0], u[0] * u[0]);
+    q[3] = fma(v[0], v[1], u[0] * u[1]);
+    q[4] = fma(v[1], v[1], u[1] * u[1]);
+  } else {
+#pragma unroll
+    for (int m = 0; m < NF; ++m) q[m] = v[m] + u[m];
+  }
+  if (DEF) q[C::NA - 1] = v[C::NP - 1] + u[C::NP - 1];
 }
 
 // Normalised epilogue shared by the direct-sum engines.  F holds the NA0 filtered quantities
@@ -258,18 +290,13 @@ __device__ __forceinline__ void finish_target(const BandedK& a, const double (&a
 //
 // PAIR: the weights of every row are even in the longitude offset (w(-d) = w(d)), so each lane adds
 // the quantities of the mirrored source columns c + d and c - d first and applies each row's weight
-// once per pair: per pair of columns 12 DMUL + NA DADD + R*NA DFMA instead of 12 DMUL + 2*R*NA DFMA.
+// once per pair: per pair of columns (sphere) 6 DMUL + 6 DFMA + 3 DADD + R*NA DFMA instead of
+// 12 DMUL + 2*R*NA DFMA.
 // The centre column (d = 0) is its own mirror and a ring-closing row's +a column is its -a column on a
 // periodic ring (the reference visits [-a, a-1]); both carry half weight, which is exact in FP64.
 template <int MODE, int NF, bool DEF, int R, bool PAIR>
-__global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(BandedK a) {
+__device__ __forceinline__ void banded_unit(const BandedK& a, int64_t gid, double* wb, int (&ri)[3][R], int lane) {
   using C = Cfg<MODE, NF, DEF>;
-  __shared__ double wbuf[kWarps][R][32];
-  __shared__ int rint[kWarps][3][R];  // per warp: a, hi, woff of the R rows for the current source row
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int64_t gid = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
-  if (gid >= static_cast<int64_t>(a.nitems) * a.nslices) return;
   const int item_id = static_cast<int>(gid / a.nslices);
   const int slice = static_cast<int>(gid - static_cast<int64_t>(item_id) * a.nslices);
   const WorkItem it = a.items[item_id];
@@ -295,7 +322,6 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
   const bool warp_act = __any_sync(0xffffffffu, any_act);
 
   const double* base = a.planes + slice * a.slice_stride + a.halo + col;
-  double* wb = &wbuf[warp][0][0];
   for (int jr = it.jr0; warp_act && jr < it.jr1; ++jr) {
     int jj = jr;
     if (jr < 0 || jr >= a.ny) {
@@ -313,16 +339,16 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
         rhi = r.hi;
         roff = r.woff;
       }
-      rint[warp][0][lane] = ra;
-      rint[warp][1][lane] = rhi;
-      rint[warp][2][lane] = roff;
+      ri[0][lane] = ra;
+      ri[1][lane] = rhi;
+      ri[2][lane] = roff;
     }
     __syncwarp();
     int A = -1, HI = -1;
 #pragma unroll
     for (int t = 0; t < R; ++t) {
-      A = max(A, rint[warp][0][t]);
-      HI = max(HI, rint[warp][1][t]);
+      A = max(A, ri[0][t]);
+      HI = max(HI, ri[1][t]);
     }
     if (A < 0) {
       __syncwarp();
@@ -336,9 +362,9 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
         double wv[R];
 #pragma unroll
         for (int t = 0; t < R; ++t) {
-          const int at = rint[warp][0][t];
-          double w = (at >= 0 && d <= at) ? __ldg(a.w + rint[warp][2][t] + d) : 0.0;
-          if (d == 0 || (d == at && rint[warp][1][t] < at)) w *= 0.5;
+          const int at = ri[0][t];
+          double w = (at >= 0 && d <= at) ? __ldg(a.w + ri[2][t] + d) : 0.0;
+          if (d == 0 || (d == at && ri[1][t] < at)) w *= 0.5;
           wv[t] = w;
         }
         __syncwarp();
@@ -356,11 +382,8 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
             v1[pl] = __ldg(sp + pl * a.plane_stride + kk);
             v2[pl] = __ldg(sm + pl * a.plane_stride - kk);
           }
-          double q[C::NA], q2[C::NA];
-          expand<MODE, NF, DEF>(v1, q);
-          expand<MODE, NF, DEF>(v2, q2);
-#pragma unroll
-          for (int m = 0; m < C::NA; ++m) q[m] += q2[m];
+          double q[C::NA];
+          expand_pair<MODE, NF, DEF>(v1, v2, q);
 #pragma unroll
           for (int t = 0; t < R; ++t) {
             const double wt = wb[t * 32 + kk];
@@ -375,8 +398,8 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
         double wv[R];
 #pragma unroll
         for (int t = 0; t < R; ++t) {
-          const int at = rint[warp][0][t];
-          wv[t] = (at >= 0 && k >= -at && k <= rint[warp][1][t]) ? __ldg(a.w + rint[warp][2][t] + abs(k)) : 0.0;
+          const int at = ri[0][t];
+          wv[t] = (at >= 0 && k >= -at && k <= ri[1][t]) ? __ldg(a.w + ri[2][t] + abs(k)) : 0.0;
         }
         __syncwarp();
 #pragma unroll
@@ -419,6 +442,43 @@ __global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(B
     if (j >= a.ny) break;
     finish_target<MODE, NF, DEF>(a, acc[t], slice, j, col);
   }
+}
+
+// Takes the next unit of the launch's queue (one atomic per warp) and hands it to every lane.
+__device__ __forceinline__ int64_t take_unit(unsigned long long* queue, int lane) {
+  unsigned long long u = 0;
+  if (lane == 0) u = atomicAdd(queue, 1ull);
+  return static_cast<int64_t>(__shfl_sync(0xffffffffu, u, 0));
+}
+
+// A warp leaves after its last (empty) take; the last warp of the launch to leave zeroes the queue
+// for the next launch.  Every warp's takes are fenced before its count, so none can follow the reset.
+__device__ __forceinline__ void leave_queue(unsigned long long* queue, int lane) {
+  if (lane != 0) return;
+  const unsigned long long nwarps = static_cast<unsigned long long>(gridDim.x) * (blockDim.x >> 5);
+  __threadfence();
+  if (atomicAdd(queue + 1, 1ull) == nwarps - 1) {
+    __threadfence();
+    atomicExch(queue, 0ull);
+    atomicExch(queue + 1, 0ull);
+  }
+}
+
+// Persistent launch: at most as many warps as fit on the GPU at once, each taking (item, slice)
+// units in the schedule's longest-first order until none is left, so no warp idles behind a slower
+// sibling of its block while units remain.  Results do not depend on which warp takes a unit.
+template <int MODE, int NF, bool DEF, int R, bool PAIR>
+__global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(BandedK a) {
+  __shared__ double wbuf[kWarps][R][32];
+  __shared__ int rint[kWarps][3][R];  // per warp: a, hi, woff of the R rows for the current source row
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int64_t total = static_cast<int64_t>(a.nitems) * a.nslices;
+  for (int64_t gid = take_unit(a.queue, lane); gid < total; gid = take_unit(a.queue, lane)) {
+    banded_unit<MODE, NF, DEF, R, PAIR>(a, gid, &wbuf[warp][0][0], rint[warp], lane);
+    __syncwarp();
+  }
+  leave_queue(a.queue, lane);
 }
 
 // Adds the partial slots of every split tile in slot order (deterministic) and finishes it: one warp
@@ -1051,15 +1111,34 @@ int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* plane
 
 namespace {
 
+// Blocks of one kernel instance that fit on the current device at once (cached per device).
+template <typename K>
+int64_t resident_blocks(K kernel) {
+  static int64_t cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  if (cached[dev] == 0) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * kWarps, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm < 1 || sms < 1)
+      return 1 << 20;
+    cached[dev] = static_cast<int64_t>(per_sm) * sms;
+  }
+  return cached[dev];
+}
+
 template <int MODE, int NF, bool DEF, int R>
 int run_banded(const BandedK& a, bool pair, cudaStream_t st) {
-  const int64_t warps = static_cast<int64_t>(a.nitems) * a.nslices;
-  const unsigned blocks = static_cast<unsigned>((warps + kWarps - 1) / kWarps);
+  const int64_t units = static_cast<int64_t>(a.nitems) * a.nslices;
+  const int64_t need = (units + kWarps - 1) / kWarps;
   prof_begin(CGEF_KERNEL_BANDED, st);
-  if (pair)
-    banded_kernel<MODE, NF, DEF, R, true><<<blocks, 32 * kWarps, 0, st>>>(a);
-  else
-    banded_kernel<MODE, NF, DEF, R, false><<<blocks, 32 * kWarps, 0, st>>>(a);
+  if (pair) {
+    const auto k = banded_kernel<MODE, NF, DEF, R, true>;
+    k<<<static_cast<unsigned>(std::min(need, resident_blocks(k))), 32 * kWarps, 0, st>>>(a);
+  } else {
+    const auto k = banded_kernel<MODE, NF, DEF, R, false>;
+    k<<<static_cast<unsigned>(std::min(need, resident_blocks(k))), 32 * kWarps, 0, st>>>(a);
+  }
   int rc = check_launch("banded_kernel");
   if (rc == CGEF_OK && a.ngroups > 0) {
     const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices * R;
@@ -1118,6 +1197,8 @@ int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* plan
   if (a.nitems == 0) return CGEF_OK;
   a.partials = partials;
   if (a.ngroups > 0 && partials == nullptr) return fail(CGEF_EINVAL, "banded: split tiles need a partials buffer");
+  a.queue = p->d_queue;
+  if (a.queue == nullptr) return fail(CGEF_EINVAL, "banded: the plan has no work queue");
   a.den_zf = p->d_den_zf;
   a.den_zf_2d = p->den_zf_2d;
   a.mask = mask;

@@ -457,6 +457,8 @@ int build_plan_tables(cgef_plan* p) {
     if (B.w.empty()) B.w.push_back(0.0);
     if ((rc = upload(p, &p->d_w, B.w.data(), B.w.size())) != CGEF_OK) return rc;
     if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
+    const unsigned long long queue0[2] = {0, 0};
+    if ((rc = upload(p, &p->d_queue, queue0, 2)) != CGEF_OK) return rc;
     if ((rc = rebuild_schedule(p, CGEF_SPLIT_WAVES, 0)) != CGEF_OK) return rc;
     // Mirrored columns may be paired when every row's interval is symmetric, or when the only
     // asymmetric rows close a periodic ring (their +a column is their -a column).
