@@ -23,6 +23,9 @@
 #ifndef CGEF_BANDED_MINB
 #define CGEF_BANDED_MINB 4
 #endif
+#ifndef CGEF_BANDED_MINB_SPHERE_PI
+#define CGEF_BANDED_MINB_SPHERE_PI 3
+#endif
 #ifndef CGEF_BANDED_UNROLL
 #define CGEF_BANDED_UNROLL 2
 #endif
@@ -31,8 +34,11 @@ namespace cgef {
 
 namespace {
 
-// Resident CTAs per SM the banded gather is compiled for, and the unroll of its inner loop.
+// Resident CTAs per SM the banded gather is compiled for, and the unroll of its inner loop.  The
+// sphere flux gather (nine accumulated quantities per row) gets the registers of three CTAs per SM:
+// at four it spills its accumulators.
 constexpr int kBandedMinBlocks = CGEF_BANDED_MINB;
+constexpr int banded_min_blocks(int mode) { return mode == kModePiSphere ? CGEF_BANDED_MINB_SPHERE_PI : kBandedMinBlocks; }
 constexpr int kBandedUnroll = CGEF_BANDED_UNROLL;
 
 __device__ __forceinline__ int wrap(int a, int n) {
@@ -468,7 +474,7 @@ __device__ __forceinline__ void leave_queue(unsigned long long* queue, int lane)
 // units in the schedule's longest-first order until none is left, so no warp idles behind a slower
 // sibling of its block while units remain.  Results do not depend on which warp takes a unit.
 template <int MODE, int NF, bool DEF, int R, bool PAIR>
-__global__ void __launch_bounds__(32 * kWarps, kBandedMinBlocks) banded_kernel(BandedK a) {
+__global__ void __launch_bounds__(32 * kWarps, banded_min_blocks(MODE)) banded_kernel(BandedK a) {
   __shared__ double wbuf[kWarps][R][32];
   __shared__ int rint[kWarps][3][R];  // per warp: a, hi, woff of the R rows for the current source row
   const int lane = threadIdx.x & 31;
