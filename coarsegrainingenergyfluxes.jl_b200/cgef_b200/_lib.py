@@ -38,7 +38,8 @@ EXPORTED = [
     "cgef_sweep_graph_create", "cgef_graph_launch", "cgef_graph_destroy", "cgef_tau_decomposition",
     "cgef_tau_decomposition_device", "cgef_pi_strain_convergence", "cgef_pi_strain_convergence_device",
     "cgef_pipeline_create", "cgef_pipeline_submit", "cgef_pipeline_drain", "cgef_pipeline_destroy",
-    "cgef_plan_set_filter_rows", "cgef_plan_get_schedule",
+    "cgef_plan_set_filter_rows", "cgef_plan_get_schedule", "cgef_plan_set_row_spectral",
+    "cgef_plan_get_row_spectral",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE = 0, 1, 2, 3, 4, 5
 CLOSURE_NPARAM = 8899
@@ -178,6 +179,10 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_plan_set_filter_rows.restype = i32
     L.cgef_plan_get_schedule.argtypes = [vp, C.POINTER(dbl), C.POINTER(i32)]
     L.cgef_plan_get_schedule.restype = i32
+    L.cgef_plan_set_row_spectral.argtypes = [vp, i32]
+    L.cgef_plan_set_row_spectral.restype = i32
+    L.cgef_plan_get_row_spectral.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    L.cgef_plan_get_row_spectral.restype = i32
     L.cgef_closure_create.argtypes = [C.POINTER(vp), C.c_uint64]
     L.cgef_closure_destroy.argtypes = [vp]
     L.cgef_closure_get_params.argtypes = [vp, vp]

@@ -18,8 +18,9 @@ CSRC = os.path.join(PKG_ROOT, "csrc")
 INCLUDE = os.path.join(REPO_ROOT, "include")
 LIB_PATH = os.path.join(HERE, "libcgef_b200.so")
 PEAK_LIB_PATH = os.path.join(HERE, "libcgef_peak.so")
-SOURCES = ["kernels.cu", "cgef_api.cu", "noalloc.cu", "closure.cu", "decomposition.cu", "pipeline.cu", "plan_build.cpp"]
-HEADERS = ["cgef_internal.h"]
+SOURCES = ["kernels.cu", "rowspec.cu", "cgef_api.cu", "noalloc.cu", "closure.cu", "decomposition.cu", "pipeline.cu",
+           "plan_build.cpp"]
+HEADERS = ["cgef_internal.h", "banded_common.cuh"]
 
 
 def _nvcc() -> str:

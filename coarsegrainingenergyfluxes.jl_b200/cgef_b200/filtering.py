@@ -123,6 +123,22 @@ class PhysicalFilterPlan:
         _lib.check(_lib.load().cgef_plan_set_split_waves(self.handle, float(waves)))
         self.split_waves = float(waves)
 
+    def set_row_spectral(self, enable: bool) -> None:
+        """Evaluate the banded sums through ring spectra (True) or directly (False); results agree to
+        FP64 rounding.  Raises ArgumentError where the plan cannot use the spectral evaluation."""
+        if enable and not self.row_spectral[0]:
+            raise ArgumentError("row-spectral evaluation is not available for this plan: it needs the banded "
+                                "engine, a periodic x axis or symmetric rows, and an even FFT length whose "
+                                "half has no prime factor above 5")
+        _lib.check(_lib.load().cgef_plan_set_row_spectral(self.handle, 1 if enable else 0))
+
+    @property
+    def row_spectral(self):
+        """(available, enabled, fft_length) of the row-spectral evaluation."""
+        a, e, n = C.c_int32(), C.c_int32(), C.c_int32()
+        _lib.check(_lib.load().cgef_plan_get_row_spectral(self.handle, C.byref(a), C.byref(e), C.byref(n)))
+        return bool(a.value), bool(e.value), int(n.value)
+
     def footprint(self):
         """The banded footprint in the reference's CSR form (di, dj, w, ptr), 0-based."""
         n = int(self.info.nentries)

@@ -136,7 +136,7 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
   if (p->engine == CGEF_ENGINE_BANDED) {
     const int na = (mode == kModePiSphere ? 9 : 5) + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
     void* part = nullptr;
-    const size_t pb = banded_partials_bytes(p, na, nbatch, mode);
+    const size_t pb = banded_scratch_bytes(p, na, nbatch, mode);
     if (pb > 0) {
       int rc = ensure_ws(p, kSlotSplit, pb, &part);
       if (rc) return rc;
@@ -257,7 +257,7 @@ int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int
   double* pl = static_cast<double*>(planes);
   if (p->engine == CGEF_ENGINE_BANDED) {
     void* part = nullptr;
-    const size_t pb = banded_partials_bytes(p, nf + (def ? 1 : 0), nbatch, kModeFields);
+    const size_t pb = banded_scratch_bytes(p, nf + (def ? 1 : 0), nbatch, kModeFields);
     if (pb > 0 && (rc = ensure_ws(p, kSlotSplit, pb, &part))) return rc;
     return launch_banded(p, kModeFields, nf, pl, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st);
   }
@@ -501,7 +501,7 @@ int32_t cgef_plan_destroy(cgef_plan* p) {
     void* ptrs[] = {p->d_mask, p->d_x, p->d_sinlam, p->d_coslam, p->d_sinphi, p->d_cosphi, p->d_area, p->d_xscale,
                     p->d_tanfac, p->d_rows, p->d_w, p->d_den_zf, p->sched[0].d_items, p->sched[0].d_groups,
                     p->sched[1].d_items, p->sched[1].d_groups, p->d_gx, p->d_gy, p->d_px, p->d_py, p->d_xe,
-                    p->d_prefix_wx, p->d_prows, p->d_queue};
+                    p->d_prefix_wx, p->d_prows, p->d_queue, p->d_rs_tw, p->d_rs_k};
     for (void* q : ptrs)
       if (q) cudaFree(q);
     for (auto& b : p->ws)
@@ -543,6 +543,25 @@ int32_t cgef_plan_set_filter_rows(cgef_plan* p, int32_t rows) {
   DeviceGuard dg(p->device);
   if (rows == kRowsTall && p->sched[1].rows == 0 && (rc = rebuild_schedule(p, p->sched[0].waves, 1))) return rc;
   p->filter_rows = rows;
+  return CGEF_OK;
+}
+
+int32_t cgef_plan_set_row_spectral(cgef_plan* p, int32_t enable) {
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (enable && p->rs_L == 0)
+    return fail(CGEF_EINVAL, "row-spectral evaluation is not available for this plan (banded engine on a periodic "
+                             "x axis or with symmetric rows, and an even FFT length whose half has factors 2, 3, 5 "
+                             "only)");
+  p->rs_on = enable != 0;
+  return CGEF_OK;
+}
+
+int32_t cgef_plan_get_row_spectral(const cgef_plan* p, int32_t* available, int32_t* enabled, int32_t* fft_length) {
+  if (!p) return fail(CGEF_EINVAL, "plan is NULL");
+  if (available) *available = p->rs_L > 0;
+  if (enabled) *enabled = p->rs_on;
+  if (fft_length) *fft_length = p->rs_L;
   return CGEF_OK;
 }
 
@@ -603,7 +622,9 @@ int32_t cgef_plan_autotune(cgef_plan* p, int32_t nbatch, double* chosen) {
     *ms_out = ms / done;
     return CGEF_OK;
   };
-  // 1. split granularity of the flux gather's schedule
+  // 1. split granularity of the direct flux gather's schedule
+  const bool rs_avail = p->rs_L > 0;
+  p->rs_on = false;
   const double cand[4] = {2.0, 4.0, 8.0, 16.0};
   double best = p->sched[0].waves, best_ms = 1e300;
   for (double w : cand) {
@@ -633,6 +654,15 @@ int32_t cgef_plan_autotune(cgef_plan* p, int32_t nbatch, double* chosen) {
                      &ms_r[k]);
     }
     p->filter_rows = (rc == CGEF_OK && ms_r[1] < ms_r[0]) ? kRowsTall : kRows;
+  }
+  // 3. direct gather or row-spectral evaluation of the flux's sums, whichever is faster here
+  if (rc == CGEF_OK && rs_avail) {
+    double ms_rs = 0.0;
+    p->rs_on = true;
+    rc = time_pass([&] { return pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0,
+                                          static_cast<double*>(gather), st); },
+                   &ms_rs);
+    p->rs_on = rc == CGEF_OK && ms_rs < best_ms;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -134,6 +135,15 @@ struct cgef_plan {
   cgef::Schedule sched[2];  // [0]: kRows-row tiles (every mode), [1]: kRowsTall rows (filters, when built)
   int filter_rows = CGEF_ROWS;  // tile height of the filter passes (kModeFields)
   bool paired = false;          // the gather adds mirrored columns first (weights even in the offset)
+  // row-spectral evaluation of the same sums: each (target row, row offset) term is a correlation
+  // along x, done as a product of ring spectra
+  int rs_L = 0;                 // FFT length along x; 0 = not available for this plan
+  int rs_nk = 0;                // spectrum bins kept, rs_L / 2 + 1
+  int rs_nrad = 0;              // Stockham passes
+  int rs_rad[16] = {};          // their radices (2, 3, 4 or 5)
+  double* d_rs_tw = nullptr;    // rs_L twiddles exp(-2 pi i n / rs_L), (re, im) pairs
+  double* d_rs_k = nullptr;     // kernel spectra / rs_L: [band][row offset][bin]
+  bool rs_on = false;           // full-grid banded launches use the row-spectral evaluation
   // separable engine
   int di_lim = 0, sep_dj_lim = 0;
   double* d_gx = nullptr;
@@ -236,11 +246,23 @@ struct GatherOut {
   int64_t slice_stride;
 };
 
-// `partials` holds banded_partials_bytes() of scratch for the split tiles (may be null when the
-// plan has none).
+// `partials` holds banded_scratch_bytes() of scratch (the direct gather's split tiles, or the
+// row-spectral evaluation's spectra when the plan uses it); `direct_only` keeps the direct gather,
+// whose scratch is banded_partials_bytes().
 int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                   const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
-                  cudaStream_t st);
+                  cudaStream_t st, bool direct_only = false);
+
+// The row-spectral evaluation of a full-grid banded launch: x-direction FFTs of the accumulated
+// quantities of every source row, the band's kernel spectra applied and summed per target row,
+// inverse FFTs, and the same epilogue as the direct gather.  `scratch` holds rowspec_bytes().
+int launch_rowspec(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                   const uint8_t* mask, int64_t mask_slice_stride, double* scratch, const GatherOut& out,
+                   cudaStream_t st);
+
+// Decides whether the plan's banded sums can be evaluated through ring spectra and, if so, builds
+// the twiddles and the kernel spectra on the device (called once the band tables are uploaded).
+int build_row_spectra(cgef_plan* p);
 
 // The same over a caller-given device schedule: work items and the split groups they belong to
 // (e.g. from subset_schedule); `partials` holds the slots that schedule numbers.
@@ -253,6 +275,18 @@ int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* plan
 inline size_t banded_partials_bytes(const cgef_plan* p, int na, int nbatch, int mode) {
   const Schedule& s = schedule_for(p, mode, na);
   return sizeof(double) * static_cast<size_t>(s.nslots) * nbatch * s.rows * na * 32;
+}
+
+// Bytes of the row-spectral evaluation's scratch: the spectra of the source rows and the summed
+// spectra of the target rows, `na` quantities over `nbatch` slices.
+inline size_t rowspec_bytes(const cgef_plan* p, int na, int nbatch) {
+  return 2 * 2 * sizeof(double) * static_cast<size_t>(nbatch) * p->ny * na * p->rs_nk;
+}
+
+// Scratch of a full-grid banded launch, whichever evaluation the plan uses.
+inline size_t banded_scratch_bytes(const cgef_plan* p, int na, int nbatch, int mode) {
+  const size_t d = banded_partials_bytes(p, na, nbatch, mode);
+  return p->rs_on ? std::max(d, rowspec_bytes(p, na, nbatch)) : d;
 }
 
 int launch_separable(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,

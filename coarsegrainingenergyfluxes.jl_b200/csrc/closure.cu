@@ -818,7 +818,7 @@ int filtered_velocity(cgef_plan* p, cgef_closure* c, int dtype, const void* u, c
   const bool def = p->strategy == CGEF_DEFORMABLE;
   if (p->engine == CGEF_ENGINE_BANDED) {
     void* part = nullptr;
-    const size_t pb = banded_partials_bytes(p, nf + (def ? 1 : 0), nbatch, kModeFields);
+    const size_t pb = banded_scratch_bytes(p, nf + (def ? 1 : 0), nbatch, kModeFields);
     if (pb > 0 && (rc = ensure_ws(p, kSlotSplit, pb, &part))) return rc;
     rc = launch_banded(p, kModeFields, nf, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st);
   } else if (p->engine == CGEF_ENGINE_SEPARABLE) {

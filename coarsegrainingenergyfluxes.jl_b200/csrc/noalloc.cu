@@ -101,7 +101,8 @@ extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const
     go.slice_stride = N;
     if (rc == CGEF_OK) {
       if (p->engine == CGEF_ENGINE_BANDED)
-        rc = launch_banded(p, kModeFields, 1, planes, pitch, np, nbatch, p->d_mask, 0, engine_b ? aux : nullptr, go, st);
+        rc = launch_banded(p, kModeFields, 1, planes, pitch, np, nbatch, p->d_mask, 0, engine_b ? aux : nullptr, go, st,
+                          true);
       else if (p->engine == CGEF_ENGINE_SEPARABLE)
         rc = launch_separable(p, kModeFields, 1, planes, pitch, np, nbatch, p->d_mask, 0, aux, go, st);
       else

@@ -466,6 +466,7 @@ int build_plan_tables(cgef_plan* p) {
     for (const BandRow& r : B.rows)
       if (r.a >= 0 && r.hi != r.a) symmetric = false;
     p->paired = CGEF_PAIRED && (symmetric || p->periodic_x);
+    if ((rc = build_row_spectra(p)) != CGEF_OK) return rc;
   } else if (p->engine == CGEF_ENGINE_SEPARABLE) {
     // Filtering.jl:1391-1463: square truncation, lim = ceil(rad / step), point-sampled profile.
     p->di_lim = p->dx > 0 ? static_cast<int>(std::ceil(p->rad / p->dx)) : 0;

@@ -143,6 +143,24 @@ int32_t cgef_plan_set_filter_rows(cgef_plan* plan, int32_t rows);
  * (both 0 off the banded engine). */
 int32_t cgef_plan_get_schedule(const cgef_plan* plan, double* waves, int32_t* filter_rows);
 
+/* Row-spectral evaluation of the banded engine's sums (no counterpart in the reference, which sums
+ * the footprint directly, Filtering.jl:1569-1744, 2536-2598).  For a target row and a row offset the
+ * footprint weights depend only on the column offset, so each such term is a correlation along x;
+ * with an FFT along x of every source row's accumulated quantities, the band's kernel spectra
+ * applied and summed per target row, and an inverse FFT, the plan computes the same sums at a cost
+ * linear, not quadratic, in the footprint's reach.  Results equal the direct sums up to FP64
+ * rounding of the transforms, and each quantity is transformed on its own, so batched applies stay
+ * bit-identical to per-field ones.  Available on a periodic x axis (FFT length Nx) or with symmetric
+ * rows on a bounded one (a zero-padded length >= Nx + the widest half-width), when the length is even
+ * and its half has no prime factor above 5; built with the plan and enabled by default when available;
+ * cgef_plan_autotune keeps whichever evaluation times faster for the flux.  Work-item subsets (the
+ * closure's judge) and cgef_filter_device_noalloc always sum directly. */
+int32_t cgef_plan_set_row_spectral(cgef_plan* plan, int32_t enable);
+/* available: the plan can use it; enabled: full-grid launches use it; fft_length: its FFT length
+ * along x (0 when unavailable).  Any pointer may be NULL. */
+int32_t cgef_plan_get_row_spectral(const cgef_plan* plan, int32_t* available, int32_t* enabled,
+                                   int32_t* fft_length);
+
 /* Banded footprint of the plan in the reference's CSR form (FilterFootprint, Filtering.jl:327-336):
  * di/dj/w have nentries entries, ptr has nbands+1 (0-based offsets).  Any pointer may be NULL. */
 int32_t cgef_plan_get_footprint(const cgef_plan* plan, int32_t* di, int32_t* dj, double* w, int64_t* ptr);
