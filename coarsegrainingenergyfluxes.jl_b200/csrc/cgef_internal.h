@@ -139,10 +139,11 @@ struct cgef_plan {
   // along x, done as a product of ring spectra
   int rs_L = 0;                 // FFT length along x; 0 = not available for this plan
   int rs_nk = 0;                // spectrum bins kept, rs_L / 2 + 1
+  int rs_nkp = 0;               // row stride of the spectra in bins: rs_nk rounded up to 32
   int rs_nrad = 0;              // Stockham passes
   int rs_rad[16] = {};          // their radices (2, 3, 4 or 5)
   double* d_rs_tw = nullptr;    // rs_L twiddles exp(-2 pi i n / rs_L), (re, im) pairs
-  double* d_rs_k = nullptr;     // kernel spectra / rs_L: [band][row offset][bin]
+  double* d_rs_k = nullptr;     // kernel spectra / rs_L: [band][row offset][bin < rs_nkp], zero past rs_nk
   bool rs_on = false;           // full-grid banded launches use the row-spectral evaluation
   // separable engine
   int di_lim = 0, sep_dj_lim = 0;
@@ -280,7 +281,7 @@ inline size_t banded_partials_bytes(const cgef_plan* p, int na, int nbatch, int 
 // Bytes of the row-spectral evaluation's scratch: the spectra of the source rows and the summed
 // spectra of the target rows, `na` quantities over `nbatch` slices.
 inline size_t rowspec_bytes(const cgef_plan* p, int na, int nbatch) {
-  return 2 * 2 * sizeof(double) * static_cast<size_t>(nbatch) * p->ny * na * p->rs_nk;
+  return 2 * 2 * sizeof(double) * static_cast<size_t>(nbatch) * p->ny * na * p->rs_nkp;
 }
 
 // Scratch of a full-grid banded launch, whichever evaluation the plan uses.

@@ -1011,7 +1011,7 @@ int dispatch_banded(bool def, int R, bool pair, const BandedK& a, cudaStream_t s
 int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                   const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
                   cudaStream_t st, bool direct_only) {
-  if (p->rs_on && !direct_only && nbatch <= 32767)  // grid z of the spectral sums: slices x 2 quantity groups
+  if (p->rs_on && !direct_only && nbatch <= 65535)  // grid z of the row-spectral kernels: one slice each
     return launch_rowspec(p, mode, nf, planes, pitch, np, nbatch, mask, mask_slice_stride, partials, out, st);
   return launch_banded_items(p, mode, nf, planes, pitch, np, nbatch, mask, mask_slice_stride, partials, nullptr, 0,
                              nullptr, 0, out, st);

@@ -35,16 +35,17 @@ namespace cgef {
 
 namespace {
 
-constexpr int kRsThreads = 256;  // threads of the FFT kernels
+constexpr int kRsThreads = 128;  // threads of the FFT kernels
+constexpr int kRsCols = 8;       // input columns a thread of the forward FFT loads at once
 constexpr int kRsMaxL = 4096;    // longest row: two buffers of kRsSeq half-length rows in shared memory
 constexpr int kRsSeq = 2;        // quantities (rows) transformed together by one FFT block
-constexpr int kRsAccThreads = 128;
-constexpr int kRsRows = 4;  // target rows per thread of the spectral accumulation
+constexpr int kRsMaxPairs = 5;  // quantity pairs of the widest pass (9 or 10 quantities): warps per block
 
 struct Fft {
   int L;   // real row length (even)
   int M;   // complex FFT length, L / 2
   int nk;  // bins kept, L / 2 + 1
+  int nkp; // row stride of the spectra in bins: nk rounded up to 32
   int nrad;
   int rad[16];
   const double2* tw;  // exp(-2 pi i n / L), n < L; the length-M roots are every second entry
@@ -58,13 +59,102 @@ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -a.y); }
 
+// Forward root of unity W_R^e = exp(-2 pi i e / R) = (cos, -sin) of 2 pi e / R, for the radices whose
+// in-register DFTs are composite.  The values are the roots to FP64 precision (computed from their
+// series to 50 digits); with the loops unrolled the index is a constant and the table folds away.
+template <int R>
+__device__ __forceinline__ double2 root(int e) {
+  e %= R;
+  if constexpr (R == 8) {
+    constexpr double c[8] = {1.0, 7.07106781186547573e-01, 0.0, -7.07106781186547573e-01,
+                             -1.0, -7.07106781186547573e-01, 0.0, 7.07106781186547573e-01};
+    constexpr double sn[8] = {0.0, 7.07106781186547573e-01, 1.0, 7.07106781186547573e-01,
+                              0.0, -7.07106781186547573e-01, -1.0, -7.07106781186547573e-01};
+    return make_double2(c[e], -sn[e]);
+  } else if constexpr (R == 9) {
+    constexpr double c[9] = {1.0, 7.66044443118978013e-01, 1.73648177666930359e-01, -0.5, -9.39692620785908428e-01,
+                             -9.39692620785908428e-01, -0.5, 1.73648177666930359e-01, 7.66044443118978013e-01};
+    constexpr double sn[9] = {0.0, 6.42787609686539363e-01, 9.84807753012208020e-01, 8.66025403784438597e-01,
+                              3.42020143325668713e-01, -3.42020143325668713e-01, -8.66025403784438597e-01,
+                              -9.84807753012208020e-01, -6.42787609686539363e-01};
+    return make_double2(c[e], -sn[e]);
+  } else if constexpr (R == 10) {
+    constexpr double c[10] = {1.0, 8.09016994374947451e-01, 3.09016994374947451e-01, -3.09016994374947451e-01,
+                              -8.09016994374947451e-01, -1.0, -8.09016994374947451e-01, -3.09016994374947451e-01,
+                              3.09016994374947451e-01, 8.09016994374947451e-01};
+    constexpr double sn[10] = {0.0, 5.87785252292473137e-01, 9.51056516295153531e-01, 9.51056516295153531e-01,
+                               5.87785252292473137e-01, 0.0, -5.87785252292473137e-01, -9.51056516295153531e-01,
+                               -9.51056516295153531e-01, -5.87785252292473137e-01};
+    return make_double2(c[e], -sn[e]);
+  } else {
+    static_assert(R == 16, "composite radices: 8, 9, 10, 16");
+    constexpr double c[16] = {1.0, 9.23879532511286738e-01, 7.07106781186547573e-01, 3.82683432365089782e-01,
+                              0.0, -3.82683432365089782e-01, -7.07106781186547573e-01, -9.23879532511286738e-01,
+                              -1.0, -9.23879532511286738e-01, -7.07106781186547573e-01, -3.82683432365089782e-01,
+                              0.0, 3.82683432365089782e-01, 7.07106781186547573e-01, 9.23879532511286738e-01};
+    constexpr double sn[16] = {0.0, 3.82683432365089782e-01, 7.07106781186547573e-01, 9.23879532511286738e-01,
+                               1.0, 9.23879532511286738e-01, 7.07106781186547573e-01, 3.82683432365089782e-01,
+                               0.0, -3.82683432365089782e-01, -7.07106781186547573e-01, -9.23879532511286738e-01,
+                               -1.0, -9.23879532511286738e-01, -7.07106781186547573e-01, -3.82683432365089782e-01};
+    return make_double2(c[e], -sn[e]);
+  }
+}
+
+// v * W_R^e; the quarter turns are exact swaps.
+template <int R>
+__device__ __forceinline__ double2 rotate(double2 v, int e) {
+  e %= R;
+  if (e == 0) return v;
+  if (4 * e == R) return make_double2(v.y, -v.x);      // -i
+  if (2 * e == R) return make_double2(-v.x, -v.y);     // -1
+  if (4 * e == 3 * R) return make_double2(-v.y, v.x);  // +i
+  return cmul(v, root<R>(e));
+}
+
+template <int R>
+__device__ __forceinline__ void dft(double2 (&v)[R]);
+
+// R = R1 R2 in registers: R2 DFTs of size R1 over the stride-R2 elements, twiddles W_R^(n2 k1), then
+// R1 DFTs of size R2; X[k1 + R1 k2] comes out in natural order.
+template <int R1, int R2>
+__device__ __forceinline__ void dft_split(double2 (&v)[R1 * R2]) {
+  constexpr int R = R1 * R2;
+  double2 t[R];
+#pragma unroll
+  for (int n2 = 0; n2 < R2; ++n2) {
+    double2 u[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) u[n1] = v[n2 + R2 * n1];
+    dft<R1>(u);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) t[k1 * R2 + n2] = rotate<R>(u[k1], n2 * k1);
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < R1; ++k1) {
+    double2 w[R2];
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) w[n2] = t[k1 * R2 + n2];
+    dft<R2>(w);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = w[k2];
+  }
+}
+
 // In-register R-point forward DFT, X_q = sum_r v_r exp(-2 pi i q r / R).
 template <int R>
-__device__ __forceinline__ void dft(double2 (&v)[R], const double2* tw, int M) {
+__device__ __forceinline__ void dft(double2 (&v)[R]) {
   if constexpr (R == 2) {
     const double2 t = v[0];
     v[0] = cadd(t, v[1]);
     v[1] = csub(t, v[1]);
+  } else if constexpr (R == 3) {
+    constexpr double s3 = 8.66025403784438597e-01;  // sin(2 pi / 3)
+    const double2 t1 = cadd(v[1], v[2]);
+    const double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
+    const double2 t3 = make_double2(s3 * (v[1].x - v[2].x), s3 * (v[1].y - v[2].y));
+    v[0] = cadd(v[0], t1);
+    v[1] = make_double2(t2.x + t3.y, t2.y - t3.x);  // t2 - i t3
+    v[2] = make_double2(t2.x - t3.y, t2.y + t3.x);  // t2 + i t3
   } else if constexpr (R == 4) {
     const double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
     const double2 a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
@@ -72,18 +162,29 @@ __device__ __forceinline__ void dft(double2 (&v)[R], const double2* tw, int M) {
     v[2] = csub(a0, a2);
     v[1] = make_double2(a1.x + a3.y, a1.y - a3.x);  // a1 - i a3
     v[3] = make_double2(a1.x - a3.y, a1.y + a3.x);  // a1 + i a3
+  } else if constexpr (R == 5) {
+    constexpr double c1 = 3.09016994374947451e-01, c2 = -8.09016994374947451e-01;  // cos(2 pi / 5), cos(4 pi / 5)
+    constexpr double s1 = 9.51056516295153531e-01, s2 = 5.87785252292473137e-01;   // sin(2 pi / 5), sin(4 pi / 5)
+    const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    const double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    const double2 a1 = make_double2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    const double2 a2 = make_double2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    const double2 b1 = make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+    const double2 b2 = make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = make_double2(a1.x + b1.y, a1.y - b1.x);  // a1 - i b1
+    v[4] = make_double2(a1.x - b1.y, a1.y + b1.x);  // a1 + i b1
+    v[2] = make_double2(a2.x + b2.y, a2.y - b2.x);  // a2 - i b2
+    v[3] = make_double2(a2.x - b2.y, a2.y + b2.x);  // a2 + i b2
+  } else if constexpr (R == 8) {
+    dft_split<2, 4>(v);
+  } else if constexpr (R == 9) {
+    dft_split<3, 3>(v);
+  } else if constexpr (R == 10) {
+    dft_split<2, 5>(v);
   } else {
-    // radix 3 and 5: the roots of unity come from the row's own twiddle table
-    double2 x[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      double2 s = v[0];
-#pragma unroll
-      for (int r = 1; r < R; ++r) s = cadd(s, cmul(v[r], __ldg(tw + 2 * (((q * r) % R) * (M / R)))));
-      x[q] = s;
-    }
-#pragma unroll
-    for (int q = 0; q < R; ++q) v[q] = x[q];
+    static_assert(R == 16, "radices 2, 3, 4, 5, 8, 9, 10, 16");
+    dft_split<4, 4>(v);
   }
 }
 
@@ -106,7 +207,7 @@ __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int 
       v[r] = as[j + r * nb];
       if (r > 0) v[r] = cmul(v[r], __ldg(tw + 2 * (jm * tstride * r)));
     }
-    dft<R>(v, tw, M);
+    dft<R>(v);
     double2* bs = b + sq * M + (j - jm) * R + jm;
 #pragma unroll
     for (int r = 0; r < R; ++r) bs[r * Ns] = v[r];
@@ -115,7 +216,7 @@ __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int 
 
 // Forward DFTs of the `nseq` length-M sequences in `a` (shared memory), `b` as scratch; returns the
 // buffer holding the transforms in natural order.  Every thread of the block must call it.
-__device__ double2* fft_block(double2* a, double2* b, int nseq, const Fft& f) {
+__device__ __forceinline__ double2* fft_block(double2* a, double2* b, int nseq, const Fft& f) {
   int Ns = 1;
   for (int p = 0; p < f.nrad; ++p) {
     const int R = f.rad[p];
@@ -123,7 +224,11 @@ __device__ double2* fft_block(double2* a, double2* b, int nseq, const Fft& f) {
       case 2: stockham_pass<2>(a, b, f.M, Ns, nseq, f.tw); break;
       case 3: stockham_pass<3>(a, b, f.M, Ns, nseq, f.tw); break;
       case 4: stockham_pass<4>(a, b, f.M, Ns, nseq, f.tw); break;
-      default: stockham_pass<5>(a, b, f.M, Ns, nseq, f.tw); break;
+      case 5: stockham_pass<5>(a, b, f.M, Ns, nseq, f.tw); break;
+      case 8: stockham_pass<8>(a, b, f.M, Ns, nseq, f.tw); break;
+      case 9: stockham_pass<9>(a, b, f.M, Ns, nseq, f.tw); break;
+      case 10: stockham_pass<10>(a, b, f.M, Ns, nseq, f.tw); break;
+      default: stockham_pass<16>(a, b, f.M, Ns, nseq, f.tw); break;
     }
     __syncthreads();
     double2* t = a;
@@ -145,6 +250,41 @@ struct RsK {
   double* F;            // [slice][m][row][nx] (aliases Q once the sums are formed)
 };
 
+// Accumulated quantity m of one source cell (the order of expand()): the fields, then (flux modes)
+// their pairwise products, then the mask.
+template <int MODE, int NF, bool DEF>
+__device__ __forceinline__ double quantity(const double (&v)[Cfg<MODE, NF, DEF>::NP], int m) {
+  using C = Cfg<MODE, NF, DEF>;
+  if (DEF && m == C::NA - 1) return v[C::NP - 1];
+  if constexpr (MODE == kModePiSphere) {
+    switch (m) {
+      case 0: return v[0];
+      case 1: return v[1];
+      case 2: return v[2];
+      case 3: return v[0] * v[0];
+      case 4: return v[0] * v[1];
+      case 5: return v[0] * v[2];
+      case 6: return v[1] * v[1];
+      case 7: return v[1] * v[2];
+      default: return v[2] * v[2];
+    }
+  } else if constexpr (MODE == kModePiCart) {
+    switch (m) {
+      case 0: return v[0];
+      case 1: return v[1];
+      case 2: return v[0] * v[0];
+      case 3: return v[0] * v[1];
+      default: return v[1] * v[1];
+    }
+  } else {
+    double r = v[0];
+#pragma unroll
+    for (int f = 1; f < NF; ++f)
+      if (m == f) r = v[f];
+    return r;
+  }
+}
+
 // Real DFTs of up to kRsSeq of the NA accumulated quantities of one source row (slice, row): each
 // row's even and odd samples form one half-length complex sequence z, and with Z = FFT(z) the row's
 // spectrum is X_k = E_k + exp(-2 pi i k / L) O_k, E_k = (Z_k + conj Z_{M-k}) / 2,
@@ -160,23 +300,25 @@ __global__ void __launch_bounds__(kRsThreads) rs_forward_kernel(RsK k) {
   const int nseq = min(kRsSeq, C::NA - m0);
   const double* row = k.planes + s * k.slice_stride + static_cast<int64_t>(jr) * k.pitch + k.halo;
   double* ad = reinterpret_cast<double*>(a);
-  for (int i = threadIdx.x; i < k.f.L; i += blockDim.x) {
-    double x[kRsSeq] = {};
-    if (i < k.nx) {
-      double v[C::NP];
+  // kRsCols columns per thread at a time, their loads issued together
+  for (int i0 = 0; i0 < k.f.L; i0 += kRsCols * kRsThreads) {
+    double v[kRsCols][C::NP];
 #pragma unroll
-      for (int pl = 0; pl < C::NP; ++pl) v[pl] = row[pl * k.plane_stride + i];
-      double q[C::NA];
-      expand<MODE, NF, DEF>(v, q);
+    for (int c = 0; c < kRsCols; ++c) {
+      const int i = i0 + c * kRsThreads + threadIdx.x;
+      const int ic = i < k.nx ? i : 0;
 #pragma unroll
-      for (int m = 0; m < C::NA; ++m)
-#pragma unroll
-        for (int e = 0; e < kRsSeq; ++e)
-          if (m == m0 + e) x[e] = q[m];
+      for (int pl = 0; pl < C::NP; ++pl) v[c][pl] = row[pl * k.plane_stride + ic];
     }
 #pragma unroll
-    for (int e = 0; e < kRsSeq; ++e)
-      if (e < nseq) ad[e * k.f.L + i] = x[e];  // sample i of sequence e: z[i/2].x (even i) or .y (odd)
+    for (int c = 0; c < kRsCols; ++c) {
+      const int i = i0 + c * kRsThreads + threadIdx.x;
+      if (i >= k.f.L) break;
+#pragma unroll
+      for (int e = 0; e < kRsSeq; ++e)
+        if (e < nseq)  // sample i of sequence e: z[i/2].x (even i) or .y (odd)
+          ad[e * k.f.L + i] = i < k.nx ? quantity<MODE, NF, DEF>(v[c], m0 + e) : 0.0;
+    }
   }
   __syncthreads();
   const double2* z = fft_block(a, b, nseq, k.f);
@@ -187,62 +329,111 @@ __global__ void __launch_bounds__(kRsThreads) rs_forward_kernel(RsK k) {
     const double2 zq = ze[q == M ? 0 : q], zc = conj2(ze[q == 0 ? 0 : M - q]);
     const double2 E = make_double2(0.5 * (zq.x + zc.x), 0.5 * (zq.y + zc.y));
     const double2 O = make_double2(0.5 * (zq.y - zc.y), -0.5 * (zq.x - zc.x));  // (zq - zc) / 2i
-    k.Q[((static_cast<int64_t>(s) * k.ny + jr) * C::NA + m0 + e) * k.f.nk + q] = cadd(E, cmul(__ldg(k.f.tw + q), O));
+    k.Q[((static_cast<int64_t>(s) * k.ny + jr) * C::NA + m0 + e) * k.f.nkp + q] = cadd(E, cmul(__ldg(k.f.tw + q), O));
   }
 }
 
-// S_j = sum_dj K_{j,dj} Q_{j+dj} per bin: one thread per (bin, kRsRows target rows, group of NQ
-// quantities of one slice).  Source rows outside a bounded y axis are skipped, as the direct sum
-// skips them; on a periodic y axis they wrap.
-template <int NQ>
-__global__ void __launch_bounds__(kRsAccThreads) rs_accumulate_kernel(RsK k, int na, int ngroups) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j0 = blockIdx.y * kRsRows;
-  const int s = blockIdx.z / ngroups;
-  const int mb = (blockIdx.z - s * ngroups) * NQ;
-  if (q >= k.f.nk) return;
-  const int nq = min(NQ, na - mb);
-  const int nk = k.f.nk;
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, bool fill) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  const int n = fill ? 16 : 0;  // 0: the 16 bytes are zero-filled and nothing is read
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gsrc), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// S_j = sum_dj K_{j,dj} Q_{j+dj} per bin.  A block owns 32 bins x TJ target rows x every quantity and
+// walks the TJ + 2D source rows its band touches; per source row it stages that row's spectra (all
+// quantities) and the TJ kernel-spectrum slices that apply to it in shared memory through a
+// kAccStages-deep cp.async pipeline, and each warp (one pair of quantities x 8 target rows) adds
+// them into its registers.  Rows off a bounded y axis stage zeros (the direct sum skips them); on a
+// periodic y axis they wrap.
+constexpr int kAccStages = 4;
+
+template <int TJ>
+__global__ void __launch_bounds__(32 * kRsMaxPairs * (TJ / 8), TJ == 16 ? 2 : 1) rs_accumulate_kernel(RsK k, int na) {
+  extern __shared__ __align__(16) unsigned char rs_acc_smem[];
+  const int npairs = (na + 1) / 2;
+  const int qbytes = na * 32 * 16;
+  const int sbytes = qbytes + TJ * 32 * 8;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int pr = warp % npairs, rg = warp / npairs;
+  const int q0 = blockIdx.x * 32;
+  const int j0 = blockIdx.y * TJ;
+  const int s = blockIdx.z;
+  const int nkp = k.f.nkp;
   const int W = 2 * k.D + 1;
-  double2 acc[kRsRows][NQ];
-#pragma unroll
-  for (int t = 0; t < kRsRows; ++t)
-#pragma unroll
-    for (int m = 0; m < NQ; ++m) acc[t][m] = make_double2(0.0, 0.0);
-  const double2* Qs = k.Q + static_cast<int64_t>(s) * k.ny * na * nk;
-  for (int jr = j0 - k.D; jr < j0 + kRsRows + k.D; ++jr) {
+  const int nsteps = TJ + 2 * k.D;
+  const double2* Qs = k.Q + static_cast<int64_t>(s) * k.ny * na * nkp + q0;
+
+  auto issue = [&](int step, int buf) {
+    unsigned char* b = rs_acc_smem + buf * sbytes;
+    const int jr = j0 - k.D + step;
     int jj = jr;
+    bool row_ok = true;
     if (jr < 0 || jr >= k.ny) {
-      if (!k.periodic_y) continue;
-      jj = jr % k.ny;
-      if (jj < 0) jj += k.ny;
-    }
-    double2 qv[NQ];
-    const double2* qrow = Qs + (static_cast<int64_t>(jj) * na + mb) * nk + q;
-#pragma unroll
-    for (int m = 0; m < NQ; ++m) qv[m] = m < nq ? qrow[m * nk] : make_double2(0.0, 0.0);
-#pragma unroll
-    for (int t = 0; t < kRsRows; ++t) {
-      const int j = j0 + t;
-      const int dj = jr - j;
-      if (j < k.ny && dj >= -k.D && dj <= k.D) {
-        const double kv = __ldg(k.kspec + (static_cast<int64_t>(k.band_stride ? j : 0) * W + dj + k.D) * nk + q);
-#pragma unroll
-        for (int m = 0; m < NQ; ++m) {
-          acc[t][m].x = fma(kv, qv[m].x, acc[t][m].x);
-          acc[t][m].y = fma(kv, qv[m].y, acc[t][m].y);
-        }
+      if (k.periodic_y) {
+        jj = jr % k.ny;
+        if (jj < 0) jj += k.ny;
+      } else {
+        row_ok = false;
+        jj = 0;
       }
     }
+    const double2* qsrc = Qs + static_cast<int64_t>(jj) * na * nkp;
+    for (int c = threadIdx.x; c < na * 32; c += blockDim.x)
+      cp_async16(b + c * 16, qsrc + static_cast<int64_t>(c >> 5) * nkp + (c & 31), row_ok);
+    for (int c = threadIdx.x; c < TJ * 16; c += blockDim.x) {
+      const int t = c >> 4;
+      const int j = j0 + t;
+      const int dj = jr - j;
+      const bool ok = row_ok && j < k.ny && dj >= -k.D && dj <= k.D;
+      const int64_t krow = ok ? static_cast<int64_t>(k.band_stride ? j : 0) * W + dj + k.D : 0;
+      cp_async16(b + qbytes + c * 16, k.kspec + krow * nkp + q0 + 2 * (c & 15), ok);
+    }
+  };
+
+  double2 acc[8][2];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) acc[t][0] = acc[t][1] = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int st = 0; st < kAccStages - 1; ++st) {
+    if (st < nsteps) issue(st, st);
+    cp_async_commit();
   }
+  const bool two = 2 * pr + 1 < na;
+  for (int st = 0; st < nsteps; ++st) {
+    cp_async_wait<kAccStages - 2>();
+    __syncthreads();
+    const int nxt = st + kAccStages - 1;
+    if (nxt < nsteps) issue(nxt, nxt % kAccStages);
+    cp_async_commit();
+    const unsigned char* b = rs_acc_smem + (st % kAccStages) * sbytes;
+    const double2* qb = reinterpret_cast<const double2*>(b);
+    const double* kb = reinterpret_cast<const double*>(b + qbytes) + rg * 8 * 32 + lane;
+    const double2 a0 = qb[2 * pr * 32 + lane];
+    const double2 a1 = two ? qb[(2 * pr + 1) * 32 + lane] : make_double2(0.0, 0.0);
 #pragma unroll
-  for (int t = 0; t < kRsRows; ++t) {
-    const int j = j0 + t;
+    for (int t = 0; t < 8; ++t) {
+      const double kv = kb[t * 32];
+      acc[t][0].x = fma(kv, a0.x, acc[t][0].x);
+      acc[t][0].y = fma(kv, a0.y, acc[t][0].y);
+      acc[t][1].x = fma(kv, a1.x, acc[t][1].x);
+      acc[t][1].y = fma(kv, a1.y, acc[t][1].y);
+    }
+  }
+  cp_async_wait<0>();
+  double2* Ss = k.S + static_cast<int64_t>(s) * k.ny * na * nkp + static_cast<int64_t>(2 * pr) * nkp + q0 + lane;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int j = j0 + rg * 8 + t;
     if (j >= k.ny) break;
-    double2* srow = k.S + ((static_cast<int64_t>(s) * k.ny + j) * na + mb) * nk + q;
-#pragma unroll
-    for (int m = 0; m < NQ; ++m)
-      if (m < nq) srow[m * nk] = acc[t][m];
+    double2* sr = Ss + static_cast<int64_t>(j) * na * nkp;
+    sr[0] = acc[t][0];
+    if (two) sr[nkp] = acc[t][1];
   }
 }
 
@@ -258,11 +449,11 @@ __global__ void __launch_bounds__(kRsThreads) rs_inverse_kernel(RsK k) {
   double2* b = rs_smem + kRsSeq * M;
   const int m0 = blockIdx.x * kRsSeq, j = blockIdx.y, s = blockIdx.z;
   const int nseq = min(kRsSeq, NA - m0);
-  const double2* S = k.S + ((static_cast<int64_t>(s) * k.ny + j) * NA + m0) * k.f.nk;
+  const double2* S = k.S + ((static_cast<int64_t>(s) * k.ny + j) * NA + m0) * k.f.nkp;
   for (int t = threadIdx.x; t < nseq * M; t += blockDim.x) {
     const int e = t / M;
     const int q = t - e * M;
-    const double2 sq = S[e * k.f.nk + q], sc = conj2(S[e * k.f.nk + M - q]);
+    const double2 sq = S[e * k.f.nkp + q], sc = conj2(S[e * k.f.nkp + M - q]);
     const double2 Ep = cadd(sq, sc);
     const double2 Op = cmul(csub(sq, sc), conj2(__ldg(k.f.tw + q)));
     // conj(E' + i O')
@@ -296,13 +487,13 @@ __global__ void __launch_bounds__(128) rs_finish_kernel(BandedK a, const double*
 // w_a cos(2 pi q a / L) for a ring-closing row (its column -a), with the cosines read from the
 // twiddle table at (q d) mod L.
 __global__ void rs_kspec_kernel(const BandRow* rows, int64_t nrows, const double* w, const double2* tw, int L, int nk,
-                                double* kspec) {
+                                int nkp, double* kspec) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t r = blockIdx.y + static_cast<int64_t>(blockIdx.z) * gridDim.y;
-  if (q >= nk || r >= nrows) return;
+  if (q >= nkp || r >= nrows) return;
   const BandRow br = rows[r];
   double sum = 0.0;
-  if (br.a >= 0) {
+  if (br.a >= 0 && q < nk) {
     const double* wr = w + br.woff;
     const int sym = min(br.a, br.hi);
     sum = wr[0];
@@ -310,7 +501,7 @@ __global__ void rs_kspec_kernel(const BandRow* rows, int64_t nrows, const double
       sum = fma(2.0 * wr[d], __ldg(&tw[static_cast<int64_t>(q) * d % L].x), sum);
     if (br.hi < br.a) sum = fma(wr[br.a], __ldg(&tw[static_cast<int64_t>(q) * br.a % L].x), sum);
   }
-  kspec[r * nk + q] = sum / L;
+  kspec[r * nkp + q] = sum / L;
 }
 
 int rs_check(const char* what) {
@@ -341,12 +532,11 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
   using C = Cfg<MODE, NF, DEF>;
   constexpr int NA = C::NA;
   constexpr int NC = (NA + kRsSeq - 1) / kRsSeq;
-  constexpr int NQ = NA <= 5 ? NA : (NA + 1) / 2;
-  constexpr int ngroups = (NA + NQ - 1) / NQ;
   RsK k{};
   k.f.L = p->rs_L;
   k.f.M = p->rs_L / 2;
   k.f.nk = p->rs_nk;
+  k.f.nkp = p->rs_nkp;
   k.f.nrad = p->rs_nrad;
   for (int i = 0; i < p->rs_nrad; ++i) k.f.rad[i] = p->rs_rad[i];
   k.f.tw = reinterpret_cast<const double2*>(p->d_rs_tw);
@@ -362,7 +552,7 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
   k.periodic_y = p->periodic_y;
   k.nslices = a.nslices;
   k.kspec = p->d_rs_k;
-  const size_t spec = static_cast<size_t>(a.nslices) * p->ny * NA * p->rs_nk;
+  const size_t spec = static_cast<size_t>(a.nslices) * p->ny * NA * p->rs_nkp;
   k.Q = reinterpret_cast<double2*>(scratch);
   k.S = k.Q + spec;
   k.F = scratch;  // Q is dead once S is formed
@@ -375,10 +565,19 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
   rs_forward_kernel<MODE, NF, DEF><<<rows, kRsThreads, smem, st>>>(k);
   rc = rs_check("rs_forward_kernel");
   if (rc == CGEF_OK) {
-    const dim3 g((p->rs_nk + kRsAccThreads - 1) / kRsAccThreads, (p->ny + kRsRows - 1) / kRsRows,
-                 a.nslices * ngroups);
-    rs_accumulate_kernel<NQ><<<g, kRsAccThreads, 0, st>>>(k, NA, ngroups);
-    rc = rs_check("rs_accumulate_kernel");
+    constexpr int npairs = (NA + 1) / 2;
+    static_assert(npairs <= kRsMaxPairs, "quantity pairs per block");
+    const int tj = p->D >= 48 ? 32 : 16;
+    const int acc_smem = kAccStages * (NA * 32 * 16 + tj * 32 * 8);
+    const dim3 g(p->rs_nkp / 32, (p->ny + tj - 1) / tj, a.nslices);
+    if (tj == 32) {
+      if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<32>))) == CGEF_OK)
+        rs_accumulate_kernel<32><<<g, 32 * npairs * 4, acc_smem, st>>>(k, NA);
+    } else {
+      if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<16>))) == CGEF_OK)
+        rs_accumulate_kernel<16><<<g, 32 * npairs * 2, acc_smem, st>>>(k, NA);
+    }
+    if (rc == CGEF_OK) rc = rs_check("rs_accumulate_kernel");
   }
   if (rc == CGEF_OK) {
     rs_inverse_kernel<NA><<<rows, kRsThreads, smem, st>>>(k);
@@ -397,15 +596,23 @@ int dispatch_rowspec(bool def, const cgef_plan* p, const BandedK& a, double* scr
   return def ? run_rowspec<MODE, NF, true>(p, a, scratch, st) : run_rowspec<MODE, NF, false>(p, a, scratch, st);
 }
 
-// Radices of a Stockham plan for L (fours first), or empty when L has a prime factor above 5.
-std::vector<int> fft_radices(int L) {
+// Radices of a Stockham plan for M with few passes (tens, nines, then sixteens, eights, fours), or
+// empty when M has a prime factor above 5.
+std::vector<int> fft_radices(int M) {
+  int e2 = 0, e3 = 0, e5 = 0;
+  while (M % 2 == 0) M /= 2, ++e2;
+  while (M % 3 == 0) M /= 3, ++e3;
+  while (M % 5 == 0) M /= 5, ++e5;
   std::vector<int> rad;
-  for (int r : {4, 2, 3, 5})
-    while (L % r == 0) {
-      rad.push_back(r);
-      L /= r;
-    }
-  if (L != 1) rad.clear();
+  if (M != 1) return rad;
+  for (; e5 > 0 && e2 > 0; --e5, --e2) rad.push_back(10);
+  for (; e5 > 0; --e5) rad.push_back(5);
+  for (; e3 >= 2; e3 -= 2) rad.push_back(9);
+  if (e3 == 1) rad.push_back(3);
+  for (; e2 >= 4; e2 -= 4) rad.push_back(16);
+  if (e2 == 3) rad.push_back(8);
+  if (e2 == 2) rad.push_back(4);
+  if (e2 == 1) rad.push_back(2);
   return rad;
 }
 
@@ -454,8 +661,9 @@ int build_row_spectra(cgef_plan* p) {
   const std::vector<int> rad = fft_radices(L / 2);
   if (rad.empty() || rad.size() > 16) return CGEF_OK;
   const int nk = L / 2 + 1;
+  const int nkp = (nk + 31) / 32 * 32;
   const int64_t nrows = static_cast<int64_t>(p->h_rows.size());
-  const size_t kbytes = sizeof(double) * static_cast<size_t>(nrows) * nk;
+  const size_t kbytes = sizeof(double) * static_cast<size_t>(nrows) * nkp;
   if (kbytes > (size_t(8) << 30)) return CGEF_OK;
 
   std::vector<double> tw(2 * static_cast<size_t>(L));
@@ -472,13 +680,14 @@ int build_row_spectra(cgef_plan* p) {
   e = cudaMalloc(reinterpret_cast<void**>(&p->d_rs_k), kbytes);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(row-spectral kernel spectra)");
   const int64_t zchunks = (nrows + 65534) / 65535;
-  const dim3 g((nk + 127) / 128, static_cast<unsigned>(std::min<int64_t>(nrows, 65535)), static_cast<unsigned>(zchunks));
-  rs_kspec_kernel<<<g, 128>>>(p->d_rows, nrows, p->d_w, reinterpret_cast<const double2*>(p->d_rs_tw), L, nk,
+  const dim3 g((nkp + 127) / 128, static_cast<unsigned>(std::min<int64_t>(nrows, 65535)), static_cast<unsigned>(zchunks));
+  rs_kspec_kernel<<<g, 128>>>(p->d_rows, nrows, p->d_w, reinterpret_cast<const double2*>(p->d_rs_tw), L, nk, nkp,
                                p->d_rs_k);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "rs_kspec_kernel");
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cuda_fail(e, "rs_kspec_kernel");
   p->rs_L = L;
   p->rs_nk = nk;
+  p->rs_nkp = nkp;
   p->rs_nrad = static_cast<int>(rad.size());
   for (size_t i = 0; i < rad.size(); ++i) p->rs_rad[i] = rad[i];
   p->rs_on = true;
