@@ -48,7 +48,8 @@ struct Fft {
   int nkp; // row stride of the spectra in bins: nk rounded up to 32
   int nrad;
   int rad[16];
-  const double2* tw;  // exp(-2 pi i n / L), n < L; the length-M roots are every second entry
+  unsigned magic[16];  // ceil(2^32 / Ns) of each pass, Ns = the product of the earlier radices
+  const double2* tw;   // exp(-2 pi i n / L), n < L; the length-M roots are every second entry
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -190,27 +191,29 @@ __device__ __forceinline__ void dft(double2 (&v)[R]) {
 
 // One Stockham autosort pass of radix R over `nseq` independent length-M sequences stored one after
 // another: butterfly j of a sequence reads a[j + r M/R], twiddles by exp(-2 pi i (j mod Ns) r /
-// (Ns R)), and writes b[(j / Ns) Ns R + j mod Ns + r Ns].
+// (Ns R)), and writes b[(j / Ns) Ns R + j mod Ns + r Ns].  j / Ns is __umulhi(j, ns_magic) with
+// ns_magic = ceil(2^32 / Ns) (Ns > 1), exact for j, Ns < 2^16.
 template <int R>
-__device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int M, int Ns, int nseq,
-                                              const double2* tw) {
+__device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int M, int Ns, unsigned ns_magic,
+                                              int nseq, const double2* tw) {
   const int nb = M / R;
-  const int tstride = M / (Ns * R);
-  for (int t = threadIdx.x; t < nseq * nb; t += blockDim.x) {
-    const int sq = t / nb;
-    const int j = t - sq * nb;
-    const int jm = j % Ns;
+  const int tstride = 2 * (M / (Ns * R));  // the length-M roots are every second table entry
+  for (int sq = 0; sq < nseq; ++sq) {
     const double2* as = a + sq * M;
-    double2 v[R];
+    double2* bsq = b + sq * M;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+      const int jq = Ns == 1 ? j : static_cast<int>(__umulhi(static_cast<unsigned>(j), ns_magic));
+      const int jm = j - jq * Ns;
+      double2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      v[r] = as[j + r * nb];
-      if (r > 0) v[r] = cmul(v[r], __ldg(tw + 2 * (jm * tstride * r)));
+      for (int r = 0; r < R; ++r) v[r] = as[j + r * nb];
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + jm * tstride * r));
+      dft<R>(v);
+      double2* bs = bsq + jq * Ns * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) bs[r * Ns] = v[r];
     }
-    dft<R>(v);
-    double2* bs = b + sq * M + (j - jm) * R + jm;
-#pragma unroll
-    for (int r = 0; r < R; ++r) bs[r * Ns] = v[r];
   }
 }
 
@@ -220,15 +223,16 @@ __device__ __forceinline__ double2* fft_block(double2* a, double2* b, int nseq, 
   int Ns = 1;
   for (int p = 0; p < f.nrad; ++p) {
     const int R = f.rad[p];
+    const unsigned mg = f.magic[p];
     switch (R) {
-      case 2: stockham_pass<2>(a, b, f.M, Ns, nseq, f.tw); break;
-      case 3: stockham_pass<3>(a, b, f.M, Ns, nseq, f.tw); break;
-      case 4: stockham_pass<4>(a, b, f.M, Ns, nseq, f.tw); break;
-      case 5: stockham_pass<5>(a, b, f.M, Ns, nseq, f.tw); break;
-      case 8: stockham_pass<8>(a, b, f.M, Ns, nseq, f.tw); break;
-      case 9: stockham_pass<9>(a, b, f.M, Ns, nseq, f.tw); break;
-      case 10: stockham_pass<10>(a, b, f.M, Ns, nseq, f.tw); break;
-      default: stockham_pass<16>(a, b, f.M, Ns, nseq, f.tw); break;
+      case 2: stockham_pass<2>(a, b, f.M, Ns, mg, nseq, f.tw); break;
+      case 3: stockham_pass<3>(a, b, f.M, Ns, mg, nseq, f.tw); break;
+      case 4: stockham_pass<4>(a, b, f.M, Ns, mg, nseq, f.tw); break;
+      case 5: stockham_pass<5>(a, b, f.M, Ns, mg, nseq, f.tw); break;
+      case 8: stockham_pass<8>(a, b, f.M, Ns, mg, nseq, f.tw); break;
+      case 9: stockham_pass<9>(a, b, f.M, Ns, mg, nseq, f.tw); break;
+      case 10: stockham_pass<10>(a, b, f.M, Ns, mg, nseq, f.tw); break;
+      default: stockham_pass<16>(a, b, f.M, Ns, mg, nseq, f.tw); break;
     }
     __syncthreads();
     double2* t = a;
@@ -322,14 +326,15 @@ __global__ void __launch_bounds__(kRsThreads) rs_forward_kernel(RsK k) {
   }
   __syncthreads();
   const double2* z = fft_block(a, b, nseq, k.f);
-  for (int t = threadIdx.x; t < nseq * k.f.nk; t += blockDim.x) {
-    const int e = t / k.f.nk;
-    const int q = t - e * k.f.nk;
+  for (int e = 0; e < nseq; ++e) {
     const double2* ze = z + e * M;
-    const double2 zq = ze[q == M ? 0 : q], zc = conj2(ze[q == 0 ? 0 : M - q]);
-    const double2 E = make_double2(0.5 * (zq.x + zc.x), 0.5 * (zq.y + zc.y));
-    const double2 O = make_double2(0.5 * (zq.y - zc.y), -0.5 * (zq.x - zc.x));  // (zq - zc) / 2i
-    k.Q[((static_cast<int64_t>(s) * k.ny + jr) * C::NA + m0 + e) * k.f.nkp + q] = cadd(E, cmul(__ldg(k.f.tw + q), O));
+    double2* Qe = k.Q + ((static_cast<int64_t>(s) * k.ny + jr) * C::NA + m0 + e) * k.f.nkp;
+    for (int q = threadIdx.x; q < k.f.nk; q += blockDim.x) {
+      const double2 zq = ze[q == M ? 0 : q], zc = conj2(ze[q == 0 ? 0 : M - q]);
+      const double2 E = make_double2(0.5 * (zq.x + zc.x), 0.5 * (zq.y + zc.y));
+      const double2 O = make_double2(0.5 * (zq.y - zc.y), -0.5 * (zq.x - zc.x));  // (zq - zc) / 2i
+      Qe[q] = cadd(E, cmul(__ldg(k.f.tw + q), O));
+    }
   }
 }
 
@@ -352,10 +357,14 @@ __device__ __forceinline__ void cp_async_wait() {
 // periodic y axis they wrap.
 constexpr int kAccStages = 4;
 
-template <int TJ>
-__global__ void __launch_bounds__(32 * kRsMaxPairs * (TJ / 8), TJ == 16 ? 2 : 1) rs_accumulate_kernel(RsK k, int na) {
+template <int TJ, int NA>
+__global__ void __launch_bounds__(32 * ((NA + 1) / 2) * (TJ / 8), TJ == 16 ? 2 : 1) rs_accumulate_kernel(RsK k) {
   extern __shared__ __align__(16) unsigned char rs_acc_smem[];
-  const int npairs = (na + 1) / 2;
+  constexpr int na = NA;
+  constexpr int npairs = (NA + 1) / 2;
+  constexpr int kThreads = 32 * npairs * (TJ / 8);
+  constexpr int kKChunks = (TJ * 16 + kThreads - 1) / kThreads;  // 16-byte kernel-spectrum chunks per thread and step
+  static_assert(kThreads >= NA * 32, "one chunk of the source spectra per thread");
   const int qbytes = na * 32 * 16;
   const int sbytes = qbytes + TJ * 32 * 8;
   const int lane = threadIdx.x & 31;
@@ -366,33 +375,45 @@ __global__ void __launch_bounds__(32 * kRsMaxPairs * (TJ / 8), TJ == 16 ? 2 : 1)
   const int s = blockIdx.z;
   const int nkp = k.f.nkp;
   const int W = 2 * k.D + 1;
-  const int nsteps = TJ + 2 * k.D;
-  const double2* Qs = k.Q + static_cast<int64_t>(s) * k.ny * na * nkp + q0;
+  // source rows jr = j0 - D + step; off a bounded y axis they are skipped
+  int st0 = 0, st1 = TJ + 2 * k.D;
+  if (!k.periodic_y) {
+    st0 = max(0, k.D - j0);
+    st1 = min(st1, k.ny - j0 + k.D);
+  }
+  // this thread's copies: one chunk of the source row's spectra (the block has at least na*32
+  // threads) and up to kKChunks slices of kernel spectra, their offsets fixed but for the row
+  const bool q_copy = static_cast<int>(threadIdx.x) < na * 32;
+  const double2* q_src = k.Q + static_cast<int64_t>(s) * k.ny * na * nkp + q0 +
+                         (q_copy ? static_cast<int64_t>(threadIdx.x >> 5) * nkp + (threadIdx.x & 31) : 0);
+  int k_j[kKChunks];
+  int64_t k_base[kKChunks];
+#pragma unroll
+  for (int i = 0; i < kKChunks; ++i) {
+    const int c = threadIdx.x + i * kThreads;
+    const int t = c >> 4;
+    k_j[i] = c < TJ * 16 ? j0 + t : k.ny;  // k.ny: no copy
+    k_base[i] = static_cast<int64_t>(k.band_stride ? k_j[i] : 0) * W + k.D - k_j[i];  // + jr = the band row
+    k_base[i] = k_base[i] * nkp + q0 + 2 * (c & 15);
+  }
 
   auto issue = [&](int step, int buf) {
     unsigned char* b = rs_acc_smem + buf * sbytes;
-    const int jr = j0 - k.D + step;
-    int jj = jr;
-    bool row_ok = true;
-    if (jr < 0 || jr >= k.ny) {
-      if (k.periodic_y) {
-        jj = jr % k.ny;
-        if (jj < 0) jj += k.ny;
-      } else {
-        row_ok = false;
-        jj = 0;
-      }
+    int jr = j0 - k.D + step;
+    if (jr < 0 || jr >= k.ny) {  // only reached on a periodic y axis
+      jr %= k.ny;
+      if (jr < 0) jr += k.ny;
     }
-    const double2* qsrc = Qs + static_cast<int64_t>(jj) * na * nkp;
-    for (int c = threadIdx.x; c < na * 32; c += blockDim.x)
-      cp_async16(b + c * 16, qsrc + static_cast<int64_t>(c >> 5) * nkp + (c & 31), row_ok);
-    for (int c = threadIdx.x; c < TJ * 16; c += blockDim.x) {
-      const int t = c >> 4;
-      const int j = j0 + t;
-      const int dj = jr - j;
-      const bool ok = row_ok && j < k.ny && dj >= -k.D && dj <= k.D;
-      const int64_t krow = ok ? static_cast<int64_t>(k.band_stride ? j : 0) * W + dj + k.D : 0;
-      cp_async16(b + qbytes + c * 16, k.kspec + krow * nkp + q0 + 2 * (c & 15), ok);
+    const int jraw = j0 - k.D + step;
+    if (q_copy) cp_async16(b + threadIdx.x * 16, q_src + static_cast<int64_t>(jr) * na * nkp, true);
+#pragma unroll
+    for (int i = 0; i < kKChunks; ++i) {
+      const int c = threadIdx.x + i * kThreads;
+      if (c < TJ * 16) {
+        const int dj = jraw - k_j[i];
+        const bool ok = k_j[i] < k.ny && dj >= -k.D && dj <= k.D;
+        cp_async16(b + qbytes + c * 16, k.kspec + (ok ? k_base[i] + static_cast<int64_t>(jraw) * nkp : 0), ok);
+      }
     }
   };
 
@@ -400,18 +421,18 @@ __global__ void __launch_bounds__(32 * kRsMaxPairs * (TJ / 8), TJ == 16 ? 2 : 1)
 #pragma unroll
   for (int t = 0; t < 8; ++t) acc[t][0] = acc[t][1] = make_double2(0.0, 0.0);
 #pragma unroll
-  for (int st = 0; st < kAccStages - 1; ++st) {
-    if (st < nsteps) issue(st, st);
+  for (int i = 0; i < kAccStages - 1; ++i) {
+    if (st0 + i < st1) issue(st0 + i, i);
     cp_async_commit();
   }
   const bool two = 2 * pr + 1 < na;
-  for (int st = 0; st < nsteps; ++st) {
+  for (int st = st0; st < st1; ++st) {
     cp_async_wait<kAccStages - 2>();
     __syncthreads();
     const int nxt = st + kAccStages - 1;
-    if (nxt < nsteps) issue(nxt, nxt % kAccStages);
+    if (nxt < st1) issue(nxt, (nxt - st0) % kAccStages);
     cp_async_commit();
-    const unsigned char* b = rs_acc_smem + (st % kAccStages) * sbytes;
+    const unsigned char* b = rs_acc_smem + ((st - st0) % kAccStages) * sbytes;
     const double2* qb = reinterpret_cast<const double2*>(b);
     const double* kb = reinterpret_cast<const double*>(b + qbytes) + rg * 8 * 32 + lane;
     const double2 a0 = qb[2 * pr * 32 + lane];
@@ -450,22 +471,20 @@ __global__ void __launch_bounds__(kRsThreads) rs_inverse_kernel(RsK k) {
   const int m0 = blockIdx.x * kRsSeq, j = blockIdx.y, s = blockIdx.z;
   const int nseq = min(kRsSeq, NA - m0);
   const double2* S = k.S + ((static_cast<int64_t>(s) * k.ny + j) * NA + m0) * k.f.nkp;
-  for (int t = threadIdx.x; t < nseq * M; t += blockDim.x) {
-    const int e = t / M;
-    const int q = t - e * M;
-    const double2 sq = S[e * k.f.nkp + q], sc = conj2(S[e * k.f.nkp + M - q]);
-    const double2 Ep = cadd(sq, sc);
-    const double2 Op = cmul(csub(sq, sc), conj2(__ldg(k.f.tw + q)));
-    // conj(E' + i O')
-    a[e * M + q] = make_double2(Ep.x - Op.y, -(Ep.y + Op.x));
-  }
+  for (int e = 0; e < nseq; ++e)
+    for (int q = threadIdx.x; q < M; q += blockDim.x) {
+      const double2 sq = S[e * k.f.nkp + q], sc = conj2(S[e * k.f.nkp + M - q]);
+      const double2 Ep = cadd(sq, sc);
+      const double2 Op = cmul(csub(sq, sc), conj2(__ldg(k.f.tw + q)));
+      // conj(E' + i O')
+      a[e * M + q] = make_double2(Ep.x - Op.y, -(Ep.y + Op.x));
+    }
   __syncthreads();
   const double2* z = fft_block(a, b, nseq, k.f);
-  for (int t = threadIdx.x; t < nseq * k.nx; t += blockDim.x) {
-    const int e = t / k.nx;
-    const int i = t - e * k.nx;
-    const double2 w = z[e * M + (i >> 1)];
-    k.F[((static_cast<int64_t>(s) * NA + m0 + e) * k.ny + j) * k.nx + i] = (i & 1) ? -w.y : w.x;
+  for (int e = 0; e < nseq; ++e) {
+    double* Fe = k.F + ((static_cast<int64_t>(s) * NA + m0 + e) * k.ny + j) * k.nx;
+    const double* zd = reinterpret_cast<const double*>(z + e * M);
+    for (int i = threadIdx.x; i < k.nx; i += blockDim.x) Fe[i] = (i & 1) ? -zd[i] : zd[i];
   }
 }
 
@@ -538,7 +557,11 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
   k.f.nk = p->rs_nk;
   k.f.nkp = p->rs_nkp;
   k.f.nrad = p->rs_nrad;
-  for (int i = 0; i < p->rs_nrad; ++i) k.f.rad[i] = p->rs_rad[i];
+  for (int i = 0, ns = 1; i < p->rs_nrad; ++i) {
+    k.f.rad[i] = p->rs_rad[i];
+    k.f.magic[i] = ns == 1 ? 0u : static_cast<unsigned>(((uint64_t(1) << 32) + ns - 1) / ns);
+    ns *= p->rs_rad[i];
+  }
   k.f.tw = reinterpret_cast<const double2*>(p->d_rs_tw);
   k.planes = a.planes;
   k.plane_stride = a.plane_stride;
@@ -571,11 +594,11 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
     const int acc_smem = kAccStages * (NA * 32 * 16 + tj * 32 * 8);
     const dim3 g(p->rs_nkp / 32, (p->ny + tj - 1) / tj, a.nslices);
     if (tj == 32) {
-      if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<32>))) == CGEF_OK)
-        rs_accumulate_kernel<32><<<g, 32 * npairs * 4, acc_smem, st>>>(k, NA);
+      if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<32, NA>))) == CGEF_OK)
+        rs_accumulate_kernel<32, NA><<<g, 32 * npairs * 4, acc_smem, st>>>(k);
     } else {
-      if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<16>))) == CGEF_OK)
-        rs_accumulate_kernel<16><<<g, 32 * npairs * 2, acc_smem, st>>>(k, NA);
+      if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<16, NA>))) == CGEF_OK)
+        rs_accumulate_kernel<16, NA><<<g, 32 * npairs * 2, acc_smem, st>>>(k);
     }
     if (rc == CGEF_OK) rc = rs_check("rs_accumulate_kernel");
   }
