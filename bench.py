@@ -52,6 +52,9 @@ def parse():
                     help="closure8: judged Pi rel-L2 above which a slice falls back to the exact path")
     ap.add_argument("--closure-epochs", type=float, default=3.0, help="closure8: training epochs over 10^7 points")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default banded schedules")
+    ap.add_argument("--evaluation", choices=("auto", "direct", "spectral"), default="auto",
+                    help="footprint sums of the banded engine: the autotuner's choice per scale (default), the "
+                         "direct gather, or the row-spectral evaluation")
     return ap.parse_args()
 
 
@@ -126,6 +129,41 @@ def algorithmic_flops(plans, grid, nslices, slice_masks) -> float:
         elif p.engine == "separable":
             total += grid.nx * grid.ny * nslices * 2 * (2 * p.info.di_max + 1 + 2 * p.info.dj_lim + 1) * K
     return total
+
+
+def apply_evaluation(plans, how: str) -> None:
+    """auto: the autotuner's choice per plan; direct / spectral: forced where the plan allows."""
+    for p in plans:
+        if how == "direct" and p.engine == "banded":
+            p.set_row_spectral(False)
+        elif how == "spectral" and p.engine == "banded" and p.row_spectral[0]:
+            p.set_row_spectral(True)
+
+
+def uses_row_spectral(p) -> bool:
+    return p.engine == "banded" and p.row_spectral[1]
+
+
+def rowspec_bytes(p, grid, nslices, na, nplanes, nout, masked) -> float:
+    """Compulsory DRAM bytes of one row-spectral launch: the staged planes read, the source spectra
+    written and read once, the kernel spectra read, the summed spectra written and read, the
+    unnormalised sums written and read, the outputs written (and the mask read)."""
+    L = p.row_spectral[2]
+    nk = L // 2 + 1
+    D = p.info.dj_lim
+    nrows = (grid.ny if grid.is_spherical else 1) * (2 * D + 1)
+    N = grid.nx * grid.ny
+    spec = nslices * grid.ny * na * nk * 16
+    return float(nslices * nplanes * N * 8 + 4 * spec + nrows * nk * 8 + 2 * nslices * na * N * 8
+                 + nslices * nout * N * 8 + (nslices * N if masked else 0))
+
+
+def hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), \
+            "measured: MEASURED_PEAKS.json hbm_gbs (STREAM-style copy on this pool's B200s)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
 
 
 # ---------------------------------------------------------------------------------------------
@@ -307,6 +345,7 @@ def run_closure(args, rank, world, local, dist):
     N = g.nx * g.ny
     plans = [cg.plan_filter(g, wl["kernel"], s) for s in scales]
     waves = [p.autotune(1) if not args.no_autotune else 4.0 for p in plans]
+    apply_evaluation(plans, args.evaluation)
     stream = torch.cuda.current_stream()
 
     # training pairs from two snapshots, 10^7 points sampled (seed 3)
@@ -415,7 +454,7 @@ def run_closure(args, rank, world, local, dist):
     launches = int(L.cgef_launch_count())
     prof = {}
     for name, kind in (("banded", _lib.KERNEL_BANDED), ("closure_mlp", _lib.KERNEL_CLOSURE),
-                       ("strain", _lib.KERNEL_STRAIN), ("stage", _lib.KERNEL_STAGE)):
+                       ("strain", _lib.KERNEL_STRAIN), ("stage", _lib.KERNEL_STAGE), ("rowspec", _lib.KERNEL_ROWSPEC)):
         tot, cnt = C.c_double(), C.c_int64()
         _lib.check(L.cgef_profile_read(kind, C.byref(tot), C.byref(cnt)))
         prof[name] = (tot.value, cnt.value)
@@ -438,8 +477,8 @@ def run_closure(args, rank, world, local, dist):
     except Exception:
         peak = None
     bt, bc = prof["banded"]
+    rt, rc_ = prof["rowspec"]
     mt, mc = prof["closure_mlp"]
-    ach = vel_flops * steps / (bt * 1e-3) / 1e12 if bt > 0 else None
     mlp_ach = N * ns * mlp_flops_per_point() * steps / (mt * 1e-3) / 1e12 if mt > 0 else None
     peaks = {}
     try:
@@ -447,15 +486,28 @@ def run_closure(args, rank, world, local, dist):
     except Exception:
         peaks = {}
     bf16 = peaks.get("bf16_tflops")
-    roofline = {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                "frac": (ach / peak) if (ach and peak) else None, "traffic": None,
-                "kernel": "banded_kernel in fields mode (3 planetary velocity components, FP64 FMA); judged "
-                          "tiles add a 9-field gather over 2% of the tiles",
-                "per_step_ms": bt / steps, "algorithmic_flops_per_step": vel_flops,
-                "mlp": {"bound": "tensor", "achieved": mlp_ach, "peak": bf16, "unit": "TFLOP/s",
-                        "frac": (mlp_ach / bf16) if (mlp_ach and bf16) else None,
-                        "per_step_ms": mt / steps, "flops_per_point": mlp_flops_per_point(),
-                        "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)"}}
+    mlp_line = {"bound": "tensor", "achieved": mlp_ach, "peak": bf16, "unit": "TFLOP/s",
+                "frac": (mlp_ach / bf16) if (mlp_ach and bf16) else None,
+                "per_step_ms": mt / steps, "flops_per_point": mlp_flops_per_point(),
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)"}
+    if rt > bt:
+        # the 3-field velocity filter runs through the row-spectral evaluation
+        hbm, hbm_source = hbm_peak()
+        vb = sum(rowspec_bytes(p, g, 1, 3, 3, 3, True) for p in plans if uses_row_spectral(p))
+        ach = vb * steps / (rt * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                    "traffic": None,
+                    "kernel": "row-spectral filter of the 3 planetary velocity components (rs_forward, rs_accumulate, "
+                              "rs_inverse, rs_finish); judged tiles add a direct 9-field gather over 2% of the tiles",
+                    "per_step_ms": rt / steps, "algorithmic_bytes_per_step": vb, "direct_gather_ms_per_step": bt / steps,
+                    "peak_source": hbm_source, "mlp": mlp_line}
+    else:
+        ach = vel_flops * steps / (bt * 1e-3) / 1e12 if bt > 0 else None
+        roofline = {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                    "frac": (ach / peak) if (ach and peak) else None, "traffic": None,
+                    "kernel": "banded_kernel in fields mode (3 planetary velocity components, FP64 FMA); judged "
+                              "tiles add a 9-field gather over 2% of the tiles",
+                    "per_step_ms": bt / steps, "algorithmic_flops_per_step": vel_flops, "mlp": mlp_line}
 
     # end to end: pinned host u, v in, Pi of every scale out, each step
     hu = torch.from_numpy(np.ascontiguousarray(wl["u"][0])).pin_memory()
@@ -566,6 +618,7 @@ def main():
              for s in wl["scales"]]
     # schedule autotuning is plan setup, like building the footprint: outside the timed region
     waves = [p.autotune(nsl) if not args.no_autotune else 4.0 for p in plans]
+    apply_evaluation(plans, args.evaluation)
     L = _lib.load()
     tdt = torch.float32 if wl["dtype"] == "f32" else torch.float64
     du = torch.from_numpy(np.ascontiguousarray(wl["u"])).to(device="cuda", dtype=tdt)
@@ -650,41 +703,72 @@ def main():
                   "gpu_launches": graph_launches,
                   "timing": "the step captured once as a CUDA graph and replayed; same L2 flush, same events"}
 
-    # dominant kernel timing (CUDA events on the launch stream, inside the timed region)
+    # dominant kernel timing (CUDA events on the launch stream, inside the timed region): the footprint
+    # sums of the direct gather or of the row-spectral evaluation, whichever took longer
     kinds = {"banded": _lib.KERNEL_BANDED, "separable": _lib.KERNEL_SEPARABLE, "prefixsum": _lib.KERNEL_PREFIX}
-    kind = kinds[plans[0].engine]
-    tot = C.c_double()
-    cnt = C.c_int64()
-    _lib.check(L.cgef_profile_read(kind, C.byref(tot), C.byref(cnt)))
-    per_launch_ms = tot.value / max(cnt.value, 1)
-    flops_step = algorithmic_flops(plans, g, nsl, wl["slice_masks"])
-    launches_per_step = max(cnt.value // steps, 1)
-    flops_launch = flops_step / launches_per_step
-    peak = None
-    try:
-        pk = C.CDLL(os.path.join(ROOT, "coarsegrainingenergyfluxes.jl_b200", "cgef_b200", "libcgef_peak.so"))
-        pk.cgef_peak_fp64_tflops.restype = C.c_double
-        pk.cgef_peak_fp64_tflops.argtypes = [C.c_int]
-        peak = float(pk.cgef_peak_fp64_tflops(local))
-    except Exception:
+    prof = {}
+    for name, kind in (("direct", kinds[plans[0].engine]), ("rowspec", _lib.KERNEL_ROWSPEC)):
+        tot, cnt = C.c_double(), C.c_int64()
+        _lib.check(L.cgef_profile_read(kind, C.byref(tot), C.byref(cnt)))
+        prof[name] = (tot.value, int(cnt.value))
+    spec_plans = [p for p in plans if uses_row_spectral(p)]
+    direct_plans = [p for p in plans if not uses_row_spectral(p)]
+    flops_all = algorithmic_flops(plans, g, nsl, wl["slice_masks"])
+    masked = g.mask is not None or wl["slice_masks"] is not None
+    if prof["rowspec"][0] >= prof["direct"][0] and spec_plans:
+        tot, cnt = prof["rowspec"]
+        per_launch_ms = tot / max(cnt, 1)
+        launches_per_step = max(cnt // steps, 1)
+        na, npl = (9, 3) if g.is_spherical else (5, 2)
+        bytes_launch = sum(rowspec_bytes(p, g, nsl, na, npl, 5, masked) for p in spec_plans) / launches_per_step
+        peak, peak_source = hbm_peak()
+        achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath)).get(f"{args.workload}:rowspec")
+            except Exception:
+                traffic = None
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": traffic,
+                    "kernel": "rs_forward_kernel + rs_accumulate_kernel + rs_inverse_kernel + rs_finish_kernel "
+                              "(row-spectral footprint sums: FFTs along x, banded spectral sums, inverse FFTs)",
+                    "per_launch_ms": per_launch_ms, "launches": cnt, "algorithmic_bytes_per_launch": bytes_launch,
+                    "direct_sum_equivalent_tflops": flops_all / launches_per_step / (per_launch_ms * 1e-3) / 1e12
+                    if not direct_plans else None,
+                    "direct_gather_launches": prof["direct"][1], "peak_source": peak_source}
+    else:
+        tot, cnt = prof["direct"]
+        per_launch_ms = tot / max(cnt, 1)
+        flops_step = algorithmic_flops(direct_plans, g, nsl, wl["slice_masks"])
+        launches_per_step = max(cnt // steps, 1)
+        flops_launch = flops_step / launches_per_step
         peak = None
-    achieved = flops_launch / (per_launch_ms * 1e-3) / 1e12
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(f"{args.workload}:{plans[0].engine}")
+            pk = C.CDLL(os.path.join(ROOT, "coarsegrainingenergyfluxes.jl_b200", "cgef_b200", "libcgef_peak.so"))
+            pk.cgef_peak_fp64_tflops.restype = C.c_double
+            pk.cgef_peak_fp64_tflops.argtypes = [C.c_int]
+            peak = float(pk.cgef_peak_fp64_tflops(local))
         except Exception:
-            traffic = None
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak and peak > 0 else None, "traffic": traffic,
-                "kernel": {"banded": "banded_kernel + banded_combine_kernel (FP64 FMA footprint gather)",
-                           "separable": "sep_row_kernel + sep_col_kernel (FP64 separable passes)",
-                           "prefixsum": "prefix_scan_kernel + prefix_sweep_kernel"}[plans[0].engine],
-                "per_launch_ms": per_launch_ms, "launches": int(cnt.value),
-                "algorithmic_flops_per_launch": flops_launch,
-                "peak_source": "measured: DFMA loop over all SMs on this GPU (libcgef_peak.so), "
-                               "nominal B200 FP64 37 TFLOP/s; MEASURED_PEAKS.json holds no FP64 figure"}
+            peak = None
+        achieved = flops_launch / (per_launch_ms * 1e-3) / 1e12
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath)).get(f"{args.workload}:{plans[0].engine}")
+            except Exception:
+                traffic = None
+        roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": (achieved / peak) if peak and peak > 0 else None, "traffic": traffic,
+                    "kernel": {"banded": "banded_kernel + banded_combine_kernel (FP64 FMA footprint gather)",
+                               "separable": "sep_row_kernel + sep_col_kernel (FP64 separable passes)",
+                               "prefixsum": "prefix_scan_kernel + prefix_sweep_kernel"}[plans[0].engine],
+                    "per_launch_ms": per_launch_ms, "launches": cnt,
+                    "algorithmic_flops_per_launch": flops_launch, "row_spectral_launches": prof["rowspec"][1],
+                    "peak_source": "measured: DFMA loop over all SMs on this GPU (libcgef_peak.so), "
+                                   "nominal B200 FP64 37 TFLOP/s; MEASURED_PEAKS.json holds no FP64 figure"}
 
     # end to end through the host C ABI: pinned inputs in, Pi (and E) out, every step
     e2e = None
@@ -771,7 +855,8 @@ def main():
                        "active_fraction": float(1.0 if g.mask is None else g.mask.mean()),
                        "l2": "flushed between steps (a 256 MiB write before every step, outside the step's own events)",
                        "parallelism": f"{world} rank(s), independent snapshots per rank",
-                       "schedule_split_waves": waves},
+                       "schedule_split_waves": waves,
+                       "row_spectral": [uses_row_spectral(p) for p in plans]},
             "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
             "graph": graph_line}
     print(json.dumps(line))

@@ -41,7 +41,8 @@ EXPORTED = [
     "cgef_plan_set_filter_rows", "cgef_plan_get_schedule", "cgef_plan_set_row_spectral",
     "cgef_plan_get_row_spectral",
 ]
-KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE = 0, 1, 2, 3, 4, 5
+KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE, KERNEL_ROWSPEC = (
+    0, 1, 2, 3, 4, 5, 6)
 CLOSURE_NPARAM = 8899
 
 

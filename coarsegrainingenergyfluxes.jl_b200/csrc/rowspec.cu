@@ -583,7 +583,7 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
   int rc;
   if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_forward_kernel<MODE, NF, DEF>))) != CGEF_OK) return rc;
   if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_inverse_kernel<NA>))) != CGEF_OK) return rc;
-  prof_begin(CGEF_KERNEL_BANDED, st);
+  prof_begin(CGEF_KERNEL_ROWSPEC, st);
   const dim3 rows(NC, p->ny, a.nslices);
   rs_forward_kernel<MODE, NF, DEF><<<rows, kRsThreads, smem, st>>>(k);
   rc = rs_check("rs_forward_kernel");
@@ -610,7 +610,7 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
     rs_finish_kernel<MODE, NF, DEF><<<dim3((p->nx + 127) / 128, p->ny, a.nslices), 128, 0, st>>>(a, scratch);
     rc = rs_check("rs_finish_kernel");
   }
-  prof_end(CGEF_KERNEL_BANDED, st);
+  prof_end(CGEF_KERNEL_ROWSPEC, st);
   return rc;
 }
 

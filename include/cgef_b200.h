@@ -359,7 +359,7 @@ void cgef_reset_launch_count(void);
  * below with CUDA events on the launch's own stream.  `cgef_profile_read` waits for the recorded
  * events and returns the summed duration (ms) and launch count of one kind since the last reset. */
 enum { CGEF_KERNEL_STAGE = 0, CGEF_KERNEL_BANDED = 1, CGEF_KERNEL_SEPARABLE = 2, CGEF_KERNEL_PREFIX = 3,
-       CGEF_KERNEL_STRAIN = 4, CGEF_KERNEL_CLOSURE = 5, CGEF_KERNEL_KINDS = 6 };
+       CGEF_KERNEL_STRAIN = 4, CGEF_KERNEL_CLOSURE = 5, CGEF_KERNEL_ROWSPEC = 6, CGEF_KERNEL_KINDS = 7 };
 void cgef_profile_enable(int32_t enable);
 int32_t cgef_profile_read(int32_t kind, double* total_ms, int64_t* launches);
 void cgef_profile_reset(void);
