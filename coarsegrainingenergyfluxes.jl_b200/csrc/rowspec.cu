@@ -39,7 +39,6 @@ constexpr int kRsThreads = 128;  // threads of the FFT kernels
 constexpr int kRsCols = 8;       // input columns a thread of the forward FFT loads at once
 constexpr int kRsMaxL = 4096;    // longest row: two buffers of kRsSeq half-length rows in shared memory
 constexpr int kRsSeq = 2;        // quantities (rows) transformed together by one FFT block
-constexpr int kRsMaxPairs = 5;  // quantity pairs of the widest pass (9 or 10 quantities): warps per block
 
 struct Fft {
   int L;   // real row length (even)
@@ -350,26 +349,30 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // S_j = sum_dj K_{j,dj} Q_{j+dj} per bin.  A block owns 32 bins x TJ target rows x every quantity and
-// walks the TJ + 2D source rows its band touches; per source row it stages that row's spectra (all
+// walks the in-domain source rows its band touches; per source row it stages that row's spectra (all
 // quantities) and the TJ kernel-spectrum slices that apply to it in shared memory through a
-// kAccStages-deep cp.async pipeline, and each warp (one pair of quantities x 8 target rows) adds
-// them into its registers.  Rows off a bounded y axis stage zeros (the direct sum skips them); on a
-// periodic y axis they wrap.
+// kAccStages-deep cp.async pipeline, and each warp adds them into a register tile of RW target rows x
+// every quantity, so one staged kernel value serves NA quantities and one staged source value RW rows
+// (NA x RW complex multiply-adds per NA + RW shared-memory reads).  Rows off a bounded y axis are
+// skipped (the direct sum skips them); on a periodic y axis they wrap.
 constexpr int kAccStages = 4;
 
+template <int NA>
+struct AccTile {
+  static constexpr int RW = NA > 5 ? 4 : 8;  // target rows of a warp's register tile
+};
+
 template <int TJ, int NA>
-__global__ void __launch_bounds__(32 * ((NA + 1) / 2) * (TJ / 8), TJ == 16 ? 2 : 1) rs_accumulate_kernel(RsK k) {
+__global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1) rs_accumulate_kernel(RsK k) {
   extern __shared__ __align__(16) unsigned char rs_acc_smem[];
-  constexpr int na = NA;
-  constexpr int npairs = (NA + 1) / 2;
-  constexpr int kThreads = 32 * npairs * (TJ / 8);
-  constexpr int kKChunks = (TJ * 16 + kThreads - 1) / kThreads;  // 16-byte kernel-spectrum chunks per thread and step
-  static_assert(kThreads >= NA * 32, "one chunk of the source spectra per thread");
-  const int qbytes = na * 32 * 16;
-  const int sbytes = qbytes + TJ * 32 * 8;
+  constexpr int RW = AccTile<NA>::RW;
+  constexpr int kThreads = 32 * (TJ / RW);
+  constexpr int kQChunks = (NA * 32 + kThreads - 1) / kThreads;  // 16-byte source-spectrum chunks per thread
+  constexpr int kKChunks = (TJ * 16 + kThreads - 1) / kThreads;  // 16-byte kernel-spectrum chunks per thread
+  constexpr int qbytes = NA * 32 * 16;
+  constexpr int sbytes = qbytes + TJ * 32 * 8;
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int pr = warp % npairs, rg = warp / npairs;
+  const int rg = threadIdx.x >> 5;  // the warp's rows: rg * RW .. rg * RW + RW - 1
   const int q0 = blockIdx.x * 32;
   const int j0 = blockIdx.y * TJ;
   const int s = blockIdx.z;
@@ -381,31 +384,37 @@ __global__ void __launch_bounds__(32 * ((NA + 1) / 2) * (TJ / 8), TJ == 16 ? 2 :
     st0 = max(0, k.D - j0);
     st1 = min(st1, k.ny - j0 + k.D);
   }
-  // this thread's copies: one chunk of the source row's spectra (the block has at least na*32
-  // threads) and up to kKChunks slices of kernel spectra, their offsets fixed but for the row
-  const bool q_copy = static_cast<int>(threadIdx.x) < na * 32;
-  const double2* q_src = k.Q + static_cast<int64_t>(s) * k.ny * na * nkp + q0 +
-                         (q_copy ? static_cast<int64_t>(threadIdx.x >> 5) * nkp + (threadIdx.x & 31) : 0);
+  // this thread's copies, their offsets fixed but for the source row
+  const double2* q_base = k.Q + static_cast<int64_t>(s) * k.ny * NA * nkp + q0;
+  int64_t q_off[kQChunks];
+#pragma unroll
+  for (int i = 0; i < kQChunks; ++i) {
+    const int c = threadIdx.x + i * kThreads;
+    q_off[i] = c < NA * 32 ? static_cast<int64_t>(c >> 5) * nkp + (c & 31) : 0;
+  }
   int k_j[kKChunks];
   int64_t k_base[kKChunks];
 #pragma unroll
   for (int i = 0; i < kKChunks; ++i) {
     const int c = threadIdx.x + i * kThreads;
-    const int t = c >> 4;
-    k_j[i] = c < TJ * 16 ? j0 + t : k.ny;  // k.ny: no copy
-    k_base[i] = static_cast<int64_t>(k.band_stride ? k_j[i] : 0) * W + k.D - k_j[i];  // + jr = the band row
-    k_base[i] = k_base[i] * nkp + q0 + 2 * (c & 15);
+    k_j[i] = c < TJ * 16 ? j0 + (c >> 4) : k.ny;  // k.ny: no copy
+    k_base[i] = (static_cast<int64_t>(k.band_stride ? k_j[i] : 0) * W + k.D - k_j[i]) * nkp + q0 + 2 * (c & 15);
   }
 
   auto issue = [&](int step, int buf) {
     unsigned char* b = rs_acc_smem + buf * sbytes;
-    int jr = j0 - k.D + step;
+    const int jraw = j0 - k.D + step;
+    int jr = jraw;
     if (jr < 0 || jr >= k.ny) {  // only reached on a periodic y axis
       jr %= k.ny;
       if (jr < 0) jr += k.ny;
     }
-    const int jraw = j0 - k.D + step;
-    if (q_copy) cp_async16(b + threadIdx.x * 16, q_src + static_cast<int64_t>(jr) * na * nkp, true);
+    const double2* qrow = q_base + static_cast<int64_t>(jr) * NA * nkp;
+#pragma unroll
+    for (int i = 0; i < kQChunks; ++i) {
+      const int c = threadIdx.x + i * kThreads;
+      if (c < NA * 32) cp_async16(b + c * 16, qrow + q_off[i], true);
+    }
 #pragma unroll
     for (int i = 0; i < kKChunks; ++i) {
       const int c = threadIdx.x + i * kThreads;
@@ -417,15 +426,16 @@ __global__ void __launch_bounds__(32 * ((NA + 1) / 2) * (TJ / 8), TJ == 16 ? 2 :
     }
   };
 
-  double2 acc[8][2];
+  double2 acc[RW][NA];
 #pragma unroll
-  for (int t = 0; t < 8; ++t) acc[t][0] = acc[t][1] = make_double2(0.0, 0.0);
+  for (int t = 0; t < RW; ++t)
+#pragma unroll
+    for (int m = 0; m < NA; ++m) acc[t][m] = make_double2(0.0, 0.0);
 #pragma unroll
   for (int i = 0; i < kAccStages - 1; ++i) {
     if (st0 + i < st1) issue(st0 + i, i);
     cp_async_commit();
   }
-  const bool two = 2 * pr + 1 < na;
   for (int st = st0; st < st1; ++st) {
     cp_async_wait<kAccStages - 2>();
     __syncthreads();
@@ -433,28 +443,30 @@ __global__ void __launch_bounds__(32 * ((NA + 1) / 2) * (TJ / 8), TJ == 16 ? 2 :
     if (nxt < st1) issue(nxt, (nxt - st0) % kAccStages);
     cp_async_commit();
     const unsigned char* b = rs_acc_smem + ((st - st0) % kAccStages) * sbytes;
-    const double2* qb = reinterpret_cast<const double2*>(b);
-    const double* kb = reinterpret_cast<const double*>(b + qbytes) + rg * 8 * 32 + lane;
-    const double2 a0 = qb[2 * pr * 32 + lane];
-    const double2 a1 = two ? qb[(2 * pr + 1) * 32 + lane] : make_double2(0.0, 0.0);
+    const double2* qb = reinterpret_cast<const double2*>(b) + lane;
+    const double* kb = reinterpret_cast<const double*>(b + qbytes) + rg * RW * 32 + lane;
+    double kv[RW];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const double kv = kb[t * 32];
-      acc[t][0].x = fma(kv, a0.x, acc[t][0].x);
-      acc[t][0].y = fma(kv, a0.y, acc[t][0].y);
-      acc[t][1].x = fma(kv, a1.x, acc[t][1].x);
-      acc[t][1].y = fma(kv, a1.y, acc[t][1].y);
+    for (int t = 0; t < RW; ++t) kv[t] = kb[t * 32];
+#pragma unroll
+    for (int m = 0; m < NA; ++m) {
+      const double2 a = qb[m * 32];
+#pragma unroll
+      for (int t = 0; t < RW; ++t) {
+        acc[t][m].x = fma(kv[t], a.x, acc[t][m].x);
+        acc[t][m].y = fma(kv[t], a.y, acc[t][m].y);
+      }
     }
   }
   cp_async_wait<0>();
-  double2* Ss = k.S + static_cast<int64_t>(s) * k.ny * na * nkp + static_cast<int64_t>(2 * pr) * nkp + q0 + lane;
+  double2* Ss = k.S + static_cast<int64_t>(s) * k.ny * NA * nkp + q0 + lane;
 #pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int j = j0 + rg * 8 + t;
+  for (int t = 0; t < RW; ++t) {
+    const int j = j0 + rg * RW + t;
     if (j >= k.ny) break;
-    double2* sr = Ss + static_cast<int64_t>(j) * na * nkp;
-    sr[0] = acc[t][0];
-    if (two) sr[nkp] = acc[t][1];
+    double2* sr = Ss + static_cast<int64_t>(j) * NA * nkp;
+#pragma unroll
+    for (int m = 0; m < NA; ++m) sr[m * nkp] = acc[t][m];
   }
 }
 
@@ -588,17 +600,16 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
   rs_forward_kernel<MODE, NF, DEF><<<rows, kRsThreads, smem, st>>>(k);
   rc = rs_check("rs_forward_kernel");
   if (rc == CGEF_OK) {
-    constexpr int npairs = (NA + 1) / 2;
-    static_assert(npairs <= kRsMaxPairs, "quantity pairs per block");
+    constexpr int RW = AccTile<NA>::RW;
     const int tj = p->D >= 48 ? 32 : 16;
     const int acc_smem = kAccStages * (NA * 32 * 16 + tj * 32 * 8);
     const dim3 g(p->rs_nkp / 32, (p->ny + tj - 1) / tj, a.nslices);
     if (tj == 32) {
       if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<32, NA>))) == CGEF_OK)
-        rs_accumulate_kernel<32, NA><<<g, 32 * npairs * 4, acc_smem, st>>>(k);
+        rs_accumulate_kernel<32, NA><<<g, 32 * (32 / RW), acc_smem, st>>>(k);
     } else {
       if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<16, NA>))) == CGEF_OK)
-        rs_accumulate_kernel<16, NA><<<g, 32 * npairs * 2, acc_smem, st>>>(k);
+        rs_accumulate_kernel<16, NA><<<g, 32 * (16 / RW), acc_smem, st>>>(k);
     }
     if (rc == CGEF_OK) rc = rs_check("rs_accumulate_kernel");
   }
