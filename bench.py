@@ -720,7 +720,15 @@ def main():
         per_launch_ms = tot / max(cnt, 1)
         launches_per_step = max(cnt // steps, 1)
         na, npl = (9, 3) if g.is_spherical else (5, 2)
-        bytes_launch = sum(rowspec_bytes(p, g, nsl, na, npl, 5, masked) for p in spec_plans) / launches_per_step
+        bytes_step = sum(rowspec_bytes(p, g, nsl, na, npl, 5, masked) for p in spec_plans)
+        # a sweep transforms the source rows once for all row-spectral scales of one FFT length: the
+        # other scales read those spectra but neither read the staged planes nor write spectra
+        L0 = spec_plans[0].row_spectral[2]
+        nshare = sum(1 for p in spec_plans if p.row_spectral[2] == L0)
+        if nshare > 1:
+            nk = L0 // 2 + 1
+            bytes_step -= (nshare - 1) * (nsl * npl * g.nx * g.ny * 8 + nsl * g.ny * na * nk * 16)
+        bytes_launch = bytes_step / launches_per_step
         peak, peak_source = hbm_peak()
         achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
         traffic = None

@@ -126,7 +126,7 @@ int mode_for(const cgef_plan* p) { return p->geometry == CGEF_SPHERICAL ? kModeP
 // Stages the inputs and runs one plan's engine for a flux computation; leaves the 5 FP64
 // gather planes (ubar, vbar, txx, txy, tyy) at `gather` with slice stride 5*N.
 int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, int nbatch, const uint8_t* mask,
-              int64_t mstride, double* gather, cudaStream_t st) {
+              int64_t mstride, double* gather, cudaStream_t st, const RsShare& share) {
   const int64_t N = static_cast<int64_t>(p->nx) * p->ny;
   GatherOut go{};
   for (int m = 0; m < 5; ++m) go.o[m] = gather + m * N;
@@ -141,6 +141,9 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
       int rc = ensure_ws(p, kSlotSplit, pb, &part);
       if (rc) return rc;
     }
+    if (p->rs_on && (share.keep || share.in))
+      return launch_rowspec(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st,
+                            share);
     return launch_banded(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st);
   }
   if (p->engine == CGEF_ENGINE_SEPARABLE) {
@@ -334,13 +337,41 @@ int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u,
   void* part = nullptr;
   const int64_t nblk = static_cast<int64_t>((p0->nx + 31) / 32) * ((p0->ny + 7) / 8);
   if ((rc = ensure_ws(p0, kSlotPartials, sizeof(double) * 2 * nblk * nbatch, &part))) return rc;
+  // The row-spectral plans of one FFT length share the source spectra: they depend on the staged fields,
+  // not on the scale, so the first such plan transforms them and the others start from its spectra.
+  int share_L = 0, nshare = 0;
+  for (int s = 0; s < nscales; ++s) {
+    const cgef_plan* q = plans[s];
+    if (q->engine != CGEF_ENGINE_BANDED || !q->rs_on) continue;
+    if (share_L == 0) share_L = q->rs_L;
+    if (q->rs_L == share_L) ++nshare;
+  }
+  double* spectra = nullptr;
+  if (nshare > 1) {
+    const int na = (mode_for(p0) == kModePiSphere ? 9 : 5) + (p0->strategy == CGEF_DEFORMABLE ? 1 : 0);
+    const cgef_plan* qs = nullptr;
+    for (int s = 0; s < nscales && !qs; ++s)
+      if (plans[s]->engine == CGEF_ENGINE_BANDED && plans[s]->rs_on) qs = plans[s];
+    void* buf = nullptr;
+    if ((rc = ensure_ws(p0, kSlotSpectra, rowspec_spectra_bytes(qs, na, nbatch), &buf))) return rc;
+    spectra = static_cast<double*>(buf);
+  }
+  bool transformed = false;
   for (int s = 0; s < nscales; ++s) {
     cgef_plan* q = plans[s];
     // the sweep's planes carry the widest halo; run each plan against them
     const int saveH = q->H;
     q->H = halo;
-    // each plan runs its engine with its own scratch (split partials, separable rows, prefix sums)
-    rc = pi_gather(q, planes, pitch, halo, np, nbatch, mask, mstride, g, st);
+    RsShare share;
+    if (spectra && q->engine == CGEF_ENGINE_BANDED && q->rs_on && q->rs_L == share_L) {
+      if (transformed)
+        share.in = spectra;
+      else
+        share.keep = spectra;
+      transformed = true;
+    }
+    // each plan runs its engine with its own scratch (split partials, separable rows, prefix sums, spectra)
+    rc = pi_gather(q, planes, pitch, halo, np, nbatch, mask, mstride, g, st, share);
     q->H = saveH;
     if (rc) return rc;
     StrainArgs sa{};

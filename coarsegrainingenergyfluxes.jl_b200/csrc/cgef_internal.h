@@ -257,9 +257,22 @@ int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, in
 // The row-spectral evaluation of a full-grid banded launch: x-direction FFTs of the accumulated
 // quantities of every source row, the band's kernel spectra applied and summed per target row,
 // inverse FFTs, and the same epilogue as the direct gather.  `scratch` holds rowspec_bytes().
+// Source spectra shared by the plans of one sweep (they depend on the staged fields and the FFT
+// length, not on the scale): `keep` = transform into this buffer and leave it there, `in` = use the
+// spectra an earlier plan left there (no forward transform).  Either way the launch's own scratch holds
+// only the summed spectra and the unnormalised sums.
+struct RsShare {
+  double* keep = nullptr;
+  const double* in = nullptr;
+};
 int launch_rowspec(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                    const uint8_t* mask, int64_t mask_slice_stride, double* scratch, const GatherOut& out,
-                   cudaStream_t st);
+                   cudaStream_t st, const RsShare& share = RsShare{});
+
+// Bytes of one sweep's shared source spectra: `na` quantities over `nbatch` slices.
+inline size_t rowspec_spectra_bytes(const cgef_plan* p, int na, int nbatch) {
+  return 2 * sizeof(double) * static_cast<size_t>(nbatch) * p->ny * na * p->rs_nkp;
+}
 
 // Decides whether the plan's banded sums can be evaluated through ring spectra and, if so, builds
 // the twiddles and the kernel spectra on the device (called once the band tables are uploaded).
@@ -366,6 +379,7 @@ enum WsSlot {
   kSlotSplit = 8,
   kSlotVel = 9,
   kSlotDecomp = 10,
+  kSlotSpectra = 11,  // a sweep's shared source spectra (row-spectral evaluation)
   kNumSlots = 12,
 };
 
@@ -393,7 +407,7 @@ int stage_pi(cgef_plan* p, int dtype, const void* u, const void* v, int nbatch, 
              int halo, double** planes_out, int* pitch_out, int* np_out, cudaStream_t st);
 // Runs the plan's engine in a flux mode: 5 FP64 planes (ubar, vbar, txx, txy, tyy) per slice.
 int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, int nbatch, const uint8_t* mask,
-              int64_t mstride, double* gather, cudaStream_t st);
+              int64_t mstride, double* gather, cudaStream_t st, const RsShare& share = RsShare{});
 int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int64_t nbatch64,
                       const uint8_t* slice_masks, const cgef_pi_outputs* out, cudaStream_t st);
 // The sweep over plans (one grid) for nbatch slices on stream st: Pi [nbatch][nscales][N] (dtype) and

@@ -559,7 +559,7 @@ int rs_smem_attr(const void* kernel) {
 }
 
 template <int MODE, int NF, bool DEF>
-int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStream_t st) {
+int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsShare& share, cudaStream_t st) {
   using C = Cfg<MODE, NF, DEF>;
   constexpr int NA = C::NA;
   constexpr int NC = (NA + kRsSeq - 1) / kRsSeq;
@@ -588,17 +588,23 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
   k.nslices = a.nslices;
   k.kspec = p->d_rs_k;
   const size_t spec = static_cast<size_t>(a.nslices) * p->ny * NA * p->rs_nkp;
-  k.Q = reinterpret_cast<double2*>(scratch);
-  k.S = k.Q + spec;
-  k.F = scratch;  // Q is dead once S is formed
+  // own scratch: [Q | S] with F over Q once S is formed; with shared source spectra: [F | S] and Q
+  // outside, transformed here (keep) or by an earlier plan of the sweep (in)
+  const bool shared = share.in != nullptr || share.keep != nullptr;
+  k.Q = shared ? reinterpret_cast<double2*>(share.in ? const_cast<double*>(share.in) : share.keep)
+               : reinterpret_cast<double2*>(scratch);
+  k.S = reinterpret_cast<double2*>(scratch) + spec;
+  k.F = scratch;
   const int smem = 2 * kRsSeq * static_cast<int>(sizeof(double2)) * (p->rs_L / 2);
   int rc;
   if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_forward_kernel<MODE, NF, DEF>))) != CGEF_OK) return rc;
   if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_inverse_kernel<NA>))) != CGEF_OK) return rc;
   prof_begin(CGEF_KERNEL_ROWSPEC, st);
   const dim3 rows(NC, p->ny, a.nslices);
-  rs_forward_kernel<MODE, NF, DEF><<<rows, kRsThreads, smem, st>>>(k);
-  rc = rs_check("rs_forward_kernel");
+  if (share.in == nullptr) {
+    rs_forward_kernel<MODE, NF, DEF><<<rows, kRsThreads, smem, st>>>(k);
+    rc = rs_check("rs_forward_kernel");
+  }
   if (rc == CGEF_OK) {
     constexpr int RW = AccTile<NA>::RW;
     const int tj = p->D >= 48 ? 32 : 16;
@@ -626,8 +632,10 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, cudaStrea
 }
 
 template <int MODE, int NF>
-int dispatch_rowspec(bool def, const cgef_plan* p, const BandedK& a, double* scratch, cudaStream_t st) {
-  return def ? run_rowspec<MODE, NF, true>(p, a, scratch, st) : run_rowspec<MODE, NF, false>(p, a, scratch, st);
+int dispatch_rowspec(bool def, const cgef_plan* p, const BandedK& a, double* scratch, const RsShare& share,
+                     cudaStream_t st) {
+  return def ? run_rowspec<MODE, NF, true>(p, a, scratch, share, st)
+             : run_rowspec<MODE, NF, false>(p, a, scratch, share, st);
 }
 
 // Radices of a Stockham plan for M with few passes (tens, nines, then sixteens, eights, fours), or
@@ -664,18 +672,18 @@ int smooth_length(int n) {
 
 int launch_rowspec(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                    const uint8_t* mask, int64_t mask_slice_stride, double* scratch, const GatherOut& out,
-                   cudaStream_t st) {
+                   cudaStream_t st, const RsShare& share) {
   if (!p->rs_on || p->d_rs_k == nullptr) return fail(CGEF_EINVAL, "row-spectral evaluation not built for this plan");
   if (scratch == nullptr) return fail(CGEF_EINVAL, "row-spectral evaluation needs its scratch buffer");
   const bool def = p->strategy == CGEF_DEFORMABLE;
   const BandedK a = make_banded_args(p, mode, planes, pitch, np, nbatch, mask, mask_slice_stride, out);
-  if (mode == kModePiSphere) return dispatch_rowspec<kModePiSphere, 1>(def, p, a, scratch, st);
-  if (mode == kModePiCart) return dispatch_rowspec<kModePiCart, 1>(def, p, a, scratch, st);
+  if (mode == kModePiSphere) return dispatch_rowspec<kModePiSphere, 1>(def, p, a, scratch, share, st);
+  if (mode == kModePiCart) return dispatch_rowspec<kModePiCart, 1>(def, p, a, scratch, share, st);
   switch (nf) {
-    case 1: return dispatch_rowspec<kModeFields, 1>(def, p, a, scratch, st);
-    case 2: return dispatch_rowspec<kModeFields, 2>(def, p, a, scratch, st);
-    case 3: return dispatch_rowspec<kModeFields, 3>(def, p, a, scratch, st);
-    case 4: return dispatch_rowspec<kModeFields, 4>(def, p, a, scratch, st);
+    case 1: return dispatch_rowspec<kModeFields, 1>(def, p, a, scratch, share, st);
+    case 2: return dispatch_rowspec<kModeFields, 2>(def, p, a, scratch, share, st);
+    case 3: return dispatch_rowspec<kModeFields, 3>(def, p, a, scratch, share, st);
+    case 4: return dispatch_rowspec<kModeFields, 4>(def, p, a, scratch, share, st);
     default: return fail(CGEF_EINVAL, "row-spectral: 1..4 fields per pass");
   }
 }

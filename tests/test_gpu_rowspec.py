@@ -165,3 +165,26 @@ def test_autotune_keeps_the_faster_evaluation_and_the_results():
     r = cg.compute_Pi_fields(u, v, g, k, 1e6, filter_plan=p)
     ref = oracle_plan(g, k, 1e6).compute_pi(u, v, NTH)
     assert rel_l2(r["Pi"], ref["Pi"]) < PI_FP64
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_sweep_sharing_source_spectra_equals_per_scale_flux(mixed):
+    # a sweep transforms the source rows once and every row-spectral scale of that FFT length starts
+    # from those spectra; each scale's flux must equal the same plan's own compute_Pi bit for bit,
+    # also when a direct-gather scale sits between the spectral ones
+    g = _sphere(seed=6)
+    us, vs = zip(*[S.sphere_fields(g, seed=30 + t, lmax=89) for t in range(2)])
+    U, V = np.stack(us), np.stack(vs)
+    k = cg.GaussianKernel(4.0)
+    scales = [3e5, 6e5, 1.2e6, 2.4e6]
+    plans = [cg.plan_filter(g, k, s) for s in scales]
+    for p in plans:
+        assert p.row_spectral[1]
+    if mixed:
+        plans[1].set_row_spectral(False)
+    res = cg.coarse_grain_batch(U, V, g, scales=scales, kernel=k, filter_plans=plans)
+    for si, (s, p) in enumerate(zip(scales, plans)):
+        one = cg.compute_Pi(None, U, V, None, g, k, s, filter_plan=p)
+        assert np.array_equal(res.Pi[:, si], one), s
+        ref = oracle_plan(g, k, s).compute_pi(us[0], vs[0], NTH)
+        assert rel_l2(res.Pi[0, si], ref["Pi"]) < PI_FP64
