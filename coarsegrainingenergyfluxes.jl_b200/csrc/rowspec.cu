@@ -35,10 +35,21 @@ namespace cgef {
 
 namespace {
 
-constexpr int kRsThreads = 128;  // threads of the FFT kernels
-constexpr int kRsCols = 8;       // input columns a thread of the forward FFT loads at once
-constexpr int kRsMaxL = 4096;    // longest row: two buffers of kRsSeq half-length rows in shared memory
-constexpr int kRsSeq = 2;        // quantities (rows) transformed together by one FFT block
+#ifndef CGEF_RS_THREADS
+#define CGEF_RS_THREADS 128
+#endif
+#ifndef CGEF_RS_SEQ
+#define CGEF_RS_SEQ 2
+#endif
+#ifndef CGEF_RS_MINB
+#define CGEF_RS_MINB 1
+#endif
+constexpr int kRsThreads = CGEF_RS_THREADS;  // threads of the FFT kernels
+constexpr int kRsMinBlocks = CGEF_RS_MINB;   // resident FFT blocks per SM the kernels are compiled for
+constexpr int kRsCols = 8;                   // input columns a thread of the forward FFT loads at once
+constexpr int kRsSeq = CGEF_RS_SEQ;          // quantities (rows) transformed together by one FFT block
+// longest row: two buffers of kRsSeq half-length rows (16 bytes a point) within 227 KB of shared memory
+constexpr int kRsMaxL = 4096 < (227 * 1024) / (16 * kRsSeq) ? 4096 : (227 * 1024) / (16 * kRsSeq);
 
 struct Fft {
   int L;   // real row length (even)
@@ -293,7 +304,7 @@ __device__ __forceinline__ double quantity(const double (&v)[Cfg<MODE, NF, DEF>:
 // spectrum is X_k = E_k + exp(-2 pi i k / L) O_k, E_k = (Z_k + conj Z_{M-k}) / 2,
 // O_k = (Z_k - conj Z_{M-k}) / 2i, for k = 0 .. M (Z_M = Z_0).
 template <int MODE, int NF, bool DEF>
-__global__ void __launch_bounds__(kRsThreads) rs_forward_kernel(RsK k) {
+__global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(RsK k) {
   using C = Cfg<MODE, NF, DEF>;
   extern __shared__ double2 rs_smem[];
   const int M = k.f.M;
@@ -356,6 +367,9 @@ __device__ __forceinline__ void cp_async_wait() {
 // (NA x RW complex multiply-adds per NA + RW shared-memory reads).  Rows off a bounded y axis are
 // skipped (the direct sum skips them); on a periodic y axis they wrap.
 constexpr int kAccStages = 4;
+// target rows of an accumulation block: 16 at every band height (32-row blocks, one per SM, were 15%
+// slower at 2000 km: every row's barrier then stalls the whole SM)
+constexpr int kAccRows = 16;
 
 template <int NA>
 struct AccTile {
@@ -475,7 +489,7 @@ __global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1) rs_accumulate_
 // the conjugate of the forward FFT of the conjugate) holds the row's even samples in its real parts
 // and its odd samples in its imaginary parts (the kernel spectra carry the 1/L).
 template <int NA>
-__global__ void __launch_bounds__(kRsThreads) rs_inverse_kernel(RsK k) {
+__global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(RsK k) {
   extern __shared__ double2 rs_smem[];
   const int M = k.f.M;
   double2* a = rs_smem;
@@ -607,16 +621,10 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
   }
   if (rc == CGEF_OK) {
     constexpr int RW = AccTile<NA>::RW;
-    const int tj = p->D >= 48 ? 32 : 16;
-    const int acc_smem = kAccStages * (NA * 32 * 16 + tj * 32 * 8);
-    const dim3 g(p->rs_nkp / 32, (p->ny + tj - 1) / tj, a.nslices);
-    if (tj == 32) {
-      if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<32, NA>))) == CGEF_OK)
-        rs_accumulate_kernel<32, NA><<<g, 32 * (32 / RW), acc_smem, st>>>(k);
-    } else {
-      if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<16, NA>))) == CGEF_OK)
-        rs_accumulate_kernel<16, NA><<<g, 32 * (16 / RW), acc_smem, st>>>(k);
-    }
+    const int acc_smem = kAccStages * (NA * 32 * 16 + kAccRows * 32 * 8);
+    const dim3 g(p->rs_nkp / 32, (p->ny + kAccRows - 1) / kAccRows, a.nslices);
+    if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<kAccRows, NA>))) == CGEF_OK)
+      rs_accumulate_kernel<kAccRows, NA><<<g, 32 * (kAccRows / RW), acc_smem, st>>>(k);
     if (rc == CGEF_OK) rc = rs_check("rs_accumulate_kernel");
   }
   if (rc == CGEF_OK) {
