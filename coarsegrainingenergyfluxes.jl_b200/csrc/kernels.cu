@@ -616,6 +616,41 @@ __device__ __forceinline__ int nb_index(int p, int off, int n, int periodic) {
 
 __device__ __forceinline__ bool act_at(const Line& L, int q) { return q >= 0 && (L.m == nullptr || L.m[q * L.stride] != 0); }
 
+// The ReduceInRun stencil of stencil() split in two: the neighbours' activity picks the case once per
+// axis (the same for every field on that axis), then apply_stencil() evaluates it for one field with
+// the same expressions, so results are identical.
+struct StencilCase {
+  int kind;  // 0: none, 1: centred, 2: forward 3-node, 3: forward 2-node, 4: backward 3-node, 5: backward 2-node
+  int m1, p1, x2;
+};
+
+__device__ __forceinline__ StencilCase stencil_case(const Line& L, int p) {
+  StencilCase c{0, nb_index(p, -1, L.n, L.periodic), nb_index(p, 1, L.n, L.periodic), -1};
+  const bool am1 = act_at(L, c.m1), ap1 = act_at(L, c.p1);
+  if (am1 && ap1) {
+    c.kind = 1;
+  } else if (ap1) {
+    c.x2 = nb_index(p, 2, L.n, L.periodic);
+    c.kind = (act_at(L, c.x2) && c.x2 != p) ? 2 : 3;
+  } else if (am1) {
+    c.x2 = nb_index(p, -2, L.n, L.periodic);
+    c.kind = (act_at(L, c.x2) && c.x2 != p) ? 4 : 5;
+  }
+  return c;
+}
+
+__device__ __forceinline__ double apply_stencil(const StencilCase& c, const double* f, int64_t stride, int p,
+                                                double h) {
+  switch (c.kind) {
+    case 1: return (f[c.p1 * stride] - f[c.m1 * stride]) / (2.0 * h);
+    case 2: return (-3.0 * f[p * stride] + 4.0 * f[c.p1 * stride] - f[c.x2 * stride]) / (2.0 * h);
+    case 3: return (f[c.p1 * stride] - f[p * stride]) / h;
+    case 4: return (3.0 * f[p * stride] - 4.0 * f[c.m1 * stride] + f[c.x2 * stride]) / (2.0 * h);
+    case 5: return (f[p * stride] - f[c.m1 * stride]) / h;
+    default: return 0.0;
+  }
+}
+
 __device__ double stencil(const Line& L, int p) {
   const int m1 = nb_index(p, -1, L.n, L.periodic), p1 = nb_index(p, 1, L.n, L.periodic);
   const bool am1 = act_at(L, m1), ap1 = act_at(L, p1);
@@ -716,16 +751,16 @@ __global__ void strain_kernel(StrainK a) {
     const double txy = a.txy ? a.txy[s * a.in_stride + pix] : 0.0;
     const double tyy = a.tyy ? a.tyy[s * a.in_stride + pix] : 0.0;
     if (act) {
-      Line Lx{ub + static_cast<int64_t>(j) * a.nx, mk ? mk + static_cast<int64_t>(j) * a.nx : nullptr, 1, a.nx,
-              a.periodic_x, a.dx};
-      Line Ly{ub + i, mk ? mk + i : nullptr, a.nx, a.ny, a.periodic_y, a.dy};
+      const Line Lx{ub + static_cast<int64_t>(j) * a.nx, mk ? mk + static_cast<int64_t>(j) * a.nx : nullptr, 1,
+                    a.nx, a.periodic_x, a.dx};
+      const Line Ly{ub + i, mk ? mk + i : nullptr, a.nx, a.ny, a.periodic_y, a.dy};
+      const StencilCase cx = stencil_case(Lx, i), cy = stencil_case(Ly, j);
+      const double* vrow = vb + static_cast<int64_t>(j) * a.nx;
       const double xs = a.xscale[j];
-      const double dudx = a.nx < 2 ? 0.0 : stencil(Lx, i) * xs;
-      const double dudy = a.ny < 2 ? 0.0 : stencil(Ly, j) * a.yscale;
-      Lx.f = vb + static_cast<int64_t>(j) * a.nx;
-      Ly.f = vb + i;
-      const double dvdx = a.nx < 2 ? 0.0 : stencil(Lx, i) * xs;
-      const double dvdy = a.ny < 2 ? 0.0 : stencil(Ly, j) * a.yscale;
+      const double dudx = a.nx < 2 ? 0.0 : apply_stencil(cx, Lx.f, 1, i, a.dx) * xs;
+      const double dudy = a.ny < 2 ? 0.0 : apply_stencil(cy, Ly.f, a.nx, j, a.dy) * a.yscale;
+      const double dvdx = a.nx < 2 ? 0.0 : apply_stencil(cx, vrow, 1, i, a.dx) * xs;
+      const double dvdy = a.ny < 2 ? 0.0 : apply_stencil(cy, vb + i, a.nx, j, a.dy) * a.yscale;
       sxx = dudx;
       syy = dvdy;
       if (a.sphere) {
