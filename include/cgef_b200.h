@@ -17,7 +17,9 @@
  *  - All calls return CGEF_OK (0) or a negative status; `cgef_last_error()` gives the message of
  *    the calling thread's last failure.
  *  - A plan is used by one host thread at a time (the reference's "one plan per task",
- *    Derivatives.jl:74-77); different plans may run concurrently.
+ *    Derivatives.jl:74-77); different plans may run concurrently.  A plan's device work is ordered
+ *    on one stream at a time: its scratch and the work queue of its direct gather are the plan's
+ *    own, so `*_device` calls of one plan on two streams must not overlap on the GPU.
  *  - Arithmetic is FP64 on the device: footprint sums accumulate with double-precision FMA and
  *    the subtraction tau = (uu)bar - ubar ubar, the normalisation and the energy reductions are
  *    FP64.  `dtype` selects only the storage type of inputs and outputs.
