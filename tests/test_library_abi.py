@@ -110,3 +110,19 @@ def test_plan_info_active_area():
     ref = O.Plan(oracle_grid(g), O.GAUSSIAN, 4.0, 5e5).active_area()
     assert p.info.active_area == pytest.approx(ref, rel=1e-14)
     assert cg.active_area(g) == pytest.approx(ref, rel=1e-12)
+
+
+@pytest.mark.skipif(_lib.device_count() > 0, reason="checks the no-device path")
+def test_row_spectral_needs_a_device_and_refuses_to_be_forced():
+    # the kernel spectra are built on the device with the plan; a host-only plan keeps the direct
+    # gather's tables and reports the spectral evaluation unavailable
+    d = math.radians(2.0)
+    g = cg.StructuredGrid(cg.SphericalGeometry(), cg.axis(d / 2, d, 180), cg.axis(-math.pi / 2 + d / 2, d, 90))
+    p = cg.plan_filter(g, cg.GaussianKernel(4.0), 5e5)
+    assert p.engine == "banded"
+    assert p.row_spectral == (False, False, 0)
+    with pytest.raises(cg.ArgumentError):
+        p.set_row_spectral(True)
+    # through the C ABI a plan without a device refuses either setting with its own status
+    assert _lib.load().cgef_plan_set_row_spectral(p.handle, 1) == _lib.CGEF_ENODEVICE
+    assert _lib.load().cgef_plan_set_row_spectral(p.handle, 0) == _lib.CGEF_ENODEVICE
