@@ -669,7 +669,6 @@ def main():
     launches = int(L.cgef_launch_count())
 
     # the same step replayed from a captured CUDA graph (cgef_sweep_graph_create / cgef_graph_launch)
-    graph_line = None
     gs = torch.cuda.Stream()  # capture needs a created stream
     torch.cuda.synchronize()
     gh = C.c_void_p()
@@ -698,10 +697,13 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms = float(t.item())
     units_per_step = g.nx * g.ny * ns * nsl
-    value = world * units_per_step * steps / (elapsed_ms / 1e3)
-    graph_line = {"value": world * units_per_step * steps / (graph_ms / 1e3), "ms_per_step": graph_ms / steps,
-                  "gpu_launches": graph_launches,
-                  "timing": "the step captured once as a CUDA graph and replayed; same L2 flush, same events"}
+    # the headline is the step replayed from the CUDA graph it was captured into once (the library's
+    # API for repeated sweeps, cgef_sweep_graph_create / cgef_graph_launch); the same step launched call
+    # by call, whose per-kernel events feed the roofline, is reported beside it as "eager"
+    value = world * units_per_step * steps / (graph_ms / 1e3)
+    eager_line = {"value": world * units_per_step * steps / (elapsed_ms / 1e3), "ms_per_step": elapsed_ms / steps,
+                  "gpu_launches": launches,
+                  "timing": "the same step launched call by call (cgef_sweep_device); same L2 flush, same events"}
 
     # dominant kernel timing (CUDA events on the launch stream, inside the timed region): the footprint
     # sums of the direct gather or of the row-spectral evaluation, whichever took longer
@@ -857,7 +859,7 @@ def main():
     if rank != 0:
         return 0
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
-            "ms_per_step": elapsed_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": graph_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if wl["dtype"] == "f64" else "f64 (f32 storage)", "data": "synthetic (seeded)",
             "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": nsl,
                        "active_fraction": float(1.0 if g.mask is None else g.mask.mean()),
@@ -865,8 +867,10 @@ def main():
                        "parallelism": f"{world} rank(s), independent snapshots per rank",
                        "schedule_split_waves": waves,
                        "row_spectral": [uses_row_spectral(p) for p in plans]},
-            "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
-            "graph": graph_line}
+            "timing": "value: K steps replayed from a CUDA graph captured once, each bracketed by CUDA events on "
+                      "the replay stream, a 256 MiB L2 flush between steps outside the events, max over ranks",
+            "gpu_launches": graph_launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+            "eager": eager_line}
     print(json.dumps(line))
     return 0
 
