@@ -722,6 +722,8 @@ def main():
         per_launch_ms = tot / max(cnt, 1)
         launches_per_step = max(cnt // steps, 1)
         na, npl = (9, 3) if g.is_spherical else (5, 2)
+        if isinstance(plans[0].strategy, cg.Deformable):  # the mask is one more quantity and plane
+            na, npl = na + 1, npl + 1
         bytes_step = sum(rowspec_bytes(p, g, nsl, na, npl, 5, masked) for p in spec_plans)
         # a sweep transforms the source rows once for all row-spectral scales of one FFT length: the
         # other scales read those spectra but neither read the staged planes nor write spectra
