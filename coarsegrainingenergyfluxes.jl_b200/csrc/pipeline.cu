@@ -6,6 +6,9 @@
 // Three streams and two device buffer sets: snapshot k copies into input set k % 2 on the H2D
 // stream, is swept on the compute stream into output set k % 2, and is copied out on the D2H
 // stream.  Events keep each set from being overwritten while the step two back still reads it.
+// Each set's sweep runs call by call on its first submit (which sizes every workspace) and is then
+// captured as a CUDA graph that the later submits replay, so the host issues one launch per sweep.
+// The graphs hold the plans as they were at that first submit.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -27,6 +30,10 @@ struct cgef_pipeline {
   double* d_e[2] = {nullptr, nullptr};
   uint8_t* d_mask = nullptr;
   cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  int64_t graph_kernels[2] = {0, 0};
+  bool no_graph[2] = {false, false};  // a capture failed: this set keeps launching call by call
   int64_t submitted = 0;
 };
 
@@ -34,6 +41,8 @@ namespace {
 
 void release(cgef_pipeline* p) {
   for (int b = 0; b < 2; ++b) {
+    if (p->exec[b]) cudaGraphExecDestroy(p->exec[b]);
+    if (p->graph[b]) cudaGraphDestroy(p->graph[b]);
     if (p->d_in[b]) cudaFree(p->d_in[b]);
     if (p->d_pi[b]) cudaFree(p->d_pi[b]);
     if (p->d_e[b]) cudaFree(p->d_e[b]);
@@ -43,6 +52,36 @@ void release(cgef_pipeline* p) {
   if (p->d_mask) cudaFree(p->d_mask);
   for (cudaStream_t s : {p->h2d, p->comp, p->d2h})
     if (s) cudaStreamDestroy(s);
+}
+
+int sweep_set(cgef_pipeline* p, int b) {
+  const char* din = static_cast<const char*>(p->d_in[b]);
+  return sweep_device(p->plans.data(), p->nscales, p->dtype, din, din + p->in_bytes, p->nbatch, p->d_mask,
+                      p->want_pi ? p->d_pi[b] : nullptr, p->d_e[b], p->comp);
+}
+
+// Captures set b's sweep on the compute stream (nothing runs; the workspaces are sized already).
+void capture_set(cgef_pipeline* p, int b) {
+  prof_suspend(true);
+  const int64_t before = cgef_launch_count();
+  cudaError_t e = cudaStreamBeginCapture(p->comp, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const int rc = sweep_set(p, b);
+    e = cudaStreamEndCapture(p->comp, &p->graph[b]);
+    if (rc != CGEF_OK && e == cudaSuccess) e = cudaErrorUnknown;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec[b], p->graph[b], 0);
+  prof_suspend(false);
+  p->graph_kernels[b] = cgef_launch_count() - before;
+  count_launch(-p->graph_kernels[b]);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (p->exec[b]) cudaGraphExecDestroy(p->exec[b]);
+    if (p->graph[b]) cudaGraphDestroy(p->graph[b]);
+    p->exec[b] = nullptr;
+    p->graph[b] = nullptr;
+    p->no_graph[b] = true;
+  }
 }
 
 }  // namespace
@@ -114,9 +153,14 @@ int32_t cgef_pipeline_submit(cgef_pipeline* p, const void* u, const void* v, voi
   if ((e = cudaStreamWaitEvent(p->comp, p->in_ready[b], 0)) != cudaSuccess ||
       (e = cudaStreamWaitEvent(p->comp, p->out_free[b], 0)) != cudaSuccess)
     return cuda_fail(e, "pipeline wait");
-  int rc = sweep_device(p->plans.data(), p->nscales, p->dtype, din, din + p->in_bytes, p->nbatch, p->d_mask,
-                        p->want_pi ? p->d_pi[b] : nullptr, energy ? p->d_e[b] : nullptr, p->comp);
-  if (rc) return rc;
+  if (p->exec[b]) {
+    if ((e = cudaGraphLaunch(p->exec[b], p->comp)) != cudaSuccess) return cuda_fail(e, "pipeline graph launch");
+    count_launch(p->graph_kernels[b]);
+  } else {
+    const int rc = sweep_set(p, b);
+    if (rc) return rc;
+    if (!p->no_graph[b]) capture_set(p, b);
+  }
   if ((e = cudaEventRecord(p->in_free[b], p->comp)) != cudaSuccess ||
       (e = cudaEventRecord(p->out_ready[b], p->comp)) != cudaSuccess)
     return cuda_fail(e, "pipeline event");
