@@ -728,6 +728,14 @@ int build_row_spectra(cgef_plan* p) {
   e = cudaMemcpy(p->d_rs_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(row-spectral twiddles)");
   e = cudaMalloc(reinterpret_cast<void**>(&p->d_rs_k), kbytes);
+  if (e == cudaErrorMemoryAllocation) {
+    // no room for the kernel spectra: the plan keeps the direct gather only
+    cudaGetLastError();
+    p->d_rs_k = nullptr;
+    cudaFree(p->d_rs_tw);
+    p->d_rs_tw = nullptr;
+    return CGEF_OK;
+  }
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(row-spectral kernel spectra)");
   const int64_t zchunks = (nrows + 65534) / 65535;
   const dim3 g((nkp + 127) / 128, static_cast<unsigned>(std::min<int64_t>(nrows, 65535)), static_cast<unsigned>(zchunks));

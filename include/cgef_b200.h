@@ -154,7 +154,9 @@ int32_t cgef_plan_get_schedule(const cgef_plan* plan, double* waves, int32_t* fi
  * rounding of the transforms, and each quantity is transformed on its own, so batched applies stay
  * bit-identical to per-field ones.  Available on a periodic x axis (FFT length Nx) or with symmetric
  * rows on a bounded one (a zero-padded length >= Nx + the widest half-width), when the length is even
- * and its half has no prime factor above 5; built with the plan and enabled by default when available;
+ * and its half has no prime factor above 5, and when the device has room for the plan's kernel spectra
+ * (8 bytes per band row and bin; 1.5 GB at 2000 km on the 0.25° sphere); built with the plan and enabled
+ * by default when available;
  * cgef_plan_autotune keeps whichever evaluation times faster for the flux.  Work-item subsets (the
  * closure's judge) and cgef_filter_device_noalloc always sum directly. */
 int32_t cgef_plan_set_row_spectral(cgef_plan* plan, int32_t enable);
