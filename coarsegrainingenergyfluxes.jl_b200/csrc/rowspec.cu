@@ -361,14 +361,16 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(Rs
     }
 #pragma unroll
     for (int u = 0; u < kRsBatch; ++u) {
-      int q = t0 + u * kRsThreads + threadIdx.x, e = 0;
-      if (q >= items) break;
+      const int t = t0 + u * kRsThreads + threadIdx.x;
+      if (t < items) {  // a guarded store, not a break: the break form measured 4% slower
+        int q = t, e = 0;
 #pragma unroll
-      for (int i = 1; i < kRsSeq; ++i)
-        if (q >= nk) q -= nk, ++e;
-      const double2 E = make_double2(0.5 * (zq[u].x + zc[u].x), 0.5 * (zq[u].y + zc[u].y));
-      const double2 O = make_double2(0.5 * (zq[u].y - zc[u].y), -0.5 * (zq[u].x - zc[u].x));  // (zq - zc) / 2i
-      Q0[e * k.f.nkp + q] = cadd(E, cmul(w[u], O));
+        for (int i = 1; i < kRsSeq; ++i)
+          if (q >= nk) q -= nk, ++e;
+        const double2 E = make_double2(0.5 * (zq[u].x + zc[u].x), 0.5 * (zq[u].y + zc[u].y));
+        const double2 O = make_double2(0.5 * (zq[u].y - zc[u].y), -0.5 * (zq[u].x - zc[u].x));  // (zq - zc) / 2i
+        Q0[e * k.f.nkp + q] = cadd(E, cmul(w[u], O));
+      }
     }
   }
 }
@@ -539,10 +541,11 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(Rs
 #pragma unroll
     for (int u = 0; u < kRsBatch; ++u) {
       const int t = t0 + u * kRsThreads + threadIdx.x;
-      if (t >= items) break;
-      const double2 Ep = cadd(sq[u], sc[u]);
-      const double2 Op = cmul(csub(sq[u], sc[u]), conj2(w[u]));
-      a[t] = make_double2(Ep.x - Op.y, -(Ep.y + Op.x));  // conj(E' + i O')
+      if (t < items) {
+        const double2 Ep = cadd(sq[u], sc[u]);
+        const double2 Op = cmul(csub(sq[u], sc[u]), conj2(w[u]));
+        a[t] = make_double2(Ep.x - Op.y, -(Ep.y + Op.x));  // conj(E' + i O')
+      }
     }
   }
   __syncthreads();
