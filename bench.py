@@ -159,22 +159,24 @@ def rowspec_bytes(p, grid, nslices, na, nplanes, nout, masked) -> float:
 
 
 def committed_traffic(key: str, nsl: int, scale_km=None):
-    """DRAM bytes (read + write) per launch from the committed ncu summary, and how they were obtained.
+    """DRAM bytes (read + write) per launch from the committed ncu summary, how they were obtained, and
+    the one-snapshot figure.
 
-    The summaries hold one snapshot's traffic at the workload's own scale; a launch of `nsl` snapshots
-    moves `nsl` times the units, so the figure is scaled by `nsl` (the traffic grows in proportion to
-    the snapshots processed).  A scale other than the workload's own has no capture: None."""
+    The summaries hold one snapshot's traffic at the workload's own scale.  A launch of several
+    snapshots has no capture of its own, and its traffic is not that figure times the snapshots (the
+    kernel spectra are read once per launch, and L2 holds less of a larger launch), so it reports None
+    with the one-snapshot figure beside it.  A scale other than the workload's own has no capture."""
     if scale_km is not None:
-        return None, None
+        return None, None, None
     try:
         t = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json"))).get(key)
     except Exception:
         t = None
     if t is None:
-        return None, None
+        return None, None, None
     if nsl == 1:
-        return float(t), "ncu capture of one launch (profiles/ncu_traffic.json)"
-    return float(t) * nsl, f"one-snapshot ncu capture (profiles/ncu_traffic.json) x {nsl} snapshots per launch"
+        return float(t), "ncu capture of one launch (profiles/ncu_traffic.json)", float(t)
+    return None, f"no capture of {nsl} snapshots per launch; one-snapshot capture beside it", float(t)
 
 
 def hbm_peak():
@@ -754,9 +756,9 @@ def main():
         bytes_launch = bytes_step / launches_per_step
         peak, peak_source = hbm_peak()
         achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
-        traffic, traffic_basis = committed_traffic(f"{args.workload}:rowspec", nsl, args.scale_km)
+        traffic, traffic_basis, traffic_one = committed_traffic(f"{args.workload}:rowspec", nsl, args.scale_km)
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": traffic, "traffic_basis": traffic_basis,
+                    "traffic": traffic, "traffic_basis": traffic_basis, "traffic_one_snapshot": traffic_one,
                     "kernel": "rs_forward_kernel + rs_accumulate_kernel + rs_inverse_kernel + rs_finish_kernel "
                               "(row-spectral footprint sums: FFTs along x, banded spectral sums, inverse FFTs)",
                     "per_launch_ms": per_launch_ms, "launches": cnt, "algorithmic_bytes_per_launch": bytes_launch,
@@ -778,10 +780,11 @@ def main():
         except Exception:
             peak = None
         achieved = flops_launch / (per_launch_ms * 1e-3) / 1e12
-        traffic, traffic_basis = committed_traffic(f"{args.workload}:{plans[0].engine}", nsl, args.scale_km)
+        traffic, traffic_basis, traffic_one = committed_traffic(f"{args.workload}:{plans[0].engine}", nsl,
+                                                                args.scale_km)
         roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": (achieved / peak) if peak and peak > 0 else None, "traffic": traffic,
-                    "traffic_basis": traffic_basis,
+                    "traffic_basis": traffic_basis, "traffic_one_snapshot": traffic_one,
                     "kernel": {"banded": "banded_kernel + banded_combine_kernel (FP64 FMA footprint gather)",
                                "separable": "sep_row_kernel + sep_col_kernel (FP64 separable passes)",
                                "prefixsum": "prefix_scan_kernel + prefix_sweep_kernel"}[plans[0].engine],
