@@ -258,7 +258,8 @@ def oracle_rate(wl, budget_s: float):
 
     A unit is Pi for one (slice, scale).  With one unit it is repeated within the budget; otherwise
     a bounded subset of units is timed and the whole workload's time is extrapolated linearly in
-    (active targets x footprint entries), the direct sum's cost."""
+    (active targets x footprint entries), the direct sum's cost.  Also returns the first timed unit's
+    FP64 Pi with its (slice, scale index), against which the GPU result is compared."""
     import oracle as O
     g = wl["grid"]
     nthreads = O.max_threads()
@@ -284,6 +285,8 @@ def oracle_rate(wl, budget_s: float):
     order = sorted(range(len(scales)), key=lambda s: entries[s])
     plans = {}
 
+    first = {}
+
     def run(t, s):
         key = (t if masks is not None else -1, s)
         if key not in plans:
@@ -292,8 +295,11 @@ def oracle_rate(wl, budget_s: float):
         u = np.asarray(wl["u"][t], dtype=np.float64)
         v = np.asarray(wl["v"][t], dtype=np.float64)
         t0 = time.perf_counter()
-        p.compute_pi(u, v, nthreads)
-        return time.perf_counter() - t0
+        out = p.compute_pi(u, v, nthreads)
+        dt = time.perf_counter() - t0
+        if not first:
+            first.update(slice=t, scale=s, Pi=out["Pi"])
+        return dt
 
     run(0, order[0])  # warm-up
     timed, spent, ccost = [], 0.0, 0.0
@@ -325,7 +331,7 @@ def oracle_rate(wl, budget_s: float):
         sample = (f"{len(timed)} timed (slice, scale) units, scales "
                   f"{sorted({round(scales[s] / 1e3) for _, s in timed})} km of slice 0 ({spent:.1f} s), "
                   f"extrapolated to all {nsl}x{len(scales)} units linearly in active targets x footprint entries")
-    return rate, nthreads, len(timed), spent, sample
+    return rate, nthreads, len(timed), spent, sample, first
 
 
 def device_steps_ms(run, steps, stream, flush) -> float:
@@ -552,7 +558,7 @@ def run_closure(args, rank, world, local, dist):
            "timing": "wall clock: pinned H2D of u, v, the closure at 8 scales, D2H of Pi"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, nth, done, el, sample = oracle_rate(wl, budget_s=20.0)
+        rate, nth, done, el, sample, _ = oracle_rate(wl, budget_s=20.0)
         cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
                "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path (plain Pi, FP64 oracle)"}
     if dist is not None:
@@ -606,7 +612,7 @@ def main():
         if rank != 0:
             return 0
         wl = make_workload(args.workload, 0, args.snapshots, args.scale_km)
-        rate, nth, done, el, sample = oracle_rate(wl, budget_s=120.0)
+        rate, nth, done, el, sample, _ = oracle_rate(wl, budget_s=120.0)
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -861,10 +867,19 @@ def main():
                "synchronous": e2e_sync}
 
     cpu = None
+    accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, nth, done, el, sample = oracle_rate(wl, budget_s=20.0)
+        rate, nth, done, el, sample, ref = oracle_rate(wl, budget_s=20.0)
         cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
                "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path (FP64 oracle, OpenMP rows)"}
+        # the metric's accuracy term: the library's Pi (host C ABI, cgef_sweep) against the FP64 oracle on
+        # the oracle's first timed unit; and the streamed output against the synchronous one
+        got = hPi[ref["slice"], ref["scale"]].to(torch.float64).numpy()
+        den = float(np.linalg.norm(ref["Pi"]))
+        streamed = outs[(n_e2e - 1) % 2][0]
+        accuracy = {"rel_l2_pi_vs_fp64_oracle": float(np.linalg.norm(got - ref["Pi"])) / (den if den > 0 else 1.0),
+                    "unit": f"Pi of snapshot {ref['slice']} at l = {wl['scales'][ref['scale']] / 1e3:g} km, all cells",
+                    "streamed_equals_synchronous": bool(torch.equal(streamed, hPi))}
 
     if dist is not None:
         dist.barrier()
@@ -883,7 +898,7 @@ def main():
             "timing": "value: K steps replayed from a CUDA graph captured once, each bracketed by CUDA events on "
                       "the replay stream, a 256 MiB L2 flush between steps outside the events, max over ranks",
             "gpu_launches": graph_launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
-            "eager": eager_line}
+            "eager": eager_line, "accuracy": accuracy}
     print(json.dumps(line))
     return 0
 
