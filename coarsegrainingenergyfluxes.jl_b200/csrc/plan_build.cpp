@@ -29,13 +29,6 @@ namespace {
 
 inline double coord(double x0, double d, int i) { return std::fma(static_cast<double>(i), d, x0); }
 
-double sphere_distance(double R, double x1, double y1, double x2, double y2) {
-  double sdp = std::sin((y2 - y1) / 2.0), sdl = std::sin((x2 - x1) / 2.0);
-  double h = sdp * sdp + std::cos(y1) * std::cos(y2) * sdl * sdl;
-  if (h > 1.0) h = 1.0;
-  return 2.0 * R * std::asin(std::sqrt(h));
-}
-
 // Column half-width that certainly covers the part of row phi2 within rad of (0, phi1): the
 // spherical band formula plus a two-cell margin, capped at `cap`.  Inclusion itself is decided by
 // the distance test, so only coverage matters here.
@@ -175,17 +168,27 @@ void build_banded(const cgef_plan* p, Banded& B) {
       const double phi2 = coord(p->y0, p->dy, jj);
       const double A = p->R * p->R * std::cos(phi2) * p->dx * p->dy;
       const int win = closed ? half : sphere_row_window(p->R, p->dx, phi, phi2, rad, half);
-      const int lo = -win;
+      // the reference visits ddi in [-win, hi]; hi = half - 1 where the ring closes on an even nx
+      // (column -half is column +half)
       const int hi = (closed && 2 * half + 1 > nx) ? half - 1 : win;
-      // weights by |di|; inclusion exactly as the reference (d <= rad at each visited offset)
+      // weights by |di|; inclusion exactly as the reference (d <= rad at each visited offset).  The
+      // great-circle distance from (0, phi) to (ddi dx, phi2) in the haversine form,
+      //     d = 2 R asin(sqrt(min(1, sin^2((phi2 - phi) / 2) + cos(phi) cos(phi2) sin^2(ddi dx / 2)))),
+      // with its row-constant factors computed once; it is even in ddi bit for bit (sin is odd), so
+      // each |ddi| is evaluated once and counted for every visited sign.
+      const double sdp = std::sin((phi2 - phi) / 2.0);
+      const double cc = std::cos(phi) * std::cos(phi2);
       int amax = -1;
       std::vector<double> wabs(static_cast<size_t>(win) + 1, 0.0);
-      for (int ddi = lo; ddi <= hi; ++ddi) {
-        double d = sphere_distance(p->R, 0.0, phi, static_cast<double>(ddi) * p->dx, phi2);
+      for (int k = 0; k <= win; ++k) {
+        const double sdl = std::sin((static_cast<double>(k) * p->dx - 0.0) / 2.0);
+        double h = sdp * sdp + cc * sdl * sdl;
+        if (h > 1.0) h = 1.0;
+        const double d = 2.0 * p->R * std::asin(std::sqrt(h));
         if (d <= rad) {
-          wabs[std::abs(ddi)] = kernel_weight(p->kernel, p->alpha, d, p->scale) * A;
-          amax = std::max(amax, std::abs(ddi));
-          ++o.n;
+          wabs[k] = kernel_weight(p->kernel, p->alpha, d, p->scale) * A;
+          amax = k;
+          o.n += k == 0 ? 1 : 1 + (k <= hi ? 1 : 0);  // -k always visited, +k up to hi
         }
       }
       if (amax >= 0) {
