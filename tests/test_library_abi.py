@@ -53,6 +53,34 @@ def test_host_plan_footprint_equals_oracle_sphere(scale, alpha):
         assert np.array_equal(a, b)
 
 
+SPHERE_GRIDS = [  # nx, ny, first latitude (deg, None = pole-to-pole centres), spacing (deg), longitude span (deg)
+    (72, 36, None, None, 360), (73, 37, None, None, 360), (120, 60, None, None, 360), (45, 30, -40.0, 2.0, 90),
+    (31, 15, -40.0, 5.0, 93), (90, 45, None, None, 360), (100, 40, 10.0, 2.0, 360), (64, 90, None, None, 360)]
+KERNEL_SCALES = [(4.0, 3e5), (6.0, 8e5), (4.0, 2.5e6), (0.0, 1.2e6), (4.0, 6e6)]  # alpha 0: top-hat
+
+
+@pytest.mark.parametrize("grid", SPHERE_GRIDS, ids=[f"{c[0]}x{c[1]}" for c in SPHERE_GRIDS])
+def test_host_banded_footprints_equal_oracle_across_grids(grid):
+    """Odd and even rings, rings that close at high latitude or at large scales, regional boxes that do
+    not wrap, Gaussian and top-hat: the exported CSR equals the oracle's, which visits every offset of
+    both signs as the reference does (Filtering.jl:675-731)."""
+    nx, ny, lat0, dlat, span = grid
+    d = math.radians(span / nx)
+    if lat0 is None:
+        dl = math.pi / ny
+        y0 = -math.pi / 2 + dl / 2
+    else:
+        dl, y0 = math.radians(dlat), math.radians(lat0)
+    g = cg.StructuredGrid(cg.SphericalGeometry(), cg.axis(d / 2, d, nx), cg.axis(y0, dl, ny), periodic=(span == 360, False))
+    for alpha, scale in KERNEL_SCALES:
+        k = cg.TopHatKernel() if alpha == 0.0 else cg.GaussianKernel(alpha)
+        got = cg.plan_filter(g, k, scale, engine="banded").footprint()
+        ref = O.Plan(oracle_grid(g), O.TOPHAT if alpha == 0.0 else O.GAUSSIAN, alpha, scale, O.ZEROFILL,
+                     O.ENGINE_BANDED).footprint()
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b), (alpha, scale)
+
+
 def test_host_plan_footprint_equals_oracle_cartesian_banded():
     g = cg.StructuredGrid(cg.CartesianGeometry(), cg.axis(0, 1000.0, 64), cg.axis(0, 1500.0, 48), periodic=(True, True))
     p = cg.plan_filter(g, cg.GaussianKernel(6.0), 8000.0, engine="banded")
