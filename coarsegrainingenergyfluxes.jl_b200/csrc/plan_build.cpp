@@ -200,25 +200,27 @@ void build_banded(const cgef_plan* p, Banded& B) {
       }
     }
   });
-  B.ptr.push_back(0);
-  int64_t total = 0;
-  for (int j = 0; j < ny; ++j) total += outs[j].n;
-  (void)total;
-  for (int j = 0; j < ny; ++j) {
+  // concatenate in band order: each band's half rows go to its offset in one pre-sized array
+  std::vector<size_t> base(static_cast<size_t>(ny) + 1, 0);
+  for (int j = 0; j < ny; ++j) base[j + 1] = base[j] + outs[j].whalf.size();
+  B.w.resize(base[ny]);
+  parallel_for(ny, [&](int j) {
     BandOut& o = outs[j];
-    const int32_t base = static_cast<int32_t>(B.w.size());
+    std::copy(o.whalf.begin(), o.whalf.end(), B.w.begin() + static_cast<std::ptrdiff_t>(base[j]));
     for (int r = 0; r < 2 * dj_lim + 1; ++r) {
       BandRow& br = B.rows[static_cast<size_t>(j) * (2 * dj_lim + 1) + r];
       if (o.a[r] >= 0) {
-        br.woff = base + o.off[r];
+        br.woff = static_cast<int32_t>(base[j]) + o.off[r];
         br.a = o.a[r];
         br.hi = o.hi[r];
-        B.Amax = std::max(B.Amax, o.a[r]);
       }
     }
-    B.w.insert(B.w.end(), o.whalf.begin(), o.whalf.end());
-    B.ptr.push_back(B.ptr.back() + o.n);
     std::vector<double>().swap(o.whalf);
+  });
+  B.ptr.push_back(0);
+  for (int j = 0; j < ny; ++j) {
+    for (int a : outs[j].a) B.Amax = std::max(B.Amax, a);
+    B.ptr.push_back(B.ptr.back() + outs[j].n);
   }
 }
 
@@ -400,14 +402,17 @@ int build_plan_tables(cgef_plan* p) {
 
   if (p->engine == CGEF_ENGINE_BANDED) {
     build_banded(p, B);
+    // the half-row tables are indexed by 32-bit offsets (BandRow::woff)
+    if (B.w.size() > static_cast<size_t>(INT32_MAX))
+      return fail(CGEF_EINVAL, "footprint too large: more than 2^31 half-row weights (reduce the scale or the grid)");
     p->D = B.D;
     p->Amax = B.Amax;
     p->dj_lim = B.D;
     p->di_max = B.Amax;
-    p->h_rows = B.rows;
-    p->h_whalf = B.w;
-    p->h_ptr = B.ptr;
-    p->nentries = B.ptr.back();
+    p->h_rows = std::move(B.rows);
+    p->h_whalf = std::move(B.w);
+    p->h_ptr = std::move(B.ptr);
+    p->nentries = p->h_ptr.back();
     // ZeroFill denominator: the footprint mass over in-domain entries, in CSR order
     // (Filtering.jl:2574-2582 accumulate w for every in-domain entry).
     const int64_t W = 2 * B.D + 1;
@@ -456,9 +461,11 @@ int build_plan_tables(cgef_plan* p) {
     // than a fair share is split along the source rows into partial items, longest first.
     p->H = std::max(B.Amax, 1);
     int rc;
-    if ((rc = upload(p, &p->d_rows, B.rows.data(), B.rows.size())) != CGEF_OK) return rc;
-    if (B.w.empty()) B.w.push_back(0.0);
-    if ((rc = upload(p, &p->d_w, B.w.data(), B.w.size())) != CGEF_OK) return rc;
+    if ((rc = upload(p, &p->d_rows, p->h_rows.data(), p->h_rows.size())) != CGEF_OK) return rc;
+    const double no_weights = 0.0;  // a footprint without entries still gets a one-element table
+    if ((rc = upload(p, &p->d_w, p->h_whalf.empty() ? &no_weights : p->h_whalf.data(),
+                     std::max<size_t>(p->h_whalf.size(), 1))) != CGEF_OK)
+      return rc;
     if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
     const unsigned long long queue0[2] = {0, 0};
     if ((rc = upload(p, &p->d_queue, queue0, 2)) != CGEF_OK) return rc;
@@ -466,7 +473,7 @@ int build_plan_tables(cgef_plan* p) {
     // Mirrored columns may be paired when every row's interval is symmetric, or when the only
     // asymmetric rows close a periodic ring (their +a column is their -a column).
     bool symmetric = true;
-    for (const BandRow& r : B.rows)
+    for (const BandRow& r : p->h_rows)
       if (r.a >= 0 && r.hi != r.a) symmetric = false;
     p->paired = CGEF_PAIRED && (symmetric || p->periodic_x);
     if ((rc = build_row_spectra(p)) != CGEF_OK) return rc;
