@@ -10,6 +10,8 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG_ROOT = os.path.dirname(HERE)
@@ -55,30 +57,42 @@ def build_peak_probe(force: bool = False) -> str:
 
 
 def build(verbose: bool = False, force: bool = False, out: str = LIB_PATH, defines=()) -> str:
-    """Compiles the library to `out` (default: in place); `defines` are extra -D tuning macros."""
+    """Compiles the library to `out` (default: in place); `defines` are extra -D tuning macros.  The
+    sources compile in parallel to objects in a temporary directory, then link into one shared library."""
     if not force and out == LIB_PATH and not needs_build():
         return out
-    cmd = [
-        _nvcc(), "-O3", "-std=c++17",
-        "-gencode", "arch=compute_100a,code=sm_100a",
-        "-lineinfo", "--fmad=false",
-        "-Xcompiler", "-fPIC", "-shared",
-        "-I", INCLUDE, "-I", CSRC,
-        *[f"-D{d}" for d in defines],
-        *[os.path.join(CSRC, s) for s in SOURCES],
-        "-o", out + ".tmp",
-    ]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
     env = dict(os.environ)
     env.setdefault("NVCC_CCBIN", "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++")
-    cmd[1:1] = ["-ccbin", env["NVCC_CCBIN"]]
-    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
-    if r.returncode != 0:
-        sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libcgef_b200.so")
+    common = [
+        _nvcc(), "-ccbin", env["NVCC_CCBIN"], "-O3", "-std=c++17",
+        "-gencode", "arch=compute_100a,code=sm_100a",
+        "-lineinfo", "--fmad=false",
+        "-Xcompiler", "-fPIC",
+        "-I", INCLUDE, "-I", CSRC,
+        *[f"-D{d}" for d in defines],
+    ]
     if verbose:
-        sys.stderr.write(r.stderr)
+        common.insert(1, "-Xptxas=-v")
+    with tempfile.TemporaryDirectory(prefix="cgef_build_") as tmp:
+        objs = [os.path.join(tmp, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+
+        def compile_one(k: int):
+            return subprocess.run(common + ["-c", os.path.join(CSRC, SOURCES[k]), "-o", objs[k]],
+                                  capture_output=True, text=True, env=env)
+
+        with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+            results = list(ex.map(compile_one, range(len(SOURCES))))
+        for r in results:
+            if r.returncode != 0 or verbose:
+                sys.stderr.write(r.stdout + r.stderr)
+        if any(r.returncode != 0 for r in results):
+            raise RuntimeError("nvcc failed building libcgef_b200.so")
+        link = [_nvcc(), "-ccbin", env["NVCC_CCBIN"], "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+                *objs, "-o", out + ".tmp"]
+        r = subprocess.run(link, capture_output=True, text=True, env=env)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc failed linking libcgef_b200.so")
     os.replace(out + ".tmp", out)
     return out
 

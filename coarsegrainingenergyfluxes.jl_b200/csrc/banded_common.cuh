@@ -44,6 +44,12 @@ struct BandedK {
   double* out[9];
   int64_t out_stride;
   unsigned long long* queue;  // [next unit, warps finished]; zero when a launch starts
+  // The stage's non-finite flags (nslices + 1, the last set when any is; stage_flags): the fast gather
+  // skips flagged slices, the zero-weight-skipping gather sums only them.
+  const int* flags;
+  // nullptr, or the unnormalised sums [slice][NA][ny][nx] are written there instead of the finished
+  // outputs (the row-spectral evaluation's layout, which its epilogue then finishes).
+  double* raw;
 };
 
 // Expands the staged values of one source cell into the accumulated quantities: the fields
@@ -175,6 +181,17 @@ __device__ __forceinline__ void finish_target(const BandedK& a, const double (&a
   write_outputs<MODE, C::NA0>(a.out, slice * a.out_stride + pix, F, zero, sl, cl, sp, cp);
 }
 
+// Stores the unnormalised sums of one target where the row-spectral evaluation keeps its own.
+template <int MODE, int NF, bool DEF>
+__device__ __forceinline__ void write_raw(const BandedK& a, const double (&acc)[Cfg<MODE, NF, DEF>::NA], int slice,
+                                          int j, int col) {
+  using C = Cfg<MODE, NF, DEF>;
+  const int64_t plane = static_cast<int64_t>(a.ny) * a.nx;
+  double* r = a.raw + static_cast<int64_t>(slice) * C::NA * plane + static_cast<int64_t>(j) * a.nx + col;
+#pragma unroll
+  for (int m = 0; m < C::NA; ++m) r[m * plane] = acc[m];
+}
+
 // The launch arguments both evaluations share: staged planes, band tables and the epilogue's
 // inputs and outputs (the direct gather adds its schedule, partials and queue).
 inline BandedK make_banded_args(const cgef_plan* p, int mode, const double* planes, int pitch, int np, int nbatch,
@@ -204,6 +221,7 @@ inline BandedK make_banded_args(const cgef_plan* p, int mode, const double* plan
   a.cosphi = sph ? p->d_cosphi : nullptr;
   for (int m = 0; m < 9; ++m) a.out[m] = out.o[m];
   a.out_stride = out.slice_stride;
+  a.flags = stage_flags(p, planes, np, pitch, nbatch);
   return a;
 }
 

@@ -167,7 +167,7 @@ int stage_pi(cgef_plan* p, int dtype, const void* u, const void* v, int nbatch, 
   const int np = (mode == kModePiSphere ? 3 : 2) + (def ? 1 : 0);
   const int pitch = pitch_for(p, halo);
   void* planes = nullptr;
-  int rc = ensure_ws(p, kSlotPlanes, sizeof(double) * np * static_cast<int64_t>(p->ny) * pitch * nbatch, &planes);
+  int rc = ensure_ws(p, kSlotPlanes, stage_bytes(p, np, pitch, nbatch), &planes);
   if (rc) return rc;
   StageArgs sa{};
   sa.a = u;
@@ -244,7 +244,7 @@ int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int
   const int np = nf + (def ? 1 : 0);
   const int pitch = pitch_for(p, p->H);
   void* planes = nullptr;
-  int rc = ensure_ws(p, kSlotPlanes, sizeof(double) * np * static_cast<int64_t>(p->ny) * pitch * nbatch, &planes);
+  int rc = ensure_ws(p, kSlotPlanes, stage_bytes(p, np, pitch, nbatch), &planes);
   if (rc) return rc;
   StageArgs sa{};
   sa.fields = fields;
@@ -424,6 +424,33 @@ extern "C" {
 
 int32_t cgef_version(void) { return CGEF_ABI_VERSION; }
 
+int32_t cgef_build_arch(void) { return 1000; }  // every .cu file refuses any other device target
+
+int32_t cgef_plan_reset_queue(cgef_plan* p) {
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (p->d_queue == nullptr) return CGEF_OK;
+  DeviceGuard dg(p->device);
+  cudaError_t e = cudaMemsetAsync(p->d_queue, 0, 2 * sizeof(unsigned long long), p->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+  return e == cudaSuccess ? CGEF_OK : cuda_fail(e, "cgef_plan_reset_queue");
+}
+
+int32_t cgef_debug_inject(void* object, int32_t what) {
+  if (!object) return fail(CGEF_EINVAL, "object is NULL");
+  if (what == CGEF_INJECT_CLOSURE_TIMEOUT) return closure_inject_timeout(static_cast<cgef_closure*>(object));
+  if (what != CGEF_INJECT_STALE_QUEUE) return fail(CGEF_EINVAL, "unknown injection");
+  cgef_plan* p = static_cast<cgef_plan*>(object);
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (p->d_queue == nullptr) return fail(CGEF_EINVAL, "the plan has no work queue (not the banded engine)");
+  DeviceGuard dg(p->device);
+  // a launch that handed out 7 units and saw 3 warps leave
+  const unsigned long long stale[2] = {7ull, 3ull};
+  cudaError_t e = cudaMemcpy(p->d_queue, stale, sizeof(stale), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? CGEF_OK : cuda_fail(e, "work queue");
+}
+
 const char* cgef_last_error(void) { return g_err.c_str(); }
 
 int32_t cgef_device_count(void) {
@@ -515,6 +542,9 @@ int32_t cgef_plan_create(cgef_plan** out, const cgef_grid_desc* g, int32_t kerne
     cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreate");
   }
+  // The allocation-free filter's fixed array is reserved on this device now, by resolving its
+  // address, so that entry point's first call on the device does not reserve it itself.
+  if (rc == CGEF_OK && p->device >= 0) rc = noalloc_prepare(p->device);
   if (rc != CGEF_OK) {
     std::string msg = g_err;
     cgef_plan_destroy(p);

@@ -10,6 +10,12 @@
 
 #include "cgef_b200.h"
 
+// Every kernel of the library is written for sm_100a (tcgen05, its shared-memory and register
+// budgets); cgef_build_arch() reports 1000 on the strength of this guard.
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ != 1000 || !defined(__CUDA_ARCH_FEAT_SM100_ALL))
+#error "libcgef_b200 device code is built for sm_100a only"
+#endif
+
 namespace cgef {
 
 // Filtering.jl:1633 and every apply path: denominators at or below this give 0.
@@ -31,6 +37,8 @@ constexpr int kRowsTall = 2 * CGEF_ROWS;
 constexpr int kWarps = CGEF_WARPS;
 // Width of the staged planes' column tiling (the pitch is padded to a multiple of this).
 constexpr int kTileCols = 160;
+// Most slices one launch takes (the grid's z extent of the per-slice kernels).
+constexpr int kMaxSlices = 65535;
 
 // One (target band j, source row offset dj) of the banded footprint: weights for longitude
 // offsets di in [-a, hi] live at w[woff + |di|] (the sphere's weight is even in di).  a < 0
@@ -175,6 +183,14 @@ double kernel_radius(int kernel, double alpha, double ell);
 // Host plan construction (plan_build.cpp).
 int build_plan_tables(cgef_plan* p);
 
+// Sets the closure's device error word from the host, as a bounded wait that ran out sets it
+// (cgef_debug_inject; closure.cu).
+int closure_inject_timeout(cgef_closure* c);
+
+// Resolves, on `device` (current), the device address of the allocation-free filter's fixed scratch
+// array (noalloc.cu); resolving it is what makes the driver reserve the array on that device.
+int noalloc_prepare(int device);
+
 // Banded schedule pieces.  Source-row costs of the R-row target group starting at j0: for each
 // source row in [j0 - D, j0 + R - 1 + D], the width of the union of the group's intervals plus a
 // per-row overhead (0 where the row is outside a bounded grid or holds no entries).
@@ -236,9 +252,27 @@ struct StageArgs {
   int nbatch;
 };
 
+// The staged planes [nbatch][np][ny][pitch] (FP64) are followed, 256-byte aligned, by nbatch + 1 int
+// flags: flag s is set when an active source cell of slice s holds a non-finite value (or, in the
+// flux modes, a non-finite product of two), the last flag when any slice's is.  The banded engine
+// sums a flagged slice with a gather that never multiplies a zero weight by a staged value, so a NaN
+// or Inf reaches exactly the targets whose footprint holds its cell, as in the reference's per-entry
+// loop (Filtering.jl:2575-2585).
+inline size_t stage_planes_bytes(const cgef_plan* p, int np, int pitch, int nbatch) {
+  return (sizeof(double) * static_cast<size_t>(np) * p->ny * pitch * nbatch + 255) / 256 * 256;
+}
+inline size_t stage_bytes(const cgef_plan* p, int np, int pitch, int nbatch) {
+  return stage_planes_bytes(p, np, pitch, nbatch) + sizeof(int) * (static_cast<size_t>(nbatch) + 1);
+}
+inline int* stage_flags(const cgef_plan* p, const double* planes, int np, int pitch, int nbatch) {
+  return reinterpret_cast<int*>(reinterpret_cast<char*>(const_cast<double*>(planes)) +
+                                stage_planes_bytes(p, np, pitch, nbatch));
+}
+
 // Writes padded FP64 planes [nbatch][np][ny][pitch] with halo H (wrapped or zero), masked
 // values, planetary components on the sphere for kModePiSphere, and a mask plane when
-// `with_mask_plane`.
+// `with_mask_plane`; then the non-finite flags after them (stage_flags).  The planes buffer holds
+// stage_bytes().
 int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* planes, int pitch, int halo, int np,
                  bool with_mask_plane, cudaStream_t st);
 
@@ -280,15 +314,26 @@ int build_row_spectra(cgef_plan* p);
 
 // The same over a caller-given device schedule: work items and the split groups they belong to
 // (e.g. from subset_schedule); `partials` holds the slots that schedule numbers.
+// Slices the stage flagged as holding a non-finite value are skipped by the fast gather and summed by
+// a second launch that skips zero weights (it returns at once when no slice is flagged).
 int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                         const uint8_t* mask, int64_t mask_slice_stride, double* partials, const WorkItem* items,
                         int nitems, const SplitGroup* groups, int ngroups, const GatherOut& out, cudaStream_t st);
 
+// Only the flagged slices, by that second gather, over the full schedule, with their unnormalised sums
+// written to `raw` in the row-spectral layout [slice][NA][ny][nx] (the row-spectral evaluation's
+// non-finite fallback; its epilogue then finishes them).
+int launch_banded_nonfinite(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                            const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
+                            cudaStream_t st, double* raw);
+
 // Bytes of partial-sum scratch a banded launch of `mode` with `na` accumulated quantities over
-// `nbatch` slices needs.
+// `nbatch` slices needs (its own schedule's, or the kRows schedule's that the non-finite pass uses).
 inline size_t banded_partials_bytes(const cgef_plan* p, int na, int nbatch, int mode) {
   const Schedule& s = schedule_for(p, mode, na);
-  return sizeof(double) * static_cast<size_t>(s.nslots) * nbatch * s.rows * na * 32;
+  const size_t own = sizeof(double) * static_cast<size_t>(s.nslots) * nbatch * s.rows * na * 32;
+  const size_t safe = sizeof(double) * static_cast<size_t>(p->sched[0].nslots) * nbatch * kRows * na * 32;
+  return std::max(own, safe);
 }
 
 // Bytes of the row-spectral evaluation's scratch: the spectra of the source rows and the summed
@@ -297,10 +342,12 @@ inline size_t rowspec_bytes(const cgef_plan* p, int na, int nbatch) {
   return 2 * 2 * sizeof(double) * static_cast<size_t>(nbatch) * p->ny * na * p->rs_nkp;
 }
 
-// Scratch of a full-grid banded launch, whichever evaluation the plan uses.
+// Scratch of a full-grid banded launch, whichever evaluation the plan uses: the row-spectral
+// evaluation's spectra, then the direct gather's split-tile partials (its non-finite fallback runs
+// while the spectral evaluation's unnormalised sums are still live).
 inline size_t banded_scratch_bytes(const cgef_plan* p, int na, int nbatch, int mode) {
   const size_t d = banded_partials_bytes(p, na, nbatch, mode);
-  return p->rs_on ? std::max(d, rowspec_bytes(p, na, nbatch)) : d;
+  return p->rs_on ? rowspec_bytes(p, na, nbatch) + d : d;
 }
 
 int launch_separable(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,

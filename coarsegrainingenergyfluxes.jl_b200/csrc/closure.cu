@@ -747,12 +747,20 @@ int check_closure(const cgef_closure* c) {
   return CGEF_OK;
 }
 
+// The error word a kernel sets when a bounded wait runs out: reported as CGEF_ETIMEOUT, then cleared
+// so that the closure's next call starts clean (the wait's kernel released its tensor memory and
+// returned; the context stays usable).
 int read_err(cgef_closure* c, cudaStream_t st) {
   int h = 0;
   cudaError_t e = cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(e, "closure error flag");
-  if (h) return fail(CGEF_ECUDA, "a closure tensor-core step did not complete within its wait limit");
+  if (h) {
+    e = cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "closure error flag reset");
+    return fail(CGEF_ETIMEOUT, "a closure tensor-core step did not complete within its wait limit");
+  }
   return CGEF_OK;
 }
 
@@ -885,6 +893,13 @@ uint64_t splitmix(uint64_t& s) {
 }
 
 }  // namespace
+
+int cgef::closure_inject_timeout(cgef_closure* c) {
+  if (!c) return fail(CGEF_EINVAL, "closure is NULL");
+  const int one = 1;
+  cudaError_t e = cudaMemcpy(c->d_err, &one, sizeof(int), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? CGEF_OK : cuda_fail(e, "closure error word");
+}
 
 extern "C" {
 

@@ -81,6 +81,9 @@ struct StageK {
   const double* sinphi;
   const double* cosphi;
   double* planes;
+  int* flags;          // nslices + 1 non-finite flags (zeroed before the launch)
+  int nslices;
+  int check_products;  // flux modes: a product of two staged values must be finite too
 };
 
 template <int MODE>
@@ -113,6 +116,18 @@ __global__ void stage_kernel(StageK a) {
       } else {
         for (int m = 0; m < a.nf; ++m) vals[m] = load_any(a.f[m], a.dtype, k);
       }
+      // an active non-finite value (or product, which the flux accumulates) flags the slice
+      const int nv = MODE == kModePiSphere ? 3 : a.nf;
+      bool bad = false;
+      for (int m = 0; m < nv; ++m) {
+        bad |= !isfinite(vals[m]);
+        if (a.check_products)
+          for (int n = m; n < nv; ++n) bad |= !isfinite(vals[m] * vals[n]);
+      }
+      if (bad) {
+        a.flags[s] = 1;
+        a.flags[a.nslices] = 1;
+      }
     }
   }
   double* out = a.planes + s * a.slice_stride + static_cast<int64_t>(j) * a.pitch + p;
@@ -137,11 +152,18 @@ __global__ void stage_kernel(StageK a) {
 // 12 DMUL + 2*R*NA DFMA.
 // The centre column (d = 0) is its own mirror and a ring-closing row's +a column is its -a column on a
 // periodic ring (the reference visits [-a, a-1]); both carry half weight, which is exact in FP64.
-template <int MODE, int NF, bool DEF, int R, bool PAIR>
+//
+// SAFE: the slice holds a non-finite source value (the stage's flag).  A zero weight (a column inside a
+// row's window but outside its disk, or outside the row's own interval in the warp's shared column
+// range) must not multiply it, so the warp skips zero weights -- the weight is the same for every
+// lane, so the branch is uniform.  The fast gather skips flagged slices and the SAFE gather sums only
+// them, so each slice is summed once.
+template <int MODE, int NF, bool DEF, int R, bool PAIR, bool SAFE>
 __device__ __forceinline__ void banded_unit(const BandedK& a, int64_t gid, double* wb, int (&ri)[3][R], int lane) {
   using C = Cfg<MODE, NF, DEF>;
   const int item_id = static_cast<int>(gid / a.nslices);
   const int slice = static_cast<int>(gid - static_cast<int64_t>(item_id) * a.nslices);
+  if ((a.flags[slice] != 0) != SAFE) return;
   const WorkItem it = a.items[item_id];
   const int col = it.x0 + lane;
   const int j0 = it.j0;
@@ -230,6 +252,7 @@ __device__ __forceinline__ void banded_unit(const BandedK& a, int64_t gid, doubl
 #pragma unroll
           for (int t = 0; t < R; ++t) {
             const double wt = wb[t * 32 + kk];
+            if (SAFE && wt == 0.0) continue;
 #pragma unroll
             for (int m = 0; m < C::NA; ++m) acc[t][m] = fma(wt, q[m], acc[t][m]);
           }
@@ -260,6 +283,7 @@ __device__ __forceinline__ void banded_unit(const BandedK& a, int64_t gid, doubl
 #pragma unroll
           for (int t = 0; t < R; ++t) {
             const double wt = wb[t * 32 + kk];
+            if (SAFE && wt == 0.0) continue;
 #pragma unroll
             for (int m = 0; m < C::NA; ++m) acc[t][m] = fma(wt, q[m], acc[t][m]);
           }
@@ -283,7 +307,10 @@ __device__ __forceinline__ void banded_unit(const BandedK& a, int64_t gid, doubl
   for (int t = 0; t < R; ++t) {
     const int j = j0 + t;
     if (j >= a.ny) break;
-    finish_target<MODE, NF, DEF>(a, acc[t], slice, j, col);
+    if (a.raw != nullptr)
+      write_raw<MODE, NF, DEF>(a, acc[t], slice, j, col);
+    else
+      finish_target<MODE, NF, DEF>(a, acc[t], slice, j, col);
   }
 }
 
@@ -310,15 +337,16 @@ __device__ __forceinline__ void leave_queue(unsigned long long* queue, int lane)
 // Persistent launch: at most as many warps as fit on the GPU at once, each taking (item, slice)
 // units in the schedule's longest-first order until none is left, so no warp idles behind a slower
 // sibling of its block while units remain.  Results do not depend on which warp takes a unit.
-template <int MODE, int NF, bool DEF, int R, bool PAIR>
+template <int MODE, int NF, bool DEF, int R, bool PAIR, bool SAFE>
 __global__ void __launch_bounds__(32 * kWarps, banded_min_blocks(MODE)) banded_kernel(BandedK a) {
   __shared__ double wbuf[kWarps][R][32];
   __shared__ int rint[kWarps][3][R];  // per warp: a, hi, woff of the R rows for the current source row
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
+  if (SAFE && a.flags[a.nslices] == 0) return;  // no flagged slice: no warp takes a unit, the queue stays 0
   const int64_t total = static_cast<int64_t>(a.nitems) * a.nslices;
   for (int64_t gid = take_unit(a.queue, lane); gid < total; gid = take_unit(a.queue, lane)) {
-    banded_unit<MODE, NF, DEF, R, PAIR>(a, gid, &wbuf[warp][0][0], rint[warp], lane);
+    banded_unit<MODE, NF, DEF, R, PAIR, SAFE>(a, gid, &wbuf[warp][0][0], rint[warp], lane);
     __syncwarp();
   }
   leave_queue(a.queue, lane);
@@ -327,7 +355,7 @@ __global__ void __launch_bounds__(32 * kWarps, banded_min_blocks(MODE)) banded_k
 // Adds the partial slots of every split tile in slot order (deterministic) and finishes it: one warp
 // per (tile, slice, target row).  The loads of four slots are in flight together; the additions stay
 // in slot order.
-template <int MODE, int NF, bool DEF, int R>
+template <int MODE, int NF, bool DEF, int R, bool SAFE>
 __global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
   using C = Cfg<MODE, NF, DEF>;
   constexpr int kAhead = 4;
@@ -338,6 +366,7 @@ __global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
   const int64_t gs = gid / R;
   const int gi = static_cast<int>(gs / a.nslices);
   const int slice = static_cast<int>(gs - static_cast<int64_t>(gi) * a.nslices);
+  if ((a.flags[slice] != 0) != SAFE) return;
   const SplitGroup g = a.groups[gi];
   const int col = g.x0 + lane;
   const int j = g.j0 + t;
@@ -363,7 +392,10 @@ __global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
   for (; q < g.nslots; ++q)
 #pragma unroll
     for (int m = 0; m < C::NA; ++m) acc[m] += p0[q * slot_stride + m * 32];
-  finish_target<MODE, NF, DEF>(a, acc, slice, j, col);
+  if (a.raw != nullptr)
+    write_raw<MODE, NF, DEF>(a, acc, slice, j, col);
+  else
+    finish_target<MODE, NF, DEF>(a, acc, slice, j, col);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -977,6 +1009,11 @@ int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* plane
   a.sinphi = p->d_sinphi;
   a.cosphi = p->d_cosphi;
   a.planes = planes;
+  a.flags = stage_flags(p, planes, np, pitch, s.nbatch);
+  a.nslices = s.nbatch;
+  a.check_products = mode != kModeFields;
+  cudaError_t e = cudaMemsetAsync(a.flags, 0, sizeof(int) * (static_cast<size_t>(s.nbatch) + 1), st);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(stage flags)");
   dim3 block(256), grid((pitch + 255) / 256, p->ny, s.nbatch);
   prof_begin(CGEF_KERNEL_STAGE, st);
   if (mode == kModePiSphere)
@@ -1005,25 +1042,32 @@ int64_t resident_blocks(K kernel) {
   return cached[dev];
 }
 
-template <int MODE, int NF, bool DEF, int R>
+// The gather (then the combine pass of split tiles) over the launch's slices: the fast gather over
+// the unflagged ones (SAFE false, timed as the banded kind), or the zero-weight-skipping one over the
+// slices the stage flagged as non-finite (SAFE true; returns at once when none is).
+template <int MODE, int NF, bool DEF, int R, bool SAFE>
 int run_banded(const BandedK& a, bool pair, cudaStream_t st) {
   const int64_t units = static_cast<int64_t>(a.nitems) * a.nslices;
   const int64_t need = (units + kWarps - 1) / kWarps;
-  prof_begin(CGEF_KERNEL_BANDED, st);
+  // the queue starts at zero even after a launch that stopped part-way (the kernel's last warp also
+  // zeroes it on the way out)
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, 2 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(work queue)");
+  if (!SAFE) prof_begin(CGEF_KERNEL_BANDED, st);
   if (pair) {
-    const auto k = banded_kernel<MODE, NF, DEF, R, true>;
+    const auto k = banded_kernel<MODE, NF, DEF, R, true, SAFE>;
     k<<<static_cast<unsigned>(std::min(need, resident_blocks(k))), 32 * kWarps, 0, st>>>(a);
   } else {
-    const auto k = banded_kernel<MODE, NF, DEF, R, false>;
+    const auto k = banded_kernel<MODE, NF, DEF, R, false, SAFE>;
     k<<<static_cast<unsigned>(std::min(need, resident_blocks(k))), 32 * kWarps, 0, st>>>(a);
   }
   int rc = check_launch("banded_kernel");
   if (rc == CGEF_OK && a.ngroups > 0) {
     const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices * R;
-    banded_combine_kernel<MODE, NF, DEF, R><<<static_cast<unsigned>((cw + 3) / 4), 128, 0, st>>>(a);
+    banded_combine_kernel<MODE, NF, DEF, R, SAFE><<<static_cast<unsigned>((cw + 3) / 4), 128, 0, st>>>(a);
     rc = check_launch("banded_combine_kernel");
   }
-  prof_end(CGEF_KERNEL_BANDED, st);
+  if (!SAFE) prof_end(CGEF_KERNEL_BANDED, st);
   return rc;
 }
 
@@ -1033,12 +1077,20 @@ template <int MODE, int NF>
 int dispatch_banded(bool def, int R, bool pair, const BandedK& a, cudaStream_t st) {
   if constexpr (MODE == kModeFields && NF + 1 <= kTallMaxQuantities) {
     if (R == kRowsTall)
-      return def ? run_banded<MODE, NF, true, kRowsTall>(a, pair, st)
-                 : run_banded<MODE, NF, false, kRowsTall>(a, pair, st);
+      return def ? run_banded<MODE, NF, true, kRowsTall, false>(a, pair, st)
+                 : run_banded<MODE, NF, false, kRowsTall, false>(a, pair, st);
   } else if constexpr (MODE == kModeFields && NF <= kTallMaxQuantities) {
-    if (R == kRowsTall && !def) return run_banded<MODE, NF, false, kRowsTall>(a, pair, st);
+    if (R == kRowsTall && !def) return run_banded<MODE, NF, false, kRowsTall, false>(a, pair, st);
   }
-  return def ? run_banded<MODE, NF, true, kRows>(a, pair, st) : run_banded<MODE, NF, false, kRows>(a, pair, st);
+  return def ? run_banded<MODE, NF, true, kRows, false>(a, pair, st)
+             : run_banded<MODE, NF, false, kRows, false>(a, pair, st);
+}
+
+// The zero-weight-skipping gather over the flagged slices: kRows-row tiles only.
+template <int MODE, int NF>
+int dispatch_banded_safe(bool def, bool pair, const BandedK& a, cudaStream_t st) {
+  return def ? run_banded<MODE, NF, true, kRows, true>(a, pair, st)
+             : run_banded<MODE, NF, false, kRows, true>(a, pair, st);
 }
 
 }  // namespace
@@ -1052,33 +1104,72 @@ int launch_banded(const cgef_plan* p, int mode, int nf, const double* planes, in
                              nullptr, 0, out, st);
 }
 
+namespace {
+
+// Both gathers of a launch, or only the zero-weight-skipping one (safe_only, writing raw sums).
+int banded_gathers(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                   const uint8_t* mask, int64_t mask_slice_stride, double* partials, const WorkItem* items, int nitems,
+                   const SplitGroup* groups, int ngroups, const GatherOut& out, cudaStream_t st, bool safe_only,
+                   double* raw) {
+  const bool def = p->strategy == CGEF_DEFORMABLE;
+  BandedK a = make_banded_args(p, mode, planes, pitch, np, nbatch, mask, mask_slice_stride, out);
+  a.raw = raw;
+  a.partials = partials;
+  a.queue = p->d_queue;
+  if (a.queue == nullptr) return fail(CGEF_EINVAL, "banded: the plan has no work queue");
+  const int na = (mode == kModePiSphere ? 9 : (mode == kModePiCart ? 5 : nf)) + (def ? 1 : 0);
+  const bool pair = p->paired;
+  if (nf < 1 || nf > 4) return fail(CGEF_EINVAL, "banded: 1..4 fields per pass");
+  int rc = CGEF_OK;
+  if (!safe_only) {
+    const Schedule& S = schedule_for(p, mode, na);
+    const int R = items ? kRows : S.rows;
+    a.items = items ? items : S.d_items;
+    a.nitems = items ? nitems : static_cast<int>(S.h_items.size());
+    a.groups = items ? groups : S.d_groups;
+    a.ngroups = items ? ngroups : static_cast<int>(S.h_groups.size());
+    if (a.nitems == 0) return CGEF_OK;
+    if (a.ngroups > 0 && partials == nullptr) return fail(CGEF_EINVAL, "banded: split tiles need a partials buffer");
+    if (mode == kModePiSphere) rc = dispatch_banded<kModePiSphere, 1>(def, R, pair, a, st);
+    else if (mode == kModePiCart) rc = dispatch_banded<kModePiCart, 1>(def, R, pair, a, st);
+    else if (nf == 1) rc = dispatch_banded<kModeFields, 1>(def, R, pair, a, st);
+    else if (nf == 2) rc = dispatch_banded<kModeFields, 2>(def, R, pair, a, st);
+    else if (nf == 3) rc = dispatch_banded<kModeFields, 3>(def, R, pair, a, st);
+    else rc = dispatch_banded<kModeFields, 4>(def, R, pair, a, st);
+    if (rc) return rc;
+  }
+  // the slices flagged as holding a non-finite value, with kRows-row tiles
+  const Schedule& S0 = p->sched[0];
+  a.items = items ? items : S0.d_items;
+  a.nitems = items ? nitems : static_cast<int>(S0.h_items.size());
+  a.groups = items ? groups : S0.d_groups;
+  a.ngroups = items ? ngroups : static_cast<int>(S0.h_groups.size());
+  if (a.nitems == 0) return CGEF_OK;
+  if (a.ngroups > 0 && partials == nullptr) return fail(CGEF_EINVAL, "banded: split tiles need a partials buffer");
+  if (mode == kModePiSphere) return dispatch_banded_safe<kModePiSphere, 1>(def, pair, a, st);
+  if (mode == kModePiCart) return dispatch_banded_safe<kModePiCart, 1>(def, pair, a, st);
+  switch (nf) {
+    case 1: return dispatch_banded_safe<kModeFields, 1>(def, pair, a, st);
+    case 2: return dispatch_banded_safe<kModeFields, 2>(def, pair, a, st);
+    case 3: return dispatch_banded_safe<kModeFields, 3>(def, pair, a, st);
+    default: return dispatch_banded_safe<kModeFields, 4>(def, pair, a, st);
+  }
+}
+
+}  // namespace
+
 int launch_banded_items(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                         const uint8_t* mask, int64_t mask_slice_stride, double* partials, const WorkItem* items,
                         int nitems, const SplitGroup* groups, int ngroups, const GatherOut& out, cudaStream_t st) {
-  const bool def = p->strategy == CGEF_DEFORMABLE;
-  BandedK a = make_banded_args(p, mode, planes, pitch, np, nbatch, mask, mask_slice_stride, out);
-  const int na = (mode == kModePiSphere ? 9 : (mode == kModePiCart ? 5 : nf)) + (def ? 1 : 0);
-  const Schedule& S = schedule_for(p, mode, na);
-  const int R = items ? kRows : S.rows;
-  a.items = items ? items : S.d_items;
-  a.nitems = items ? nitems : static_cast<int>(S.h_items.size());
-  a.groups = items ? groups : S.d_groups;
-  a.ngroups = items ? ngroups : static_cast<int>(S.h_groups.size());
-  if (a.nitems == 0) return CGEF_OK;
-  a.partials = partials;
-  if (a.ngroups > 0 && partials == nullptr) return fail(CGEF_EINVAL, "banded: split tiles need a partials buffer");
-  a.queue = p->d_queue;
-  if (a.queue == nullptr) return fail(CGEF_EINVAL, "banded: the plan has no work queue");
-  const bool pair = p->paired;
-  if (mode == kModePiSphere) return dispatch_banded<kModePiSphere, 1>(def, R, pair, a, st);
-  if (mode == kModePiCart) return dispatch_banded<kModePiCart, 1>(def, R, pair, a, st);
-  switch (nf) {
-    case 1: return dispatch_banded<kModeFields, 1>(def, R, pair, a, st);
-    case 2: return dispatch_banded<kModeFields, 2>(def, R, pair, a, st);
-    case 3: return dispatch_banded<kModeFields, 3>(def, R, pair, a, st);
-    case 4: return dispatch_banded<kModeFields, 4>(def, R, pair, a, st);
-    default: return fail(CGEF_EINVAL, "banded: 1..4 fields per pass");
-  }
+  return banded_gathers(p, mode, mode == kModeFields ? nf : 1, planes, pitch, np, nbatch, mask, mask_slice_stride,
+                        partials, items, nitems, groups, ngroups, out, st, false, nullptr);
+}
+
+int launch_banded_nonfinite(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                            const uint8_t* mask, int64_t mask_slice_stride, double* partials, const GatherOut& out,
+                            cudaStream_t st, double* raw) {
+  return banded_gathers(p, mode, mode == kModeFields ? nf : 1, planes, pitch, np, nbatch, mask, mask_slice_stride,
+                        partials, nullptr, 0, nullptr, 0, out, st, true, raw);
 }
 
 namespace {

@@ -3,14 +3,19 @@
 //
 // The scratch is g_noalloc_scratch below: kNoallocScratchBytes of device memory that every GPU
 // which loads the library holds until the process exits.  Host code cannot use the array's name
-// as a device address (in host code it names a host-side stand-in), so the first call on each
-// device, with that device current, resolves the address with cudaGetSymbolAddress and keeps it;
-// later calls reuse it.
+// as a device address (in host code it names a host-side stand-in), so the address is resolved with
+// cudaGetSymbolAddress once per device, with that device current, and kept.  The CUDA driver loads
+// this file's module -- and so reserves the array -- only when something first asks for it, and
+// resolving the address is that request.  cgef_plan_create therefore resolves it on the plan's
+// device (noalloc_prepare), so the allocation-free entry point itself never makes the driver
+// reserve memory; should a plan reach it on a device where that did not happen, its call resolves
+// the address then.
 //
-// Every call shares the one array and the array keeps the previous call's contents.  Nothing in it
-// needs to start at zero: the staging kernel writes every element the filter then reads, halos
-// included.  Calls whose work overlaps on the GPU (different streams, or different host threads)
-// race on the array and must be serialised by the caller.
+// Every call shares the one array and the array keeps the previous call's contents.  The non-finite
+// flags after the staged planes are zeroed by the call (cudaMemsetAsync, which allocates nothing)
+// and the staging kernel writes every other element the filter then reads, halos included.  Calls
+// whose work overlaps on the GPU (different streams, or different host threads) race on the array and
+// must be serialised by the caller.
 #include <mutex>
 
 #include "cgef_internal.h"
@@ -44,6 +49,11 @@ size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 
 }  // namespace
 
+int cgef::noalloc_prepare(int device) {
+  unsigned char* ptr = nullptr;
+  return noalloc_scratch(device, &ptr);
+}
+
 extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const void* field, void* out,
                                               int64_t nbatch64, void* stream) {
   using namespace cgef;
@@ -62,7 +72,7 @@ extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const
 
   // Scratch layout: staged planes, then the engine's intermediate, then (FP32 callers) the FP64
   // result before conversion.
-  const size_t planes_b = round256(sizeof(double) * np * static_cast<size_t>(p->ny) * pitch * nbatch);
+  const size_t planes_b = round256(stage_bytes(p, np, pitch, nbatch));
   size_t engine_b = 0;
   if (p->engine == CGEF_ENGINE_SEPARABLE) engine_b = round256(sizeof(double) * 2 * static_cast<size_t>(N) * nbatch);
   if (p->engine == CGEF_ENGINE_PREFIXSUM)

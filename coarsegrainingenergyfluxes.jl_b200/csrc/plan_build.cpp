@@ -102,14 +102,19 @@ struct Banded {
 // Banded footprint (Filtering.jl:636-732).  Each (band, row offset) holds a contiguous
 // longitude interval [-a, hi]; weights are stored once per |di| because the kernel of the
 // great-circle (or Euclidean) distance is even in di.  A column inside the interval that fails
-// d <= rad keeps weight 0, which adds nothing to either sum, so the entry set is the reference's.
-void build_banded(const cgef_plan* p, Banded& B) {
+// d <= rad keeps weight 0, which adds nothing to either sum of finite values, so the entry set is the
+// reference's (a slice holding a non-finite value is summed with zero weights skipped).
+int build_banded(const cgef_plan* p, Banded& B) {
   const int nx = p->nx, ny = p->ny;
   const double rad = p->rad;
   const bool sphere = p->geometry == CGEF_SPHERICAL;
   if (!sphere) {
-    const int di_lim = p->dx > 0 ? static_cast<int>(std::ceil(rad / p->dx)) : 0;
-    const int dj_lim = p->dy > 0 ? static_cast<int>(std::ceil(rad / p->dy)) : 0;
+    const double cells_x = p->dx > 0 ? std::ceil(rad / p->dx) : 0.0;
+    const double cells_y = p->dy > 0 ? std::ceil(rad / p->dy) : 0.0;
+    if ((2.0 * cells_y + 1.0) * (cells_x + 1.0) > static_cast<double>(INT32_MAX))
+      return fail(CGEF_EINVAL, "footprint too large: more than 2^31 half-row weights (reduce the scale or the grid)");
+    const int di_lim = static_cast<int>(cells_x);
+    const int dj_lim = static_cast<int>(cells_y);
     const double A = p->dx * p->dy;
     B.D = dj_lim;
     B.rows.assign(2 * dj_lim + 1, BandRow{0, -1, -1, 0});
@@ -137,7 +142,7 @@ void build_banded(const cgef_plan* p, Banded& B) {
       }
     }
     B.ptr.push_back(n);
-    return;
+    return CGEF_OK;
   }
   const int dj_lim = p->dy > 0 ? static_cast<int>(std::ceil(rad / (p->R * p->dy))) : 0;
   const int half = nx / 2;
@@ -203,6 +208,9 @@ void build_banded(const cgef_plan* p, Banded& B) {
   // concatenate in band order: each band's half rows go to its offset in one pre-sized array
   std::vector<size_t> base(static_cast<size_t>(ny) + 1, 0);
   for (int j = 0; j < ny; ++j) base[j + 1] = base[j] + outs[j].whalf.size();
+  // the half rows are indexed by 32-bit offsets (BandRow::woff): refuse before sizing the table
+  if (base[ny] > static_cast<size_t>(INT32_MAX))
+    return fail(CGEF_EINVAL, "footprint too large: more than 2^31 half-row weights (reduce the scale or the grid)");
   B.w.resize(base[ny]);
   parallel_for(ny, [&](int j) {
     BandOut& o = outs[j];
@@ -222,6 +230,7 @@ void build_banded(const cgef_plan* p, Banded& B) {
     for (int a : outs[j].a) B.Amax = std::max(B.Amax, a);
     B.ptr.push_back(B.ptr.back() + outs[j].n);
   }
+  return CGEF_OK;
 }
 
 }  // namespace
@@ -401,10 +410,7 @@ int build_plan_tables(cgef_plan* p) {
   std::vector<PrefixRow> prows;
 
   if (p->engine == CGEF_ENGINE_BANDED) {
-    build_banded(p, B);
-    // the half-row tables are indexed by 32-bit offsets (BandRow::woff)
-    if (B.w.size() > static_cast<size_t>(INT32_MAX))
-      return fail(CGEF_EINVAL, "footprint too large: more than 2^31 half-row weights (reduce the scale or the grid)");
+    if (int rc = build_banded(p, B)) return rc;
     p->D = B.D;
     p->Amax = B.Amax;
     p->dj_lim = B.D;

@@ -675,6 +675,17 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
     rc = rs_check("rs_inverse_kernel");
   }
   if (rc == CGEF_OK) {
+    // A non-finite source value would reach every bin of its row's spectrum, so every target the row
+    // feeds; the direct sum lets it reach only the targets whose footprint holds the cell.  The stage
+    // flags such slices, and the direct gather sums them again here over the spectral sums (a launch
+    // that finds no flag returns at once).
+    double* partials = reinterpret_cast<double*>(reinterpret_cast<char*>(scratch) + rowspec_bytes(p, NA, a.nslices));
+    GatherOut none{};
+    none.slice_stride = a.out_stride;
+    rc = launch_banded_nonfinite(p, MODE, NF, a.planes, a.pitch, static_cast<int>(a.slice_stride / a.plane_stride),
+                                 a.nslices, a.mask, a.mask_stride, partials, none, st, scratch);
+  }
+  if (rc == CGEF_OK) {
     rs_finish_kernel<MODE, NF, DEF><<<dim3((p->nx + 127) / 128, p->ny, a.nslices), 128, 0, st>>>(a, scratch);
     rc = rs_check("rs_finish_kernel");
   }

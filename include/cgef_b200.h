@@ -44,7 +44,8 @@ enum {
   CGEF_ECUDA = -3,        /* a CUDA runtime call failed */
   CGEF_ESTRATEGY = -4,    /* plan built for another mask strategy (Filtering.jl:952-965, 1484-1503) */
   CGEF_EUNSUPPORTED = -5, /* combination outside the supported path */
-  CGEF_ENODEVICE = -6     /* no CUDA device visible */
+  CGEF_ENODEVICE = -6,    /* no CUDA device visible */
+  CGEF_ETIMEOUT = -7      /* a bounded device-side wait ran out (the call's results are not valid) */
 };
 
 /* Geometry (FlowGeometries.Geometry.CartesianGeometry / SphericalGeometry). */
@@ -112,6 +113,10 @@ const char* cgef_last_error(void);
 /* Number of visible CUDA devices (0 when none; never fails). */
 int32_t cgef_device_count(void);
 
+/* The device architecture the library's kernels are compiled for, in __CUDA_ARCH__ form: 1000 for
+ * sm_100a (the build refuses any other target).  No device needed. */
+int32_t cgef_build_arch(void);
+
 /* Filtering.plan_filter (Filtering.jl:2931-2954) plus the GPU extension's prepare_workspace
  * upload (Filtering.jl:2910-2912; ext/CoarseGrainingEnergyFluxesKernelAbstractionsExt.jl:474-571):
  * builds the engine's tables on the host once and keeps them resident on the current device.
@@ -121,6 +126,13 @@ int32_t cgef_plan_create(cgef_plan** out, const cgef_grid_desc* grid, int32_t ke
 
 /* Releases the plan's device and host memory. */
 int32_t cgef_plan_destroy(cgef_plan* plan);
+
+/* Zeroes the work queue of the plan's direct gather, synchronously (no counterpart in the reference,
+ * whose loops have no queue).  Each gather launch takes its work items from this queue and the last
+ * warp to leave zeroes it; a launch that stopped part-way would leave it mid-count, so every launch
+ * also zeroes it first (stream-ordered) and a stale queue never reaches a later launch.  This call is
+ * for a host that wants the queue clean at once. */
+int32_t cgef_plan_reset_queue(cgef_plan* plan);
 
 /* Plan statistics. */
 int32_t cgef_plan_get_info(const cgef_plan* plan, cgef_plan_info* info);
@@ -248,10 +260,11 @@ int32_t cgef_pipeline_destroy(cgef_pipeline* pipeline);
  * cudaMalloc would bypass and which can leave no memory for it), or a loop with a fixed memory
  * budget.  The scratch is one 64 MiB array compiled into the library, which every GPU that loads
  * the library holds until the process exits; a grid and batch needing more is rejected with
- * CGEF_EINVAL.  The first call on each device resolves the array's device address (with that
- * device current); make that first call before any stream capture.  All calls share the array and
- * it keeps the last call's contents, so calls that overlap on the GPU race: serialise them.
- * Same arguments and results as cgef_filter_device. */
+ * CGEF_EINVAL.  The CUDA driver reserves the array on a device, and the library resolves its device
+ * address there, when the first plan is created on that device (cgef_plan_create, with that device
+ * current), so a call of this entry point never makes the driver reserve memory; create plans before
+ * any stream capture.  All calls share the array and it keeps the last call's contents, so calls that
+ * overlap on the GPU race: serialise them.  Same arguments and results as cgef_filter_device. */
 int32_t cgef_filter_device_noalloc(cgef_plan* plan, int32_t dtype, const void* field, void* out, int64_t nbatch,
                                    void* stream);
 
@@ -353,6 +366,15 @@ int32_t cgef_closure_grad_device(cgef_closure* c, const float* x, const float* t
 int32_t cgef_closure_pi_device(cgef_closure* c, cgef_plan* plan, int32_t dtype, const void* u, const void* v,
                                int64_t nbatch, const uint8_t* slice_masks, double judge_fraction,
                                uint64_t judge_seed, double tol, void* pi, cgef_closure_report* report, void* stream);
+
+/* Failure injection for the tests of the failure paths (no counterpart in the reference).  Host side
+ * only: it writes one device word with a synchronous copy and never makes a kernel fault or wait.
+ * CGEF_INJECT_CLOSURE_TIMEOUT: `object` is a cgef_closure*; its device error word is set as a bounded
+ * tensor-core wait that ran out sets it, so its next call returns CGEF_ETIMEOUT (and clears it).
+ * CGEF_INJECT_STALE_QUEUE: `object` is a cgef_plan*; its direct gather's work queue is left as a launch
+ * that stopped part-way would leave it. */
+enum { CGEF_INJECT_CLOSURE_TIMEOUT = 1, CGEF_INJECT_STALE_QUEUE = 2 };
+int32_t cgef_debug_inject(void* object, int32_t what);
 
 /* Tracing (no counterpart in the reference, which has none).  Kernel launches made by this
  * thread's calls since the last reset. */

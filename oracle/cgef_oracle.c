@@ -120,8 +120,10 @@ static int sphere_row_window(const orc_grid* g, double phi1, double phi2, double
   return (int)w;
 }
 
+/* rows: NULL, or ny flags; bands of unflagged rows are left empty (the row-subset oracle, which
+ * evaluates only the target rows a test compares). */
 static void footprint_build(const orc_grid* g, int kernel, double alpha, double ell, orc_footprint* fp,
-                            int fill) {
+                            int fill, const uint8_t* rows) {
   double rad = orc_kernel_radius(kernel, alpha, ell);
   int64_t n = 0;
   if (g->geometry == ORC_CART) {
@@ -154,6 +156,10 @@ static void footprint_build(const orc_grid* g, int kernel, double alpha, double 
   int half = nx / 2;
   if (fill) fp->ptr[0] = 0;
   for (int j = 0; j < ny; ++j) {
+    if (rows && !rows[j]) {
+      if (fill) fp->ptr[j + 1] = n;
+      continue;
+    }
     double phi = gy_coord(g, j);
     /* The band's window: capped at one turn (Filtering.jl:692), and asymmetric by one when it
      * closes the ring (Filtering.jl:711-713).  The band closes the ring when some row it
@@ -234,21 +240,34 @@ static void footprint_apply_row(const orc_grid* g, const orc_footprint* fp, int 
   }
 }
 
+/* rows: NULL, or ny flags; unflagged rows are not evaluated and read 0. */
 static void footprint_apply(const orc_grid* g, const orc_footprint* fp, int strategy, int K,
-                            const double* const* fields, double* const* outs, int nthreads) {
+                            const double* const* fields, double* const* outs, int nthreads, const uint8_t* rows) {
 #ifdef _OPENMP
   if (nthreads <= 0) nthreads = omp_get_max_threads();
 #pragma omp parallel num_threads(nthreads)
   {
     double* acc = (double*)malloc(sizeof(double) * 2 * (K > 0 ? K : 1));
 #pragma omp for schedule(dynamic, 1)
-    for (int j = 0; j < g->ny; ++j) footprint_apply_row(g, fp, strategy, K, fields, outs, j, acc, acc + K);
+    for (int j = 0; j < g->ny; ++j) {
+      if (rows && !rows[j]) {
+        for (int m = 0; m < K; ++m) memset(outs[m] + (int64_t)j * g->nx, 0, sizeof(double) * g->nx);
+        continue;
+      }
+      footprint_apply_row(g, fp, strategy, K, fields, outs, j, acc, acc + K);
+    }
     free(acc);
   }
 #else
   (void)nthreads;
   double* acc = (double*)malloc(sizeof(double) * 2 * (K > 0 ? K : 1));
-  for (int j = 0; j < g->ny; ++j) footprint_apply_row(g, fp, strategy, K, fields, outs, j, acc, acc + K);
+  for (int j = 0; j < g->ny; ++j) {
+    if (rows && !rows[j]) {
+      for (int m = 0; m < K; ++m) memset(outs[m] + (int64_t)j * g->nx, 0, sizeof(double) * g->nx);
+      continue;
+    }
+    footprint_apply_row(g, fp, strategy, K, fields, outs, j, acc, acc + K);
+  }
   free(acc);
 #endif
 }
@@ -543,6 +562,7 @@ typedef struct {
   orc_separable sp;
   orc_prefix pp;
   uint8_t* mask_copy;
+  uint8_t* rows; /* banded: NULL, or ny flags of the target rows evaluated (orc_plan_new_rows) */
 } orc_plan;
 
 int orc_default_engine(int geometry, int kernel) {
@@ -551,10 +571,19 @@ int orc_default_engine(int geometry, int kernel) {
   return ORC_ENGINE_BANDED;
 }
 
-orc_plan* orc_plan_new(int geometry, int nx, int ny, double x0, double dx, double y0, double dy, double R,
-                       int periodic_x, int periodic_y, const uint8_t* mask, int kernel, double alpha,
-                       double ell, int strategy, int engine) {
+/* rows: NULL (every target row), or ny flags: a banded plan then builds and evaluates only the
+ * flagged target rows' bands, and every other row of a filter output reads 0.  compute_Pi!'s
+ * strain at row j reads the filtered velocities of rows j-2..j+2, so its Pi is the full plan's
+ * wherever those five rows are flagged.  This keeps footprints of thousands of kilometres on the
+ * full 0.25-degree sphere within seconds of CPU time for the rows a test compares. */
+orc_plan* orc_plan_new_rows(int geometry, int nx, int ny, double x0, double dx, double y0, double dy, double R,
+                            int periodic_x, int periodic_y, const uint8_t* mask, int kernel, double alpha,
+                            double ell, int strategy, int engine, const uint8_t* rows) {
   orc_plan* p = (orc_plan*)calloc(1, sizeof(orc_plan));
+  if (rows) {
+    p->rows = (uint8_t*)malloc((size_t)ny);
+    memcpy(p->rows, rows, (size_t)ny);
+  }
   p->g.geometry = geometry;
   p->g.nx = nx;
   p->g.ny = ny;
@@ -576,12 +605,12 @@ orc_plan* orc_plan_new(int geometry, int nx, int ny, double x0, double dx, doubl
   p->strategy = strategy;
   p->engine = engine > 0 ? engine : orc_default_engine(geometry, kernel);
   if (p->engine == ORC_ENGINE_BANDED) {
-    footprint_build(&p->g, kernel, alpha, ell, &p->fp, 0);
+    footprint_build(&p->g, kernel, alpha, ell, &p->fp, 0, p->rows);
     p->fp.di = (int*)malloc(sizeof(int) * (p->fp.nentries + 1));
     p->fp.dj = (int*)malloc(sizeof(int) * (p->fp.nentries + 1));
     p->fp.w = (double*)malloc(sizeof(double) * (p->fp.nentries + 1));
     p->fp.ptr = (int64_t*)malloc(sizeof(int64_t) * (p->fp.nbands + 1));
-    footprint_build(&p->g, kernel, alpha, ell, &p->fp, 1);
+    footprint_build(&p->g, kernel, alpha, ell, &p->fp, 1, p->rows);
   } else if (p->engine == ORC_ENGINE_SEPARABLE) {
     separable_build(&p->g, alpha, ell, strategy, &p->sp);
   } else {
@@ -590,8 +619,16 @@ orc_plan* orc_plan_new(int geometry, int nx, int ny, double x0, double dx, doubl
   return p;
 }
 
+orc_plan* orc_plan_new(int geometry, int nx, int ny, double x0, double dx, double y0, double dy, double R,
+                       int periodic_x, int periodic_y, const uint8_t* mask, int kernel, double alpha,
+                       double ell, int strategy, int engine) {
+  return orc_plan_new_rows(geometry, nx, ny, x0, dx, y0, dy, R, periodic_x, periodic_y, mask, kernel, alpha, ell,
+                           strategy, engine, NULL);
+}
+
 void orc_plan_free(orc_plan* p) {
   if (!p) return;
+  free(p->rows);
   free(p->fp.di);
   free(p->fp.dj);
   free(p->fp.w);
@@ -629,7 +666,7 @@ void orc_plan_separable_lims(const orc_plan* p, int* lims) {
 /* filter_apply_batch! (Filtering.jl:3360-3375): K fields through one plan. */
 void orc_filter_batch(const orc_plan* p, int K, const double* const* fields, double* const* outs, int nthreads) {
   if (p->engine == ORC_ENGINE_BANDED) {
-    footprint_apply(&p->g, &p->fp, p->strategy, K, fields, outs, nthreads);
+    footprint_apply(&p->g, &p->fp, p->strategy, K, fields, outs, nthreads, p->rows);
   } else if (p->engine == ORC_ENGINE_SEPARABLE) {
     for (int m = 0; m < K; ++m) separable_apply(&p->g, &p->sp, fields[m], outs[m]);
   } else {
@@ -955,7 +992,7 @@ int64_t orc_count_entries(int geometry, int nx, int ny, double x0, double dx, do
   orc_grid g = {geometry, nx, ny, x0, dx, y0, dy, R, periodic_x, periodic_y, NULL};
   if (geometry == ORC_CART) {
     orc_footprint fp;
-    footprint_build(&g, kernel, alpha, ell, &fp, 0);
+    footprint_build(&g, kernel, alpha, ell, &fp, 0, NULL);
     return fp.nentries;
   }
   double rad = orc_kernel_radius(kernel, alpha, ell);

@@ -46,6 +46,8 @@ def lib():
         L.orc_plan_new.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                    C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_double,
                                    C.c_int, C.c_int]
+        L.orc_plan_new_rows.restype = C.c_void_p
+        L.orc_plan_new_rows.argtypes = L.orc_plan_new.argtypes + [C.c_void_p]
         L.orc_plan_free.argtypes = [C.c_void_p]
         L.orc_plan_engine.argtypes = [C.c_void_p]
         L.orc_plan_nentries.argtypes = [C.c_void_p]
@@ -115,15 +117,24 @@ class Grid:
 
 
 class Plan:
-    """One oracle filter plan (engine chosen as the reference dispatches, unless forced)."""
+    """One oracle filter plan (engine chosen as the reference dispatches, unless forced).
+
+    `rows` (banded engine): None, or the target rows to evaluate; every other row of a filter output
+    reads 0 and only those rows' footprint bands are built.  Use `rows_for_pi` to widen the rows a
+    test compares by the strain stencil's reach, so Pi at those rows equals the full plan's.
+    """
 
     def __init__(self, grid: Grid, kernel: int, alpha: float, ell: float, strategy: int = ZEROFILL,
-                 engine: int = ENGINE_AUTO):
+                 engine: int = ENGINE_AUTO, rows: Optional[Sequence[int]] = None):
         self.grid = grid
         self._mask = grid.mask_u8()
-        self.h = lib().orc_plan_new(grid.geometry, grid.nx, grid.ny, grid.x0, grid.dx, grid.y0, grid.dy, grid.R,
-                                    int(grid.periodic_x), int(grid.periodic_y), _ptr(self._mask), kernel, alpha,
-                                    ell, strategy, engine)
+        self._rows = None
+        if rows is not None:
+            self._rows = np.zeros(grid.ny, np.uint8)
+            self._rows[np.asarray(rows, dtype=np.int64)] = 1
+        self.h = lib().orc_plan_new_rows(grid.geometry, grid.nx, grid.ny, grid.x0, grid.dx, grid.y0, grid.dy,
+                                         grid.R, int(grid.periodic_x), int(grid.periodic_y), _ptr(self._mask),
+                                         kernel, alpha, ell, strategy, engine, _ptr(self._rows))
         self.kernel, self.alpha, self.ell, self.strategy = kernel, alpha, ell, strategy
 
     def __del__(self):
@@ -192,6 +203,20 @@ class Plan:
 
     def cumulative_energy_one(self, u: np.ndarray, v: np.ndarray, nthreads: int = 1) -> float:
         return lib().orc_cumulative_energy_one(self.h, _ptr(_f64(u)), _ptr(_f64(v)), nthreads)
+
+
+def rows_for_pi(rows: Sequence[int], ny: int, periodic_y: bool = False) -> np.ndarray:
+    """The rows a row-subset plan must evaluate for compute_pi's Pi to be exact at `rows`: the
+    3-node ReduceInRun stencil along y reads up to two rows either side."""
+    out = set()
+    for j in rows:
+        for d in range(-2, 3):
+            jj = j + d
+            if periodic_y:
+                out.add(jj % ny)
+            elif 0 <= jj < ny:
+                out.add(jj)
+    return np.array(sorted(out), dtype=np.int64)
 
 
 def kernel_radius(kernel: int, alpha: float, ell: float) -> float:

@@ -34,11 +34,15 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_library_is_built_for_sm100a():
-    import subprocess
-    out = subprocess.run(["cuobjdump", "--list-elf", _lib.library_path()], capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in out.stdout
+    # every .cu file refuses to compile device code for any target but sm_100a (cgef_internal.h)
+    assert _lib.load().cgef_build_arch() == 1000
+
+
+def test_failure_entry_points_refuse_null_objects():
+    L = _lib.load()
+    assert L.cgef_plan_reset_queue(None) == _lib.CGEF_EINVAL
+    assert L.cgef_debug_inject(None, _lib.INJECT_STALE_QUEUE) == _lib.CGEF_EINVAL
+    assert L.cgef_debug_inject(None, _lib.INJECT_CLOSURE_TIMEOUT) == _lib.CGEF_EINVAL
 
 
 @pytest.mark.parametrize("scale,alpha", [(1e5, 4.0), (3e5, 6.0), (1.2e6, 4.0)])
