@@ -14,8 +14,10 @@ Gaussian alpha = 4, l = 100 km, ZeroFill, ~30% land -- one scale x one snapshot 
 
 `value` times the device-resident path (inputs already in HBM, an L2 flush between steps inside
 the timed region); `e2e` times the host C-ABI call (pinned host inputs copied in, Pi copied out)
-every step.  `--impl reference` times the CPU FP64 oracle -- the restated threaded reference path
--- on the host's cores instead.
+every step.  The default run (sphere1, one rank) adds two sub-records to its line, the metric's
+"plain vs batched/closure": `batched` (the sweep24x8 workload, measured the same way) and `closure`
+(the closure8 workload).  `--impl reference` times the CPU FP64 oracle -- the restated threaded
+reference path -- on the host's cores instead, with the same `config`.
 """
 from __future__ import annotations
 
@@ -55,6 +57,12 @@ def parse():
     ap.add_argument("--evaluation", choices=("auto", "direct", "spectral"), default="auto",
                     help="footprint sums of the banded engine: the autotuner's choice per scale (default), the "
                          "direct gather, or the row-spectral evaluation")
+    ap.add_argument("--no-subrecords", action="store_true",
+                    help="sphere1: time the headline only, without the batched (24 scales x 8 snapshots) and "
+                         "closure sub-records")
+    ap.add_argument("--batched-steps", type=int, default=6, help="timed steps of the batched sub-record")
+    ap.add_argument("--clocks-out", default=None,
+                    help="directory for the nvidia-smi clock samples (default: a temporary directory)")
     return ap.parse_args()
 
 
@@ -195,8 +203,10 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+    def __init__(self, device_index: int, out_dir=None):
+        import tempfile
+        d = out_dir if out_dir else tempfile.mkdtemp(prefix="cgef_clocks_")
+        self.path = os.path.join(d, f"clocks_rank{device_index}.csv")
         self.proc = None
         self.dev = device_index
 
@@ -353,8 +363,9 @@ def mlp_flops_per_point() -> float:
     return 2.0 * (5 * 64 + 64 * 64 + 64 * 64 + 64 * 3)
 
 
-def run_closure(args, rank, world, local, dist):
-    """closure8: train the closure on exact pairs, then time closure vs plain Pi at 8 scales."""
+def run_closure(args, rank, world, local, dist, steps=None, with_cpu=True):
+    """closure8: train the closure on exact pairs, then time closure vs plain Pi at 8 scales.  Returns the
+    record (value, ms_per_step, roofline, e2e, cpu_baseline, clocks, the closure's accuracy terms)."""
     import ctypes as C
 
     import torch
@@ -470,8 +481,8 @@ def run_closure(args, rank, world, local, dist):
             L.cgef_profile_enable(1)
         return device_steps_ms(lambda k: fn(k + 100), steps, stream, flush)
 
-    steps = args.steps or 3
-    sampler = ClockSampler(local)
+    steps = steps or args.steps or 3
+    sampler = ClockSampler(local, args.clocks_out)
     sampler.start()
     time.sleep(0.3)
     ms_open = timed(lambda k: closure_step(k, tol=float("inf")), steps)
@@ -495,28 +506,15 @@ def run_closure(args, rank, world, local, dist):
     # roofline of the dominant kernel (the 3-field FP64 velocity gather) and of the tensor-core MLP
     act = g.mask.sum(axis=1).astype(np.float64)
     vel_flops = sum(float((act * p.band_counts()).sum()) * 3 * 2 for p in plans)
-    peak = None
-    try:
-        pk = C.CDLL(os.path.join(ROOT, "coarsegrainingenergyfluxes.jl_b200", "cgef_b200", "libcgef_peak.so"))
-        pk.cgef_peak_fp64_tflops.restype = C.c_double
-        pk.cgef_peak_fp64_tflops.argtypes = [C.c_int]
-        peak = float(pk.cgef_peak_fp64_tflops(local))
-    except Exception:
-        peak = None
+    peak = fp64_peak(local)
     bt, bc = prof["banded"]
     rt, rc_ = prof["rowspec"]
     mt, mc = prof["closure_mlp"]
     mlp_ach = N * ns * mlp_flops_per_point() * steps / (mt * 1e-3) / 1e12 if mt > 0 else None
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        peaks = {}
-    bf16 = peaks.get("bf16_tflops")
+    bf16, bf16_source = bf16_peak()
     mlp_line = {"bound": "tensor", "achieved": mlp_ach, "peak": bf16, "unit": "TFLOP/s",
                 "frac": (mlp_ach / bf16) if (mlp_ach and bf16) else None,
-                "per_step_ms": mt / steps, "flops_per_point": mlp_flops_per_point(),
-                "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)"}
+                "per_step_ms": mt / steps, "flops_per_point": mlp_flops_per_point(), "peak_source": bf16_source}
     if rt > bt:
         # the 3-field velocity filter runs through the row-spectral evaluation
         hbm, hbm_source = hbm_peak()
@@ -549,46 +547,38 @@ def run_closure(args, rank, world, local, dist):
         torch.cuda.synchronize()
 
     e2e_step(0)
+    if dist is not None:
+        dist.barrier()
     t0 = time.perf_counter()
     for k in range(steps):
         e2e_step(k + 1)
     el = time.perf_counter() - t0
+    el = max_over_ranks(el, dist)
     e2e = {"value": world * units * steps / el, "unit": UNIT, "h2d_bytes_per_step": 2 * N * 8,
            "d2h_bytes_per_step": ns * N * 8, "steps": steps,
            "timing": "wall clock: pinned H2D of u, v, the closure at 8 scales, D2H of Pi"}
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and with_cpu and not args.no_cpu_baseline:
         rate, nth, done, el, sample, _ = oracle_rate(wl, budget_s=20.0)
         cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
                "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path (plain Pi, FP64 oracle)"}
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return 0
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": ms_closure / steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 flux, bf16 closure (fp32 accumulate)", "data": "synthetic (seeded)",
-            "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": 1,
-                       "judge_fraction": 0.02, "tol": args.closure_tol, "schedule_split_waves": waves,
-                       "l2": "flushed between steps (a 256 MiB write before every step, outside the step's own events)",
-                       "parallelism": f"{world} rank(s), independent snapshots per rank"},
-            "closure": {"plain_value": plain_value, "plain_ms_per_step": ms_plain / steps,
-                        "speedup_vs_plain": value / plain_value, "fallback_slices_per_step": fallbacks,
-                        "no_fallback_value": world * units * steps / (ms_open / 1e3),
-                        "no_fallback_ms_per_step": ms_open / steps,
-                        "no_fallback_speedup_vs_plain": (world * units * steps / (ms_open / 1e3)) / plain_value,
-                        "no_fallback_est_rel_l2": [r.est_rel_l2 for r in reports_open],
-                        "pi_rel_l2_raw": raw_err, "pi_rel_l2_judged": judged_err,
-                        "gradient_model_pi_rel_l2": ngm_err, "gradient_model_fitted_pi_rel_l2": ngm_fit_err,
-                        "est_rel_l2_judge": [r.est_rel_l2 for r in reports],
-                        "scales_km": [s / 1e3 for s in scales],
-                        "training": {"points": 10_000_000, "batch": batch, "steps": int(nsteps),
-                                     "seconds": train_s, "pairs_seconds": pairs_s,
-                                     "loss_first": float(losses[:10].mean()), "loss_last": float(losses[-50:].mean())}},
+    return {"value": value, "unit": UNIT, "steps": steps, "ms_per_step": ms_closure / steps,
+            "dtype": "f64 flux, bf16 closure (fp32 accumulate)", "config": workload_config(wl),
+            "run": {"judge_fraction": 0.02, "tol": args.closure_tol, "schedule_split_waves": waves,
+                    "parallelism": f"{world} rank(s), independent snapshots per rank"},
+            "plain_value": plain_value, "plain_ms_per_step": ms_plain / steps,
+            "speedup_vs_plain": value / plain_value, "fallback_slices_per_step": fallbacks,
+            "no_fallback_value": world * units * steps / (ms_open / 1e3),
+            "no_fallback_ms_per_step": ms_open / steps,
+            "no_fallback_speedup_vs_plain": (world * units * steps / (ms_open / 1e3)) / plain_value,
+            "no_fallback_est_rel_l2": [r.est_rel_l2 for r in reports_open],
+            "pi_rel_l2_raw": raw_err, "pi_rel_l2_judged": judged_err,
+            "gradient_model_pi_rel_l2": ngm_err, "gradient_model_fitted_pi_rel_l2": ngm_fit_err,
+            "est_rel_l2_judge": [r.est_rel_l2 for r in reports], "scales_km": [s / 1e3 for s in scales],
+            "training": {"points": 10_000_000, "batch": batch, "steps": int(nsteps), "seconds": train_s,
+                         "pairs_seconds": pairs_s, "loss_first": float(losses[:10].mean()),
+                         "loss_last": float(losses[-50:].mean())},
             "gpu_launches": launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks}
-    print(json.dumps(line))
-    return 0
 
 
 def cpu_model() -> str:
@@ -601,58 +591,87 @@ def cpu_model() -> str:
     return "unknown"
 
 
-# ---------------------------------------------------------------------------------------------
-def main():
-    args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+def fp64_peak(local: int):
+    """The FP64 FMA peak measured in this run by libcgef_peak.so (a DFMA loop over all SMs)."""
+    import ctypes as C
+    try:
+        pk = C.CDLL(os.path.join(ROOT, "coarsegrainingenergyfluxes.jl_b200", "cgef_b200", "libcgef_peak.so"))
+        pk.cgef_peak_fp64_tflops.restype = C.c_double
+        pk.cgef_peak_fp64_tflops.argtypes = [C.c_int]
+        return float(pk.cgef_peak_fp64_tflops(local))
+    except Exception:
+        return None
 
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        wl = make_workload(args.workload, 0, args.snapshots, args.scale_km)
-        rate, nth, done, el, sample, _ = oracle_rate(wl, budget_s=120.0)
-        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded)", "config": {"workload": wl["desc"], "nx": wl["grid"].nx,
-                                                          "ny": wl["grid"].ny, "scales": len(wl["scales"]),
-                                                          "snapshots": int(wl["u"].shape[0])},
-                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
-                                 "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path"},
-                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
-        return 0
+
+def bf16_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]), \
+            "measured: MEASURED_PEAKS.json bf16_tflops (cuBLAS burst on this pool's B200s)"
+    except Exception:
+        return 1590.0, "fallback 1.59 PFLOP/s (earlier cuBLAS bf16 burst measurement on this pool)"
+
+
+def max_over_ranks(x: float, dist) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+L2_NOTE = ("GPU arm: a 256 MiB write flushes L2 before every timed step, outside the step's own CUDA events; "
+           "CPU arm (the oracle on the host cores): no flush")
+
+
+def workload_config(wl) -> dict:
+    """The workload, in the same words from both arms (the GPU's and --impl reference)."""
+    g = wl["grid"]
+    if wl["slice_masks"] is not None:
+        act = float(np.mean(wl["slice_masks"]))
+    else:
+        act = float(1.0 if g.mask is None else np.mean(g.mask))
+    return {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": len(wl["scales"]),
+            "snapshots": int(wl["u"].shape[0]), "active_fraction": act, "storage": wl["dtype"], "l2": L2_NOTE}
+
+
+def compulsory_bytes(g, nsl: int, ns: int, bsz: int, slice_masks) -> float:
+    """Bytes a step must move at least: u, v (and the masks) read once, Pi and E written once."""
+    N = g.nx * g.ny
+    masks = nsl * N if slice_masks is not None else (N if g.mask is not None else 0)
+    return float(2 * nsl * N * bsz + masks + nsl * ns * N * bsz + nsl * ns * 8)
+
+
+def measure_sweep(args, name, rank, world, local, dist, *, snapshots=1, scale_km=None, steps=None, e2e_steps=None,
+                  with_cpu=True, cpu_budget=20.0):
+    """Times one sweep workload (Pi and E(l) of every slice at every scale): the step replayed from its
+    CUDA graph (the value), launched call by call (eager; its per-kernel events feed the roofline), and
+    end to end through the host C ABI; plus the CPU baseline and the accuracy against the FP64 oracle
+    (rank 0 of one rank).  Returns the record."""
+    import ctypes as C
 
     import torch
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
     import cgef_b200 as cg
     from cgef_b200 import _lib
 
-    if args.workload == "closure8":
-        return run_closure(args, rank, world, local, dist)
-    wl = make_workload(args.workload, rank, args.snapshots, args.scale_km)
+    L = _lib.load()
+    wl = make_workload(name, rank, snapshots, scale_km)
     g = wl["grid"]
     nsl = int(wl["u"].shape[0])
     ns = len(wl["scales"])
+    t0 = time.perf_counter()
     plans = [cg.plan_filter(g.with_mask(None) if wl["slice_masks"] is not None else g, wl["kernel"], s)
              for s in wl["scales"]]
     # schedule autotuning is plan setup, like building the footprint: outside the timed region
     waves = [p.autotune(nsl) if not args.no_autotune else 4.0 for p in plans]
     apply_evaluation(plans, args.evaluation)
-    L = _lib.load()
+    setup_s = time.perf_counter() - t0
     tdt = torch.float32 if wl["dtype"] == "f32" else torch.float64
     du = torch.from_numpy(np.ascontiguousarray(wl["u"])).to(device="cuda", dtype=tdt)
     dv = torch.from_numpy(np.ascontiguousarray(wl["v"])).to(device="cuda", dtype=tdt)
     dm = None if wl["slice_masks"] is None else torch.from_numpy(wl["slice_masks"].astype(np.uint8)).cuda()
     dt_code = _lib.F32 if tdt == torch.float32 else _lib.F64
-    import ctypes as C
     parr = (C.c_void_p * ns)(*[p.handle.value for p in plans])
     dPi = torch.empty((nsl, ns) + g.shape, dtype=tdt, device="cuda")
     dE = torch.empty((nsl, ns), dtype=torch.float64, device="cuda")
@@ -664,23 +683,22 @@ def main():
                                        stream.cuda_stream))
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    steps = args.steps
     if steps is None:
-        # about 5 s of timed work
+        # about 5 s of timed work (every rank takes the slowest rank's count)
         step()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(3):
             step()
         torch.cuda.synchronize()
-        per = (time.perf_counter() - t0) / 3
+        per = max_over_ranks((time.perf_counter() - t0) / 3, dist)
         steps = int(max(3, min(5000, 5.0 / max(per, 1e-6))))
     for _ in range(max(args.warmup, 3)):
         flush.fill_(1.0)
         step()
     torch.cuda.synchronize()
 
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(local, args.clocks_out)
     sampler.start()
     time.sleep(0.3)
     L.cgef_reset_launch_count()
@@ -714,17 +732,11 @@ def main():
         graph_ms = device_steps_ms(lambda k: _lib.check(L.cgef_graph_launch(gh, gs.cuda_stream)), steps, gs, flush)
     graph_launches = int(L.cgef_launch_count())
     _lib.check(L.cgef_graph_destroy(gh))
-    if dist is not None:
-        t = torch.tensor([graph_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        graph_ms = float(t.item())
+    graph_ms = max_over_ranks(graph_ms, dist)
     clocks = sampler.stop()
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, dist)
     units_per_step = g.nx * g.ny * ns * nsl
-    # the headline is the step replayed from the CUDA graph it was captured into once (the library's
+    # the value is the step replayed from the CUDA graph it was captured into once (the library's
     # API for repeated sweeps, cgef_sweep_graph_create / cgef_graph_launch); the same step launched call
     # by call, whose per-kernel events feed the roofline, is reported beside it as "eager"
     value = world * units_per_step * steps / (graph_ms / 1e3)
@@ -736,10 +748,10 @@ def main():
     # sums of the direct gather or of the row-spectral evaluation, whichever took longer
     kinds = {"banded": _lib.KERNEL_BANDED, "separable": _lib.KERNEL_SEPARABLE, "prefixsum": _lib.KERNEL_PREFIX}
     prof = {}
-    for name, kind in (("direct", kinds[plans[0].engine]), ("rowspec", _lib.KERNEL_ROWSPEC)):
+    for pname, kind in (("direct", kinds[plans[0].engine]), ("rowspec", _lib.KERNEL_ROWSPEC)):
         tot, cnt = C.c_double(), C.c_int64()
         _lib.check(L.cgef_profile_read(kind, C.byref(tot), C.byref(cnt)))
-        prof[name] = (tot.value, int(cnt.value))
+        prof[pname] = (tot.value, int(cnt.value))
     spec_plans = [p for p in plans if uses_row_spectral(p)]
     direct_plans = [p for p in plans if not uses_row_spectral(p)]
     flops_all = algorithmic_flops(plans, g, nsl, wl["slice_masks"])
@@ -762,7 +774,7 @@ def main():
         bytes_launch = bytes_step / launches_per_step
         peak, peak_source = hbm_peak()
         achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
-        traffic, traffic_basis, traffic_one = committed_traffic(f"{args.workload}:rowspec", nsl, args.scale_km)
+        traffic, traffic_basis, traffic_one = committed_traffic(f"{name}:rowspec", nsl, scale_km)
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": traffic, "traffic_basis": traffic_basis, "traffic_one_snapshot": traffic_one,
                     "kernel": "rs_forward_kernel + rs_accumulate_kernel + rs_inverse_kernel + rs_finish_kernel "
@@ -777,17 +789,9 @@ def main():
         flops_step = algorithmic_flops(direct_plans, g, nsl, wl["slice_masks"])
         launches_per_step = max(cnt // steps, 1)
         flops_launch = flops_step / launches_per_step
-        peak = None
-        try:
-            pk = C.CDLL(os.path.join(ROOT, "coarsegrainingenergyfluxes.jl_b200", "cgef_b200", "libcgef_peak.so"))
-            pk.cgef_peak_fp64_tflops.restype = C.c_double
-            pk.cgef_peak_fp64_tflops.argtypes = [C.c_int]
-            peak = float(pk.cgef_peak_fp64_tflops(local))
-        except Exception:
-            peak = None
+        peak = fp64_peak(local)
         achieved = flops_launch / (per_launch_ms * 1e-3) / 1e12
-        traffic, traffic_basis, traffic_one = committed_traffic(f"{args.workload}:{plans[0].engine}", nsl,
-                                                                args.scale_km)
+        traffic, traffic_basis, traffic_one = committed_traffic(f"{name}:{plans[0].engine}", nsl, scale_km)
         roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": (achieved / peak) if peak and peak > 0 else None, "traffic": traffic,
                     "traffic_basis": traffic_basis, "traffic_one_snapshot": traffic_one,
@@ -798,78 +802,78 @@ def main():
                     "algorithmic_flops_per_launch": flops_launch, "row_spectral_launches": prof["rowspec"][1],
                     "peak_source": "measured: DFMA loop over all SMs on this GPU (libcgef_peak.so), "
                                    "nominal B200 FP64 37 TFLOP/s; MEASURED_PEAKS.json holds no FP64 figure"}
+    # second term: the step's compulsory bytes (inputs read once, outputs written once) over the whole
+    # step, against HBM -- how far the step is from the problem's own I/O bound
+    bsz = 4 if tdt == torch.float32 else 8
+    comp = compulsory_bytes(g, nsl, ns, bsz, wl["slice_masks"])
+    hbm, hbm_source = hbm_peak()
+    comp_ach = comp / (graph_ms / steps * 1e-3) / 1e9
+    roofline["compulsory"] = {"bound": "hbm", "bytes_per_step": comp, "achieved": comp_ach, "peak": hbm,
+                              "unit": "GB/s", "frac": comp_ach / hbm, "peak_source": hbm_source,
+                              "what": "u, v (and masks) read once, Pi and E written once, over the whole step "
+                                      "(graph replay) -- the problem's own I/O"}
 
     # end to end through the host C ABI: pinned inputs in, Pi (and E) out, every step
-    e2e = None
-    if True:  # every rank, so the barriers pair up
-        hu = torch.from_numpy(np.ascontiguousarray(wl["u"])).to(dtype=tdt).pin_memory()
-        hv = torch.from_numpy(np.ascontiguousarray(wl["v"])).to(dtype=tdt).pin_memory()
-        hPi = torch.empty((nsl, ns) + g.shape, dtype=tdt).pin_memory()
-        hE = torch.empty((nsl, ns), dtype=torch.float64).pin_memory()
-        hm = None if wl["slice_masks"] is None else torch.from_numpy(wl["slice_masks"].astype(np.uint8)).pin_memory()
+    hu = torch.from_numpy(np.ascontiguousarray(wl["u"])).to(dtype=tdt).pin_memory()
+    hv = torch.from_numpy(np.ascontiguousarray(wl["v"])).to(dtype=tdt).pin_memory()
+    hPi = torch.empty((nsl, ns) + g.shape, dtype=tdt).pin_memory()
+    hE = torch.empty((nsl, ns), dtype=torch.float64).pin_memory()
+    hm = None if wl["slice_masks"] is None else torch.from_numpy(wl["slice_masks"].astype(np.uint8)).pin_memory()
 
-        def host_step():
-            _lib.check(L.cgef_sweep(parr, ns, dt_code, hu.data_ptr(), hv.data_ptr(), nsl,
-                                    None if hm is None else hm.data_ptr(), hPi.data_ptr(), hE.data_ptr()))
+    def host_step():
+        _lib.check(L.cgef_sweep(parr, ns, dt_code, hu.data_ptr(), hv.data_ptr(), nsl,
+                                None if hm is None else hm.data_ptr(), hPi.data_ptr(), hE.data_ptr()))
 
+    host_step()
+    per_step_s = elapsed_ms / 1e3 / steps
+    n_e2e = e2e_steps if e2e_steps is not None else (
+        args.e2e_steps if args.e2e_steps is not None else max(2, min(steps, 200, int(4.0 / per_step_s))))
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
         host_step()
-        per_step_s = elapsed_ms / 1e3 / steps
-        n_e2e = args.e2e_steps if args.e2e_steps is not None else max(2, min(steps, 200, int(4.0 / per_step_s)))
-        if dist is not None:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(n_e2e):
-            host_step()
-        el = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([el], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        bsz = 4 if tdt == torch.float32 else 8
-        e2e_sync = {"value": world * units_per_step * n_e2e / el, "unit": UNIT,
-                    "h2d_bytes_per_step": int(2 * nsl * g.nx * g.ny * bsz + (0 if hm is None else hm.numel())),
-                    "d2h_bytes_per_step": int(nsl * ns * g.nx * g.ny * bsz + nsl * ns * 8), "steps": n_e2e,
-                    "timing": "wall clock around synchronous cgef_sweep calls (host buffers, pinned)"}
+    el = max_over_ranks(time.perf_counter() - t0, dist)
+    e2e_sync = {"value": world * units_per_step * n_e2e / el, "unit": UNIT,
+                "h2d_bytes_per_step": int(2 * nsl * g.nx * g.ny * bsz + (0 if hm is None else hm.numel())),
+                "d2h_bytes_per_step": int(nsl * ns * g.nx * g.ny * bsz + nsl * ns * 8), "steps": n_e2e,
+                "timing": "wall clock around synchronous cgef_sweep calls (host buffers, pinned)"}
 
-        # the same steps streamed through cgef_pipeline_*: every step still copies its u, v in and its Pi
-        # and E out, but a step's copies overlap its neighbours' sweeps (double-buffered device memory)
-        ph = C.c_void_p()
-        _lib.check(L.cgef_pipeline_create(C.byref(ph), parr, ns, dt_code, nsl, None if hm is None else hm.data_ptr(),
-                                          1))
-        outs = [(torch.empty_like(hPi).pin_memory(), torch.empty_like(hE).pin_memory()) for _ in range(2)]
+    # the same steps streamed through cgef_pipeline_*: every step still copies its u, v in and its Pi
+    # and E out, but a step's copies overlap its neighbours' sweeps (double-buffered device memory)
+    ph = C.c_void_p()
+    _lib.check(L.cgef_pipeline_create(C.byref(ph), parr, ns, dt_code, nsl, None if hm is None else hm.data_ptr(), 1))
+    outs = [(torch.empty_like(hPi).pin_memory(), torch.empty_like(hE).pin_memory()) for _ in range(2)]
 
-        def submit(k):
-            pi_k, e_k = outs[k % 2]
-            _lib.check(L.cgef_pipeline_submit(ph, hu.data_ptr(), hv.data_ptr(), pi_k.data_ptr(), e_k.data_ptr()))
+    def submit(k):
+        pi_k, e_k = outs[k % 2]
+        _lib.check(L.cgef_pipeline_submit(ph, hu.data_ptr(), hv.data_ptr(), pi_k.data_ptr(), e_k.data_ptr()))
 
-        submit(0)
-        submit(1)
-        _lib.check(L.cgef_pipeline_drain(ph))
-        if dist is not None:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for k in range(n_e2e):
-            submit(k)
-        _lib.check(L.cgef_pipeline_drain(ph))
-        el = time.perf_counter() - t0
-        _lib.check(L.cgef_pipeline_destroy(ph))
-        if dist is not None:
-            t = torch.tensor([el], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
-        e2e = {"value": world * units_per_step * n_e2e / el, "unit": UNIT,
-               "h2d_bytes_per_step": int(2 * nsl * g.nx * g.ny * bsz),
-               "d2h_bytes_per_step": int(nsl * ns * g.nx * g.ny * bsz + nsl * ns * 8), "steps": n_e2e,
-               "timing": "wall clock from the first cgef_pipeline_submit to cgef_pipeline_drain: pinned u, v "
-                         "copied in and Pi, E copied out for every step, overlapping the neighbouring steps' "
-                         "sweeps (the per-level masks, if any, are copied once at create); no L2 flush: "
-                         "each step's inputs arrive by H2D",
-               "synchronous": e2e_sync}
+    submit(0)
+    submit(1)
+    _lib.check(L.cgef_pipeline_drain(ph))
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(n_e2e):
+        submit(k)
+    _lib.check(L.cgef_pipeline_drain(ph))
+    el = time.perf_counter() - t0
+    _lib.check(L.cgef_pipeline_destroy(ph))
+    el = max_over_ranks(el, dist)
+    e2e = {"value": world * units_per_step * n_e2e / el, "unit": UNIT,
+           "h2d_bytes_per_step": int(2 * nsl * g.nx * g.ny * bsz),
+           "d2h_bytes_per_step": int(nsl * ns * g.nx * g.ny * bsz + nsl * ns * 8), "steps": n_e2e,
+           "timing": "wall clock from the first cgef_pipeline_submit to cgef_pipeline_drain: pinned u, v "
+                     "copied in and Pi, E copied out for every step, overlapping the neighbouring steps' "
+                     "sweeps (the per-level masks, if any, are copied once at create); no L2 flush: "
+                     "each step's inputs arrive by H2D",
+           "synchronous": e2e_sync}
 
     cpu = None
     accuracy = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, nth, done, el, sample, ref = oracle_rate(wl, budget_s=20.0)
+    if rank == 0 and world == 1 and with_cpu and not args.no_cpu_baseline:
+        rate, nth, done, el, sample, ref = oracle_rate(wl, budget_s=cpu_budget)
         cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
                "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path (FP64 oracle, OpenMP rows)"}
         # the metric's accuracy term: the library's Pi (host C ABI, cgef_sweep) against the FP64 oracle on
@@ -881,24 +885,75 @@ def main():
                     "unit": f"Pi of snapshot {ref['slice']} at l = {wl['scales'][ref['scale']] / 1e3:g} km, all cells",
                     "streamed_equals_synchronous": bool(torch.equal(streamed, hPi))}
 
+    return {"value": value, "unit": UNIT, "steps": steps, "ms_per_step": graph_ms / steps,
+            "dtype": "f64" if wl["dtype"] == "f64" else "f64 (f32 storage)", "config": workload_config(wl),
+            "run": {"parallelism": f"{world} rank(s), independent snapshots per rank",
+                    "schedule_split_waves": waves, "row_spectral": [uses_row_spectral(p) for p in plans],
+                    "plan_setup_seconds": setup_s},
+            "timing": "value: K steps replayed from a CUDA graph captured once, each bracketed by CUDA events on "
+                      "the replay stream, a 256 MiB L2 flush between steps outside the events, max over ranks",
+            "gpu_launches": graph_launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+            "eager": eager_line, "accuracy": accuracy}
+
+
+def headline(args, world, rec) -> dict:
+    line = {"metric": METRIC, "value": rec["value"], "unit": UNIT, "n_gpus": world, "steps": rec["steps"],
+            "warmup": args.warmup, "ms_per_step": rec["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": rec["dtype"], "data": "synthetic (seeded)", "config": rec["config"]}
+    line.update({k: v for k, v in rec.items() if k not in line and k not in ("unit",)})
+    return line
+
+
+# ---------------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        wl = make_workload(args.workload, 0, args.snapshots, args.scale_km)
+        rate, nth, done, el, sample, _ = oracle_rate(wl, budget_s=120.0)
+        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded)", "config": workload_config(wl),
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
+                                 "sample": sample + f"; CPU {cpu_model()}; restated reference threaded path"},
+                "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.workload == "closure8":
+        line = headline(args, world, run_closure(args, rank, world, local, dist))
+    else:
+        line = headline(args, world, measure_sweep(args, args.workload, rank, world, local, dist,
+                                                   snapshots=args.snapshots, scale_km=args.scale_km,
+                                                   steps=args.steps))
+        # the metric compares the plain path with the batched sweep and the closure: the default run
+        # measures both beside the headline (one rank; a scaling run times the headline only)
+        if (args.workload == "sphere1" and args.snapshots == 1 and args.scale_km is None and world == 1
+                and not args.no_subrecords):
+            b = measure_sweep(args, "sweep24x8", rank, world, local, dist, steps=args.batched_steps, e2e_steps=2,
+                              cpu_budget=15.0)
+            b["speedup_vs_plain"] = b["value"] / line["value"]
+            line["batched"] = b
+            line["closure"] = run_closure(args, rank, world, local, dist, steps=3)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
-            "ms_per_step": graph_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if wl["dtype"] == "f64" else "f64 (f32 storage)", "data": "synthetic (seeded)",
-            "config": {"workload": wl["desc"], "nx": g.nx, "ny": g.ny, "scales": ns, "snapshots": nsl,
-                       "active_fraction": float(1.0 if g.mask is None else g.mask.mean()),
-                       "l2": "flushed between steps (a 256 MiB write before every step, outside the step's own events)",
-                       "parallelism": f"{world} rank(s), independent snapshots per rank",
-                       "schedule_split_waves": waves,
-                       "row_spectral": [uses_row_spectral(p) for p in plans]},
-            "timing": "value: K steps replayed from a CUDA graph captured once, each bracketed by CUDA events on "
-                      "the replay stream, a 256 MiB L2 flush between steps outside the events, max over ranks",
-            "gpu_launches": graph_launches, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
-            "eager": eager_line, "accuracy": accuracy}
     print(json.dumps(line))
     return 0
 

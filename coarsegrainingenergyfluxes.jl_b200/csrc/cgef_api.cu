@@ -683,27 +683,41 @@ int32_t cgef_plan_autotune(cgef_plan* p, int32_t nbatch, double* chosen) {
     *ms_out = ms / done;
     return CGEF_OK;
   };
-  // 1. split granularity of the direct flux gather's schedule
+  auto flux_pass = [&] {
+    return pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0, static_cast<double*>(gather), st);
+  };
+  // 0. the row-spectral evaluation of the flux's sums, where the plan has it, and the direct gather at
+  // the default granularity: when the direct gather is more than twice slower, the spectral evaluation
+  // is kept without tuning the direct gather's schedule (at large scales that tuning would cost seconds
+  // of gathers that the plan will never run)
   const bool rs_avail = p->rs_L > 0;
+  double ms_rs = 1e300;
+  if (rs_avail) {
+    p->rs_on = true;
+    rc = time_pass(flux_pass, &ms_rs);
+  }
   p->rs_on = false;
-  const double cand[4] = {2.0, 4.0, 8.0, 16.0};
   double best = p->sched[0].waves, best_ms = 1e300;
+  if (rc == CGEF_OK) rc = time_pass(flux_pass, &best_ms);
+  const bool spectral_clear = rc == CGEF_OK && rs_avail && best_ms > 2.0 * ms_rs;
+  // 1. split granularity of the direct flux gather's schedule
+  const double cand[4] = {2.0, 4.0, 8.0, 16.0};
   for (double w : cand) {
+    if (rc != CGEF_OK || spectral_clear) break;
+    if (w == best) continue;
     double ms = 0.0;
     if ((rc = rebuild_schedule(p, w, 0))) break;
-    if ((rc = time_pass([&] { return pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0,
-                                               static_cast<double*>(gather), st); },
-                        &ms)))
-      break;
+    if ((rc = time_pass(flux_pass, &ms))) break;
     if (ms < best_ms) {
       best_ms = ms;
       best = w;
     }
   }
   if (rc == CGEF_OK) rc = rebuild_schedule(p, best, 0);
-  // 2. tile height of the filter passes (timed on a three-field pass: the velocity gather)
+  // 2. tile height of the filter passes (timed on a three-field pass: the velocity gather); the
+  // spectral evaluation serves the filter passes too where it is kept
   if (rc == CGEF_OK) rc = rebuild_schedule(p, best, 1);
-  if (rc == CGEF_OK) {
+  if (rc == CGEF_OK && !spectral_clear) {
     const void* f[3] = {zin, zin, zin};
     double* G = static_cast<double*>(gather);
     double* o[3] = {G, G + N, G + 2 * N};
@@ -717,14 +731,7 @@ int32_t cgef_plan_autotune(cgef_plan* p, int32_t nbatch, double* chosen) {
     p->filter_rows = (rc == CGEF_OK && ms_r[1] < ms_r[0]) ? kRowsTall : kRows;
   }
   // 3. direct gather or row-spectral evaluation of the flux's sums, whichever is faster here
-  if (rc == CGEF_OK && rs_avail) {
-    double ms_rs = 0.0;
-    p->rs_on = true;
-    rc = time_pass([&] { return pi_gather(p, planes, pitch, p->H, np, nbatch, p->d_mask, 0,
-                                          static_cast<double*>(gather), st); },
-                   &ms_rs);
-    p->rs_on = rc == CGEF_OK && ms_rs < best_ms;
-  }
+  p->rs_on = rc == CGEF_OK && rs_avail && ms_rs < best_ms;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;

@@ -138,13 +138,16 @@ int32_t cgef_plan_reset_queue(cgef_plan* plan);
 int32_t cgef_plan_get_info(const cgef_plan* plan, cgef_plan_info* info);
 
 /* Schedule autotuner of the banded engine (no counterpart in the reference, whose loops have no
- * schedule).  Times the flux gather on this plan's grid and mask (zero-valued inputs; the gather's
- * cost depends on the footprint and the mask, not on the values) for each candidate split
- * granularity -- the work-item schedule cut into about 2, 4, 8 or 16 rounds of resident warps per
- * SM -- and keeps the fastest; `chosen` (may be NULL) receives it.  It then times a three-field
- * filter pass with 4- and 8-row tiles and keeps the faster for the filter passes.  A no-op for the separable and
- * prefix engines.  Results stay within FP64 rounding of each other across schedules: only the
- * order in which a split tile's partial sums are added changes. */
+ * schedule).  Times the flux's footprint sums on this plan's grid and mask (zero-valued inputs; their
+ * cost depends on the footprint and the mask, not on the values): first the row-spectral evaluation
+ * (where the plan has it) and the direct gather at its current granularity.  When the direct gather is
+ * more than twice slower the spectral evaluation is kept and nothing else is timed.  Otherwise each
+ * candidate split granularity of the direct gather -- the work-item schedule cut into about 2, 4, 8 or
+ * 16 rounds of resident warps per SM -- is timed and the fastest kept (`chosen`, may be NULL, receives
+ * it); a three-field filter pass is timed with 4- and 8-row tiles and the faster kept for the filter
+ * passes; and the faster of the two evaluations is kept.  A no-op for the separable and prefix engines.
+ * Results stay within FP64 rounding of each other across schedules: only the order in which a split
+ * tile's partial sums are added changes. */
 int32_t cgef_plan_autotune(cgef_plan* plan, int32_t nbatch, double* chosen);
 /* Sets the split granularity directly (rounds of resident warps per SM, > 0; the default is 4). */
 int32_t cgef_plan_set_split_waves(cgef_plan* plan, double waves);
