@@ -110,6 +110,41 @@ __device__ __forceinline__ void expand_pair(const double (&v)[Cfg<MODE, NF, DEF>
   if (DEF) q[C::NA - 1] = v[C::NP - 1] + u[C::NP - 1];
 }
 
+// The local-frame filtered velocity from the planetary one (sphere, Diagnostics.jl:596-610): the
+// east and north unit vectors e = (-sin lam, cos lam, 0), n = (-sin phi cos lam, -sin phi sin lam,
+// cos phi).  Shared by every epilogue so all of them round alike.
+__device__ __forceinline__ void local_velocity(double ub0, double ub1, double ub2, double sl, double cl, double sp,
+                                               double cp, double& u, double& v) {
+  const double e0 = -sl, e1 = cl, e2 = 0.0;
+  const double n0 = -sp * cl, n1 = -sp * sl, n2 = cp;
+  u = e0 * ub0 + e1 * ub1 + e2 * ub2;
+  v = n0 * ub0 + n1 * ub1 + n2 * ub2;
+}
+
+// tau = (u_i u_j)bar - ubar_i ubar_j in the planetary frame, rotated to east/north (Diagnostics.jl:
+// 612-650); F holds the normalised quantities of the sphere flux (3 velocities, 6 products).
+__device__ __forceinline__ void local_tau_sphere(const double* F, double sl, double cl, double sp, double cp,
+                                                 double& txx, double& txy, double& tyy) {
+  const double ub0 = F[0], ub1 = F[1], ub2 = F[2];
+  const double e0 = -sl, e1 = cl, e2 = 0.0;
+  const double n0 = -sp * cl, n1 = -sp * sl, n2 = cp;
+  const double t00 = F[3] - ub0 * ub0;
+  const double t01 = F[4] - ub0 * ub1;
+  const double t02 = F[5] - ub0 * ub2;
+  const double t11 = F[6] - ub1 * ub1;
+  const double t12 = F[7] - ub1 * ub2;
+  const double t22 = F[8] - ub2 * ub2;
+  const double te0 = t00 * e0 + t01 * e1 + t02 * e2;
+  const double te1 = t01 * e0 + t11 * e1 + t12 * e2;
+  const double te2 = t02 * e0 + t12 * e1 + t22 * e2;
+  const double tn0 = t00 * n0 + t01 * n1 + t02 * n2;
+  const double tn1 = t01 * n0 + t11 * n1 + t12 * n2;
+  const double tn2 = t02 * n0 + t12 * n1 + t22 * n2;
+  txx = e0 * te0 + e1 * te1 + e2 * te2;
+  txy = e0 * tn0 + e1 * tn1 + e2 * tn2;
+  tyy = n0 * tn0 + n1 * tn1 + n2 * tn2;
+}
+
 // Normalised epilogue shared by the direct-sum engines.  F holds the NA0 filtered quantities
 // (already divided by the denominator); writes the mode's outputs at offset o.
 template <int MODE, int NA0>
@@ -135,26 +170,14 @@ __device__ __forceinline__ void write_outputs(double* const (&out)[9], int64_t o
     return;
   }
   // Sphere (Diagnostics.jl:596-650): planetary ubar and tau, rotated to east/north.
-  const double ub0 = F[0], ub1 = F[1], ub2 = F[2];
-  const double e0 = -sl, e1 = cl, e2 = 0.0;
-  const double n0 = -sp * cl, n1 = -sp * sl, n2 = cp;
-  out[0][o] = e0 * ub0 + e1 * ub1 + e2 * ub2;
-  out[1][o] = n0 * ub0 + n1 * ub1 + n2 * ub2;
-  const double t00 = F[3] - ub0 * ub0;
-  const double t01 = F[4] - ub0 * ub1;
-  const double t02 = F[5] - ub0 * ub2;
-  const double t11 = F[6] - ub1 * ub1;
-  const double t12 = F[7] - ub1 * ub2;
-  const double t22 = F[8] - ub2 * ub2;
-  const double te0 = t00 * e0 + t01 * e1 + t02 * e2;
-  const double te1 = t01 * e0 + t11 * e1 + t12 * e2;
-  const double te2 = t02 * e0 + t12 * e1 + t22 * e2;
-  const double tn0 = t00 * n0 + t01 * n1 + t02 * n2;
-  const double tn1 = t01 * n0 + t11 * n1 + t12 * n2;
-  const double tn2 = t02 * n0 + t12 * n1 + t22 * n2;
-  out[2][o] = e0 * te0 + e1 * te1 + e2 * te2;
-  out[3][o] = e0 * tn0 + e1 * tn1 + e2 * tn2;
-  out[4][o] = n0 * tn0 + n1 * tn1 + n2 * tn2;
+  double u, v, txx, txy, tyy;
+  local_velocity(F[0], F[1], F[2], sl, cl, sp, cp, u, v);
+  local_tau_sphere(F, sl, cl, sp, cp, txx, txy, tyy);
+  out[0][o] = u;
+  out[1][o] = v;
+  out[2][o] = txx;
+  out[3][o] = txy;
+  out[4][o] = tyy;
 }
 
 // Finishes one target (row t of a tile) from its accumulated sums: normalise, then write the
@@ -171,9 +194,11 @@ __device__ __forceinline__ void finish_target(const BandedK& a, const double (&a
   else
     den = a.den_zf_2d ? a.den_zf[pix] : a.den_zf[j];
   const bool zero = !act || !(den > kNormEps);
+  // one reciprocal per target (every epilogue of the flux normalises this way, so they round alike)
+  const double inv = 1.0 / den;
   double F[C::NA0];
 #pragma unroll
-  for (int m = 0; m < C::NA0; ++m) F[m] = zero ? 0.0 : acc[m] / den;
+  for (int m = 0; m < C::NA0; ++m) F[m] = zero ? 0.0 : acc[m] * inv;
   const double sl = a.sinlam ? a.sinlam[col] : 0.0;
   const double cl = a.coslam ? a.coslam[col] : 0.0;
   const double sp = a.sinphi ? a.sinphi[j] : 0.0;

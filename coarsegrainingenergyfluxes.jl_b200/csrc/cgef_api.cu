@@ -126,7 +126,8 @@ int mode_for(const cgef_plan* p) { return p->geometry == CGEF_SPHERICAL ? kModeP
 // Stages the inputs and runs one plan's engine for a flux computation; leaves the 5 FP64
 // gather planes (ubar, vbar, txx, txy, tyy) at `gather` with slice stride 5*N.
 int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, int nbatch, const uint8_t* mask,
-              int64_t mstride, double* gather, cudaStream_t st, const RsShare& share) {
+              int64_t mstride, double* gather, cudaStream_t st, const RsShare& share, const double** raw_out) {
+  if (raw_out) *raw_out = nullptr;
   const int64_t N = static_cast<int64_t>(p->nx) * p->ny;
   GatherOut go{};
   for (int m = 0; m < 5; ++m) go.o[m] = gather + m * N;
@@ -141,10 +142,14 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
       int rc = ensure_ws(p, kSlotSplit, pb, &part);
       if (rc) return rc;
     }
-    if (p->rs_on && (share.keep || share.in))
-      return launch_rowspec(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st,
-                            share);
-    return launch_banded(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st);
+    if (p->rs_on) {
+      int rc = launch_rowspec(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st,
+                              share, raw_out != nullptr);
+      if (rc == CGEF_OK && raw_out) *raw_out = static_cast<const double*>(part);
+      return rc;
+    }
+    return launch_banded(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st,
+                         true);
   }
   if (p->engine == CGEF_ENGINE_SEPARABLE) {
     const int na = 5 + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
@@ -201,8 +206,10 @@ int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int
   void* gather = nullptr;
   if ((rc = ensure_ws(p, kSlotGather, sizeof(double) * 5 * N * nbatch, &gather))) return rc;
   double* g = static_cast<double*>(gather);
-  if ((rc = pi_gather(p, planes, pitch, p->H, np, nbatch, mask, mstride, g, st))) return rc;
+  const double* raw = nullptr;
+  if ((rc = pi_gather(p, planes, pitch, p->H, np, nbatch, mask, mstride, g, st, RsShare{}, &raw))) return rc;
   StrainArgs sa{};
+  sa.raw = raw;
   sa.ubar = g;
   sa.vbar = g + N;
   sa.txx = g + 2 * N;
@@ -371,10 +378,12 @@ int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u,
       transformed = true;
     }
     // each plan runs its engine with its own scratch (split partials, separable rows, prefix sums, spectra)
-    rc = pi_gather(q, planes, pitch, halo, np, nbatch, mask, mstride, g, st, share);
+    const double* raw = nullptr;
+    rc = pi_gather(q, planes, pitch, halo, np, nbatch, mask, mstride, g, st, share, &raw);
     q->H = saveH;
     if (rc) return rc;
     StrainArgs sa{};
+    sa.raw = raw;
     sa.ubar = g;
     sa.vbar = g + N;
     sa.txx = g + 2 * N;

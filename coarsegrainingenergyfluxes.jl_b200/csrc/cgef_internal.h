@@ -299,9 +299,11 @@ struct RsShare {
   double* keep = nullptr;
   const double* in = nullptr;
 };
+// `leave_raw` (flux modes): stop before the epilogue and leave the unnormalised sums [slice][NA][ny][nx]
+// at the start of `scratch`, for the strain pass to finish (StrainArgs::raw).
 int launch_rowspec(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                    const uint8_t* mask, int64_t mask_slice_stride, double* scratch, const GatherOut& out,
-                   cudaStream_t st, const RsShare& share = RsShare{});
+                   cudaStream_t st, const RsShare& share = RsShare{}, bool leave_raw = false);
 
 // Bytes of one sweep's shared source spectra: `na` quantities over `nbatch` slices.
 inline size_t rowspec_spectra_bytes(const cgef_plan* p, int na, int nbatch) {
@@ -395,6 +397,9 @@ struct StrainArgs {
   // strain / convergence split (plane; outputs of dtype, out_slice_stride): total, strain,
   // convergence, divergence, strain magnitude.  nullptr = skip.
   void* sc[5];
+  // The row-spectral evaluation's unnormalised sums [slice][NA][ny][nx] (pi_gather's raw output):
+  // finished here instead of reading ubar, vbar and tau.  nullptr = the finished planes.
+  const double* raw = nullptr;
 };
 
 int launch_strain(const cgef_plan* p, const StrainArgs& a, cudaStream_t st);
@@ -452,9 +457,12 @@ int mode_for(const cgef_plan* p);
 // Stages u, v (planetary components on the sphere) into padded planes in slot kSlotPlanes.
 int stage_pi(cgef_plan* p, int dtype, const void* u, const void* v, int nbatch, const uint8_t* mask, int64_t mstride,
              int halo, double** planes_out, int* pitch_out, int* np_out, cudaStream_t st);
-// Runs the plan's engine in a flux mode: 5 FP64 planes (ubar, vbar, txx, txy, tyy) per slice.
+// Runs the plan's engine in a flux mode: 5 FP64 planes (ubar, vbar, txx, txy, tyy) per slice.  With
+// `raw_out`, a plan on the row-spectral evaluation instead leaves its unnormalised sums and points
+// *raw_out at them (nullptr otherwise), for a strain pass that finishes them itself.
 int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, int nbatch, const uint8_t* mask,
-              int64_t mstride, double* gather, cudaStream_t st, const RsShare& share = RsShare{});
+              int64_t mstride, double* gather, cudaStream_t st, const RsShare& share = RsShare{},
+              const double** raw_out = nullptr);
 int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int64_t nbatch64,
                       const uint8_t* slice_masks, const cgef_pi_outputs* out, cudaStream_t st);
 // The sweep over plans (one grid) for nbatch slices on stream st: Pi [nbatch][nscales][N] (dtype) and

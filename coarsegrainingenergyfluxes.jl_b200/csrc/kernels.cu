@@ -343,8 +343,18 @@ __global__ void __launch_bounds__(32 * kWarps, banded_min_blocks(MODE)) banded_k
   __shared__ int rint[kWarps][3][R];  // per warp: a, hi, woff of the R rows for the current source row
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  if (SAFE && a.flags[a.nslices] == 0) return;  // no flagged slice: no warp takes a unit, the queue stays 0
   const int64_t total = static_cast<int64_t>(a.nitems) * a.nslices;
+  if (SAFE) {
+    // the rare non-finite pass: a small grid striding over the units, no queue (no flagged slice: it
+    // returns at once)
+    if (a.flags[a.nslices] == 0) return;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * kWarps;
+    for (int64_t gid = static_cast<int64_t>(blockIdx.x) * kWarps + warp; gid < total; gid += stride) {
+      banded_unit<MODE, NF, DEF, R, PAIR, SAFE>(a, gid, &wbuf[warp][0][0], rint[warp], lane);
+      __syncwarp();
+    }
+    return;
+  }
   for (int64_t gid = take_unit(a.queue, lane); gid < total; gid = take_unit(a.queue, lane)) {
     banded_unit<MODE, NF, DEF, R, PAIR, SAFE>(a, gid, &wbuf[warp][0][0], rint[warp], lane);
     __syncwarp();
@@ -352,16 +362,11 @@ __global__ void __launch_bounds__(32 * kWarps, banded_min_blocks(MODE)) banded_k
   leave_queue(a.queue, lane);
 }
 
-// Adds the partial slots of every split tile in slot order (deterministic) and finishes it: one warp
-// per (tile, slice, target row).  The loads of four slots are in flight together; the additions stay
-// in slot order.
+// One (split tile, slice, target row) of the combine pass: the slots added in slot order, then finished.
 template <int MODE, int NF, bool DEF, int R, bool SAFE>
-__global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
+__device__ __forceinline__ void combine_group_row(const BandedK& a, int64_t gid, int lane) {
   using C = Cfg<MODE, NF, DEF>;
   constexpr int kAhead = 4;
-  const int lane = threadIdx.x & 31;
-  const int64_t gid = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  if (gid >= static_cast<int64_t>(a.ngroups) * a.nslices * R) return;
   const int t = static_cast<int>(gid % R);
   const int64_t gs = gid / R;
   const int gi = static_cast<int>(gs / a.nslices);
@@ -396,6 +401,19 @@ __global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
     write_raw<MODE, NF, DEF>(a, acc, slice, j, col);
   else
     finish_target<MODE, NF, DEF>(a, acc, slice, j, col);
+}
+
+// Adds the partial slots of every split tile in slot order (deterministic) and finishes it: one warp
+// per (tile, slice, target row).  The loads of four slots are in flight together; the additions stay
+// in slot order.
+template <int MODE, int NF, bool DEF, int R, bool SAFE>
+__global__ void __launch_bounds__(128) banded_combine_kernel(BandedK a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t total = static_cast<int64_t>(a.ngroups) * a.nslices * R;
+  if (SAFE && a.flags[a.nslices] == 0) return;
+  const int64_t stride = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t gid = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; gid < total; gid += stride)
+    combine_group_row<MODE, NF, DEF, R, SAFE>(a, gid, lane);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -671,16 +689,32 @@ __device__ __forceinline__ StencilCase stencil_case(const Line& L, int p) {
   return c;
 }
 
-__device__ __forceinline__ double apply_stencil(const StencilCase& c, const double* f, int64_t stride, int p,
-                                                double h) {
+// The case's formula on the values at the point (f0) and at its neighbours m1, p1 and x2 (the second
+// neighbour on the case's side); values a case does not use are ignored.
+__device__ __forceinline__ double stencil_eval(const StencilCase& c, double f0, double fm1, double fp1, double fx2,
+                                               double h) {
   switch (c.kind) {
-    case 1: return (f[c.p1 * stride] - f[c.m1 * stride]) / (2.0 * h);
-    case 2: return (-3.0 * f[p * stride] + 4.0 * f[c.p1 * stride] - f[c.x2 * stride]) / (2.0 * h);
-    case 3: return (f[c.p1 * stride] - f[p * stride]) / h;
-    case 4: return (3.0 * f[p * stride] - 4.0 * f[c.m1 * stride] + f[c.x2 * stride]) / (2.0 * h);
-    case 5: return (f[p * stride] - f[c.m1 * stride]) / h;
+    case 1: return (fp1 - fm1) / (2.0 * h);
+    case 2: return (-3.0 * f0 + 4.0 * fp1 - fx2) / (2.0 * h);
+    case 3: return (fp1 - f0) / h;
+    case 4: return (3.0 * f0 - 4.0 * fm1 + fx2) / (2.0 * h);
+    case 5: return (f0 - fm1) / h;
     default: return 0.0;
   }
+}
+
+// Which neighbours a case reads.
+__device__ __forceinline__ bool uses_m1(const StencilCase& c) { return c.kind == 1 || c.kind == 4 || c.kind == 5; }
+__device__ __forceinline__ bool uses_p1(const StencilCase& c) { return c.kind == 1 || c.kind == 2 || c.kind == 3; }
+__device__ __forceinline__ bool uses_x2(const StencilCase& c) { return c.kind == 2 || c.kind == 4; }
+
+__device__ __forceinline__ double apply_stencil(const StencilCase& c, const double* f, int64_t stride, int p,
+                                                double h) {
+  const double f0 = f[p * stride];
+  const double fm1 = uses_m1(c) ? f[c.m1 * stride] : 0.0;
+  const double fp1 = uses_p1(c) ? f[c.p1 * stride] : 0.0;
+  const double fx2 = uses_x2(c) ? f[c.x2 * stride] : 0.0;
+  return stencil_eval(c, f0, fm1, fp1, fx2, h);
 }
 
 __device__ double stencil(const Line& L, int p) {
@@ -734,9 +768,97 @@ struct StrainK {
   double* gpartials;  // [slice][block][2]: sum of |grad|^2 and active count
   // strain / convergence split of the flux (plane): total, strain, convergence, divergence, |strain|
   void* sc[5];
+  // Row-spectral source (strain_kernel with RAW): the unnormalised footprint sums of the flux's
+  // quantities, [slice][NA][ny][nx], finished here at each target and at its stencil neighbours with
+  // the arithmetic of finish_target; ub, vb and the tau planes are then unused.
+  const double* raw;
+  const double* den_zf;  // ZeroFill denominator per row (periodic x) or per cell
+  int den_zf_2d;
+  const double* sinlam;
+  const double* coslam;
+  const double* sinphi;
+  const double* cosphi;
 };
 
 constexpr int kStrainBX = 32, kStrainBY = 8;
+
+// Finishing of the raw sums: the normalisation of finish_target (inactive targets and denominators
+// at or below kNormEps give 0), then the local-frame velocity of write_outputs.
+template <int MODE, bool DEF>
+struct RawFlux {
+  static constexpr int NA0 = MODE == kModePiSphere ? 9 : 5;
+  static constexpr int NA = NA0 + (DEF ? 1 : 0);
+  static constexpr int NV = MODE == kModePiSphere ? 3 : 2;
+};
+
+template <int MODE, bool DEF>
+__device__ __forceinline__ bool raw_zero(const StrainK& a, const double* Fs, int64_t plane, int64_t pix, int j,
+                                         bool act, double& den) {
+  if (DEF)
+    den = Fs[(RawFlux<MODE, DEF>::NA - 1) * plane + pix];
+  else
+    den = a.den_zf_2d ? a.den_zf[pix] : a.den_zf[j];
+  return !act || !(den > kNormEps);
+}
+
+// Finished local velocity at (j, i) of the slice whose raw sums start at Fs.
+template <int MODE, bool DEF>
+__device__ __forceinline__ void raw_velocity(const StrainK& a, const double* Fs, const uint8_t* mk, int j, int i,
+                                             double& u, double& v) {
+  using R = RawFlux<MODE, DEF>;
+  const int64_t plane = static_cast<int64_t>(a.nx) * a.ny;
+  const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+  const bool act = mk == nullptr || mk[pix] != 0;
+  double den;
+  const bool zero = raw_zero<MODE, DEF>(a, Fs, plane, pix, j, act, den);
+  if (zero) {
+    u = 0.0;
+    v = 0.0;
+    return;
+  }
+  const double inv = 1.0 / den;
+  double F[R::NV];
+#pragma unroll
+  for (int m = 0; m < R::NV; ++m) F[m] = Fs[m * plane + pix] * inv;
+  if constexpr (MODE == kModePiSphere) {
+    local_velocity(F[0], F[1], F[2], a.sinlam[i], a.coslam[i], a.sinphi[j], a.cosphi[j], u, v);
+  } else {
+    u = F[0];
+    v = F[1];
+  }
+}
+
+// Finished local velocity and stress at target (j, i).
+template <int MODE, bool DEF>
+__device__ __forceinline__ void raw_target(const StrainK& a, const double* Fs, const uint8_t* mk, int j, int i,
+                                           double& u, double& v, double& txx, double& txy, double& tyy) {
+  using R = RawFlux<MODE, DEF>;
+  const int64_t plane = static_cast<int64_t>(a.nx) * a.ny;
+  const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+  const bool act = mk == nullptr || mk[pix] != 0;
+  double den;
+  const bool zero = raw_zero<MODE, DEF>(a, Fs, plane, pix, j, act, den);
+  if (zero) {
+    u = v = txx = txy = tyy = 0.0;
+    return;
+  }
+  const double inv = 1.0 / den;
+  double F[R::NA0];
+#pragma unroll
+  for (int m = 0; m < R::NA0; ++m) F[m] = Fs[m * plane + pix] * inv;
+  if constexpr (MODE == kModePiSphere) {
+    const double sl = a.sinlam[i], cl = a.coslam[i], sp = a.sinphi[j], cp = a.cosphi[j];
+    local_velocity(F[0], F[1], F[2], sl, cl, sp, cp, u, v);
+    local_tau_sphere(F, sl, cl, sp, cp, txx, txy, tyy);
+  } else {
+    // Diagnostics.jl:525-527
+    u = F[0];
+    v = F[1];
+    txx = F[2] - F[0] * F[0];
+    txy = F[3] - F[0] * F[1];
+    tyy = F[4] - F[1] * F[1];
+  }
+}
 
 __device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
   // deterministic: warp shuffles in a fixed tree, then warp results in order
@@ -763,36 +885,115 @@ __device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
   }
 }
 
-__global__ void strain_kernel(StrainK a) {
+// One block per 32 x 8 target tile: the filtered local velocity over the tile and a halo of kStrainHalo
+// cells (the 3-node stencil's reach along either axis) is loaded once into shared memory -- from the
+// finished planes of the direct engines (RAW false), or finished here from the row-spectral
+// evaluation's raw sums (RAW true; MODE, DEF: the flux's quantities), the same values bit for bit, so
+// that evaluation writes no finished planes.  The stencil cases come from the mask; the values they
+// read come from the tile.
+constexpr int kStrainHalo = 2;
+
+// stencil_case() from the activity of the neighbours at -1, +1, -2 and +2 along the axis, as the tile
+// holds them (0 off a bounded axis, the wrapped cell on a periodic one).  Equal to stencil_case() for
+// axes of three or more cells (with two, a periodic cell's -1 and +1 neighbours are one cell, which
+// makes the case centred or empty and never reads x2; with one, the derivative is 0 regardless).  Only
+// the kind matters here: the values come from the tile by offset.
+__device__ __forceinline__ StencilCase tile_case(unsigned char am1, unsigned char ap1, unsigned char am2,
+                                                 unsigned char ap2) {
+  StencilCase c{0, -1, -1, -1};
+  if (am1 && ap1)
+    c.kind = 1;
+  else if (ap1)
+    c.kind = ap2 ? 2 : 3;
+  else if (am1)
+    c.kind = am2 ? 4 : 5;
+  return c;
+}
+
+template <bool RAW, int MODE, bool DEF>
+__global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a) {
+  constexpr int TW = kStrainBX + 2 * kStrainHalo, TH = kStrainBY + 2 * kStrainHalo;
   __shared__ double sh[2 * (kStrainBX * kStrainBY / 32)];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  __shared__ double tu[TH][TW];
+  __shared__ double tv[TH][TW];
+  __shared__ unsigned char tm[TH][TW];  // activity (0 off a bounded axis)
+  const int x0 = blockIdx.x * kStrainBX, y0 = blockIdx.y * kStrainBY;
   const int s = blockIdx.z;
+  const uint8_t* mk = a.mask ? a.mask + s * a.mask_stride : nullptr;
+  const double* ub = RAW ? nullptr : a.ub + s * a.in_stride;
+  const double* vb = RAW ? nullptr : a.vb + s * a.in_stride;
+  const double* Fs = RAW ? a.raw + s * static_cast<int64_t>(RawFlux<MODE, DEF>::NA) * a.nx * a.ny : nullptr;
+  for (int c = threadIdx.y * kStrainBX + threadIdx.x; c < TW * TH; c += kStrainBX * kStrainBY) {
+    const int r = c / TW, q = c - r * TW;
+    int jj = y0 - kStrainHalo + r, ii = x0 - kStrainHalo + q;
+    bool inside = true;
+    if (jj < 0 || jj >= a.ny) {
+      if (a.periodic_y)
+        jj = wrap(jj, a.ny);
+      else
+        inside = false;
+    }
+    if (ii < 0 || ii >= a.nx) {
+      if (a.periodic_x)
+        ii = wrap(ii, a.nx);
+      else
+        inside = false;
+    }
+    double u = 0.0, v = 0.0;
+    unsigned char am = 0;
+    if (inside) {
+      am = mk == nullptr || mk[static_cast<int64_t>(jj) * a.nx + ii] != 0;
+      if (RAW) {
+        raw_velocity<MODE, DEF>(a, Fs, mk, jj, ii, u, v);
+      } else {
+        const int64_t k = static_cast<int64_t>(jj) * a.nx + ii;
+        u = ub[k];
+        v = vb[k];
+      }
+    }
+    tu[r][q] = u;
+    tv[r][q] = v;
+    tm[r][q] = am;
+  }
+  __syncthreads();
+  const int i = x0 + threadIdx.x;
+  const int j = y0 + threadIdx.y;
+  const int cx0 = threadIdx.x + kStrainHalo, cy0 = threadIdx.y + kStrainHalo;
   double e_num = 0.0, e_area = 0.0, g_sum = 0.0, g_cnt = 0.0;
   if (i < a.nx && j < a.ny) {
     const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
     const int64_t o = s * a.out_stride + pix;
-    const uint8_t* mk = a.mask ? a.mask + s * a.mask_stride : nullptr;
     const bool act = mk == nullptr || mk[pix] != 0;
-    const double* ub = a.ub + s * a.in_stride;
-    const double* vb = a.vb + s * a.in_stride;
     double sxx = 0.0, sxy = 0.0, syy = 0.0, pi = 0.0;
     double g1 = 0.0, g2 = 0.0;  // du/dy and dv/dx + u t (the two halves of 2 S_en)
-    const double u0 = ub[pix], v0 = vb[pix];
-    const double txx = a.txx ? a.txx[s * a.in_stride + pix] : 0.0;
-    const double txy = a.txy ? a.txy[s * a.in_stride + pix] : 0.0;
-    const double tyy = a.tyy ? a.tyy[s * a.in_stride + pix] : 0.0;
+    double u0, v0, txx, txy, tyy;
+    if (RAW) {
+      raw_target<MODE, DEF>(a, Fs, mk, j, i, u0, v0, txx, txy, tyy);
+    } else {
+      u0 = tu[cy0][cx0];
+      v0 = tv[cy0][cx0];
+      txx = a.txx ? a.txx[s * a.in_stride + pix] : 0.0;
+      txy = a.txy ? a.txy[s * a.in_stride + pix] : 0.0;
+      tyy = a.tyy ? a.tyy[s * a.in_stride + pix] : 0.0;
+    }
     if (act) {
-      const Line Lx{ub + static_cast<int64_t>(j) * a.nx, mk ? mk + static_cast<int64_t>(j) * a.nx : nullptr, 1,
-                    a.nx, a.periodic_x, a.dx};
-      const Line Ly{ub + i, mk ? mk + i : nullptr, a.nx, a.ny, a.periodic_y, a.dy};
-      const StencilCase cx = stencil_case(Lx, i), cy = stencil_case(Ly, j);
-      const double* vrow = vb + static_cast<int64_t>(j) * a.nx;
+      const StencilCase cx = tile_case(tm[cy0][cx0 - 1], tm[cy0][cx0 + 1], tm[cy0][cx0 - 2], tm[cy0][cx0 + 2]);
+      const StencilCase cy = tile_case(tm[cy0 - 1][cx0], tm[cy0 + 1][cx0], tm[cy0 - 2][cx0], tm[cy0 + 2][cx0]);
       const double xs = a.xscale[j];
-      const double dudx = a.nx < 2 ? 0.0 : apply_stencil(cx, Lx.f, 1, i, a.dx) * xs;
-      const double dudy = a.ny < 2 ? 0.0 : apply_stencil(cy, Ly.f, a.nx, j, a.dy) * a.yscale;
-      const double dvdx = a.nx < 2 ? 0.0 : apply_stencil(cx, vrow, 1, i, a.dx) * xs;
-      const double dvdy = a.ny < 2 ? 0.0 : apply_stencil(cy, vb + i, a.nx, j, a.dy) * a.yscale;
+      // the tile holds every neighbour a case reads: m1 and p1 at -1 and +1, x2 at +2 (forward) or -2
+      const int dx2 = cx.kind == 2 ? 2 : -2, dy2 = cy.kind == 2 ? 2 : -2;
+      const double dudx = a.nx < 2 ? 0.0
+                                   : stencil_eval(cx, u0, tu[cy0][cx0 - 1], tu[cy0][cx0 + 1], tu[cy0][cx0 + dx2],
+                                                  a.dx) * xs;
+      const double dvdx = a.nx < 2 ? 0.0
+                                   : stencil_eval(cx, v0, tv[cy0][cx0 - 1], tv[cy0][cx0 + 1], tv[cy0][cx0 + dx2],
+                                                  a.dx) * xs;
+      const double dudy = a.ny < 2 ? 0.0
+                                   : stencil_eval(cy, u0, tu[cy0 - 1][cx0], tu[cy0 + 1][cx0], tu[cy0 + dy2][cx0],
+                                                  a.dy) * a.yscale;
+      const double dvdy = a.ny < 2 ? 0.0
+                                   : stencil_eval(cy, v0, tv[cy0 - 1][cx0], tv[cy0 + 1][cx0], tv[cy0 + dy2][cx0],
+                                                  a.dy) * a.yscale;
       sxx = dudx;
       syy = dvdy;
       if (a.sphere) {
@@ -1026,6 +1227,19 @@ int launch_stage(const cgef_plan* p, int mode, const StageArgs& s, double* plane
 
 namespace {
 
+// SMs of the current device (cached per device).
+int sm_count() {
+  static int cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  if (cached[dev] == 0) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) return 148;
+    cached[dev] = sms;
+  }
+  return cached[dev];
+}
+
 // Blocks of one kernel instance that fit on the current device at once (cached per device).
 template <typename K>
 int64_t resident_blocks(K kernel) {
@@ -1049,22 +1263,35 @@ template <int MODE, int NF, bool DEF, int R, bool SAFE>
 int run_banded(const BandedK& a, bool pair, cudaStream_t st) {
   const int64_t units = static_cast<int64_t>(a.nitems) * a.nslices;
   const int64_t need = (units + kWarps - 1) / kWarps;
-  // the queue starts at zero even after a launch that stopped part-way (the kernel's last warp also
-  // zeroes it on the way out)
-  cudaError_t e = cudaMemsetAsync(a.queue, 0, 2 * sizeof(unsigned long long), st);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(work queue)");
-  if (!SAFE) prof_begin(CGEF_KERNEL_BANDED, st);
-  if (pair) {
-    const auto k = banded_kernel<MODE, NF, DEF, R, true, SAFE>;
-    k<<<static_cast<unsigned>(std::min(need, resident_blocks(k))), 32 * kWarps, 0, st>>>(a);
+  const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices * R;
+  int64_t cblocks = (cw + 3) / 4;
+  if (SAFE) {
+    // the non-finite pass strides over its units with two blocks per SM and no queue: launched on
+    // every row-spectral evaluation, it mostly finds no flag and returns at once
+    const int64_t small = 2 * static_cast<int64_t>(sm_count());
+    if (pair) {
+      banded_kernel<MODE, NF, DEF, R, true, true><<<static_cast<unsigned>(std::min(need, small)), 32 * kWarps, 0, st>>>(a);
+    } else {
+      banded_kernel<MODE, NF, DEF, R, false, true><<<static_cast<unsigned>(std::min(need, small)), 32 * kWarps, 0, st>>>(a);
+    }
+    cblocks = std::min(cblocks, small);
   } else {
-    const auto k = banded_kernel<MODE, NF, DEF, R, false, SAFE>;
-    k<<<static_cast<unsigned>(std::min(need, resident_blocks(k))), 32 * kWarps, 0, st>>>(a);
+    // the queue starts at zero even after a launch that stopped part-way (the kernel's last warp also
+    // zeroes it on the way out)
+    cudaError_t e = cudaMemsetAsync(a.queue, 0, 2 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(work queue)");
+    prof_begin(CGEF_KERNEL_BANDED, st);
+    if (pair) {
+      const auto k = banded_kernel<MODE, NF, DEF, R, true, false>;
+      k<<<static_cast<unsigned>(std::min(need, resident_blocks(k))), 32 * kWarps, 0, st>>>(a);
+    } else {
+      const auto k = banded_kernel<MODE, NF, DEF, R, false, false>;
+      k<<<static_cast<unsigned>(std::min(need, resident_blocks(k))), 32 * kWarps, 0, st>>>(a);
+    }
   }
   int rc = check_launch("banded_kernel");
   if (rc == CGEF_OK && a.ngroups > 0) {
-    const int64_t cw = static_cast<int64_t>(a.ngroups) * a.nslices * R;
-    banded_combine_kernel<MODE, NF, DEF, R, SAFE><<<static_cast<unsigned>((cw + 3) / 4), 128, 0, st>>>(a);
+    banded_combine_kernel<MODE, NF, DEF, R, SAFE><<<static_cast<unsigned>(cblocks), 128, 0, st>>>(a);
     rc = check_launch("banded_combine_kernel");
   }
   if (!SAFE) prof_end(CGEF_KERNEL_BANDED, st);
@@ -1339,10 +1566,25 @@ int launch_strain(const cgef_plan* p, const StrainArgs& s, cudaStream_t st) {
   a.grad_scale = s.grad_scale;
   a.gpartials = s.grad_mean ? s.grad_partials : nullptr;
   for (int k = 0; k < 5; ++k) a.sc[k] = s.sc[k];
+  a.raw = s.raw;
+  a.den_zf = p->d_den_zf;
+  a.den_zf_2d = p->den_zf_2d;
+  a.sinlam = p->d_sinlam;
+  a.coslam = p->d_coslam;
+  a.sinphi = p->d_sinphi;
+  a.cosphi = p->d_cosphi;
   dim3 block(kStrainBX, kStrainBY), grid((p->nx + kStrainBX - 1) / kStrainBX, (p->ny + kStrainBY - 1) / kStrainBY,
                                          s.nbatch);
+  const bool sph = p->geometry == CGEF_SPHERICAL, def = p->strategy == CGEF_DEFORMABLE;
   prof_begin(CGEF_KERNEL_STRAIN, st);
-  strain_kernel<<<grid, block, 0, st>>>(a);
+  if (s.raw == nullptr)
+    strain_kernel<false, kModePiSphere, false><<<grid, block, 0, st>>>(a);
+  else if (sph)
+    def ? strain_kernel<true, kModePiSphere, true><<<grid, block, 0, st>>>(a)
+        : strain_kernel<true, kModePiSphere, false><<<grid, block, 0, st>>>(a);
+  else
+    def ? strain_kernel<true, kModePiCart, true><<<grid, block, 0, st>>>(a)
+        : strain_kernel<true, kModePiCart, false><<<grid, block, 0, st>>>(a);
   prof_end(CGEF_KERNEL_STRAIN, st);
   int rc = check_launch("strain_kernel");
   if (rc) return rc;

@@ -235,6 +235,47 @@ __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int 
   }
 }
 
+// The same pass with its input and output through functors: src(sq, n) gives element n of sequence sq,
+// sink(sq, n, v) takes element n of the pass's output.  The inverse transform writes its last pass
+// straight out as real samples, so that pass needs no shared-memory round trip and no barrier after it.
+template <int R, typename Src, typename Sink>
+__device__ __forceinline__ void stockham_pass_io(Src src, Sink sink, int M, int Ns, unsigned ns_magic, int nseq,
+                                                 const double2* tw) {
+  const int nb = M / R;
+  const int tstride = 2 * (M / (Ns * R));
+  for (int t = threadIdx.x; t < nseq * nb; t += blockDim.x) {
+    int sq = 0, j = t;
+#pragma unroll
+    for (int e = 1; e < kRsSeq; ++e)
+      if (j >= nb) j -= nb, ++sq;
+    const int jq = Ns == 1 ? j : static_cast<int>(__umulhi(static_cast<unsigned>(j), ns_magic));
+    const int jm = j - jq * Ns;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src(sq, j + r * nb);
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + jm * tstride * r));
+    dft<R>(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) sink(sq, jq * Ns * R + jm + r * Ns, v[r]);
+  }
+}
+
+template <typename Src, typename Sink>
+__device__ __forceinline__ void pass_io(int R, Src src, Sink sink, int M, int Ns, unsigned mg, int nseq,
+                                        const double2* tw) {
+  switch (R) {
+    case 2: stockham_pass_io<2>(src, sink, M, Ns, mg, nseq, tw); break;
+    case 3: stockham_pass_io<3>(src, sink, M, Ns, mg, nseq, tw); break;
+    case 4: stockham_pass_io<4>(src, sink, M, Ns, mg, nseq, tw); break;
+    case 5: stockham_pass_io<5>(src, sink, M, Ns, mg, nseq, tw); break;
+    case 8: stockham_pass_io<8>(src, sink, M, Ns, mg, nseq, tw); break;
+    case 9: stockham_pass_io<9>(src, sink, M, Ns, mg, nseq, tw); break;
+    case 10: stockham_pass_io<10>(src, sink, M, Ns, mg, nseq, tw); break;
+    default: stockham_pass_io<16>(src, sink, M, Ns, mg, nseq, tw); break;
+  }
+}
+
 // Forward DFTs of the `nseq` length-M sequences in `a` (shared memory), `b` as scratch; returns the
 // buffer holding the transforms in natural order.  Every thread of the block must call it.
 __device__ __forceinline__ double2* fft_block(double2* a, double2* b, int nseq, const Fft& f) {
@@ -549,11 +590,34 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(Rs
     }
   }
   __syncthreads();
-  const double2* z = fft_block(a, b, nseq, k.f);
-  for (int e = 0; e < nseq; ++e) {
-    double* Fe = k.F + ((static_cast<int64_t>(s) * NA + m0 + e) * k.ny + j) * k.nx;
-    const double* zd = reinterpret_cast<const double*>(z + e * M);
-    for (int i = threadIdx.x; i < k.nx; i += blockDim.x) Fe[i] = (i & 1) ? -zd[i] : zd[i];
+  // the passes; the last one writes the row's samples straight out: element n is samples 2n (real part)
+  // and 2n + 1 (minus the imaginary part), with no shared-memory round trip or barrier after it
+  double* Fb = k.F + ((static_cast<int64_t>(s) * NA + m0) * k.ny + j) * k.nx;
+  const int64_t fstride = static_cast<int64_t>(k.ny) * k.nx;  // between quantities
+  const int nx = k.nx;
+  auto to_row = [Fb, fstride, nx](int e, int n, double2 z) {
+    double* Fe = Fb + e * fstride;
+    if (2 * n < nx) Fe[2 * n] = z.x;
+    if (2 * n + 1 < nx) Fe[2 * n + 1] = -z.y;
+  };
+  const int np = k.f.nrad;
+  int Ns = 1;
+  for (int pass = 0; pass < np; ++pass) {
+    const int R = k.f.rad[pass];
+    const unsigned mg = k.f.magic[pass];
+    const double2* src = a;
+    auto from_smem = [src, M](int e, int n) { return src[e * M + n]; };
+    if (pass == np - 1) {
+      pass_io(R, from_smem, to_row, M, Ns, mg, nseq, k.f.tw);
+    } else {
+      double2* dst = b;
+      pass_io(R, from_smem, [dst, M](int e, int n, double2 v) { dst[e * M + n] = v; }, M, Ns, mg, nseq, k.f.tw);
+      __syncthreads();
+      double2* t = a;
+      a = b;
+      b = t;
+    }
+    Ns *= R;
   }
 }
 
@@ -616,7 +680,8 @@ int rs_smem_attr(const void* kernel) {
 }
 
 template <int MODE, int NF, bool DEF>
-int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsShare& share, cudaStream_t st) {
+int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsShare& share, bool leave_raw,
+                cudaStream_t st) {
   using C = Cfg<MODE, NF, DEF>;
   constexpr int NA = C::NA;
   constexpr int NC = (NA + kRsSeq - 1) / kRsSeq;
@@ -685,7 +750,7 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
     rc = launch_banded_nonfinite(p, MODE, NF, a.planes, a.pitch, static_cast<int>(a.slice_stride / a.plane_stride),
                                  a.nslices, a.mask, a.mask_stride, partials, none, st, scratch);
   }
-  if (rc == CGEF_OK) {
+  if (rc == CGEF_OK && !leave_raw) {
     rs_finish_kernel<MODE, NF, DEF><<<dim3((p->nx + 127) / 128, p->ny, a.nslices), 128, 0, st>>>(a, scratch);
     rc = rs_check("rs_finish_kernel");
   }
@@ -695,9 +760,9 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
 
 template <int MODE, int NF>
 int dispatch_rowspec(bool def, const cgef_plan* p, const BandedK& a, double* scratch, const RsShare& share,
-                     cudaStream_t st) {
-  return def ? run_rowspec<MODE, NF, true>(p, a, scratch, share, st)
-             : run_rowspec<MODE, NF, false>(p, a, scratch, share, st);
+                     bool leave_raw, cudaStream_t st) {
+  return def ? run_rowspec<MODE, NF, true>(p, a, scratch, share, leave_raw, st)
+             : run_rowspec<MODE, NF, false>(p, a, scratch, share, leave_raw, st);
 }
 
 // Radices of a Stockham plan for M with few passes (tens, nines, then sixteens, eights, fours), or
@@ -734,18 +799,19 @@ int smooth_length(int n) {
 
 int launch_rowspec(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                    const uint8_t* mask, int64_t mask_slice_stride, double* scratch, const GatherOut& out,
-                   cudaStream_t st, const RsShare& share) {
+                   cudaStream_t st, const RsShare& share, bool leave_raw) {
   if (!p->rs_on || p->d_rs_k == nullptr) return fail(CGEF_EINVAL, "row-spectral evaluation not built for this plan");
   if (scratch == nullptr) return fail(CGEF_EINVAL, "row-spectral evaluation needs its scratch buffer");
   const bool def = p->strategy == CGEF_DEFORMABLE;
   const BandedK a = make_banded_args(p, mode, planes, pitch, np, nbatch, mask, mask_slice_stride, out);
-  if (mode == kModePiSphere) return dispatch_rowspec<kModePiSphere, 1>(def, p, a, scratch, share, st);
-  if (mode == kModePiCart) return dispatch_rowspec<kModePiCart, 1>(def, p, a, scratch, share, st);
+  const bool raw = leave_raw && mode != kModeFields;
+  if (mode == kModePiSphere) return dispatch_rowspec<kModePiSphere, 1>(def, p, a, scratch, share, raw, st);
+  if (mode == kModePiCart) return dispatch_rowspec<kModePiCart, 1>(def, p, a, scratch, share, raw, st);
   switch (nf) {
-    case 1: return dispatch_rowspec<kModeFields, 1>(def, p, a, scratch, share, st);
-    case 2: return dispatch_rowspec<kModeFields, 2>(def, p, a, scratch, share, st);
-    case 3: return dispatch_rowspec<kModeFields, 3>(def, p, a, scratch, share, st);
-    case 4: return dispatch_rowspec<kModeFields, 4>(def, p, a, scratch, share, st);
+    case 1: return dispatch_rowspec<kModeFields, 1>(def, p, a, scratch, share, raw, st);
+    case 2: return dispatch_rowspec<kModeFields, 2>(def, p, a, scratch, share, raw, st);
+    case 3: return dispatch_rowspec<kModeFields, 3>(def, p, a, scratch, share, raw, st);
+    case 4: return dispatch_rowspec<kModeFields, 4>(def, p, a, scratch, share, raw, st);
     default: return fail(CGEF_EINVAL, "row-spectral: 1..4 fields per pass");
   }
 }
