@@ -571,7 +571,7 @@ int32_t cgef_plan_destroy(cgef_plan* p) {
     void* ptrs[] = {p->d_mask, p->d_x, p->d_sinlam, p->d_coslam, p->d_sinphi, p->d_cosphi, p->d_area, p->d_xscale,
                     p->d_tanfac, p->d_rows, p->d_w, p->d_den_zf, p->sched[0].d_items, p->sched[0].d_groups,
                     p->sched[1].d_items, p->sched[1].d_groups, p->d_gx, p->d_gy, p->d_px, p->d_py, p->d_xe,
-                    p->d_prefix_wx, p->d_prows, p->d_queue, p->d_rs_tw, p->d_rs_k};
+                    p->d_prefix_wx, p->d_prows, p->d_queue, p->d_rs_tw, p->d_rs_k, p->d_rs_ptw};
     for (void* q : ptrs)
       if (q) cudaFree(q);
     for (auto& b : p->ws)

@@ -152,6 +152,8 @@ struct cgef_plan {
   int rs_rad[16] = {};          // their radices (2, 3, 4 or 5)
   double* d_rs_tw = nullptr;    // rs_L twiddles exp(-2 pi i n / rs_L), (re, im) pairs
   double* d_rs_k = nullptr;     // kernel spectra / rs_L: [band][row offset][bin < rs_nkp], zero past rs_nk
+  double* d_rs_ptw = nullptr;   // per-pass twiddles, pass p at rs_poff[p] (complex), [r - 1][jm]
+  int rs_poff[16] = {};
   bool rs_on = false;           // full-grid banded launches use the row-spectral evaluation
   // separable engine
   int di_lim = 0, sep_dj_lim = 0;

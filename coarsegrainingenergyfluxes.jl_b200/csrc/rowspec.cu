@@ -65,6 +65,10 @@ struct Fft {
   int rad[16];
   unsigned magic[16];  // ceil(2^32 / Ns) of each pass, Ns = the product of the earlier radices
   const double2* tw;   // exp(-2 pi i n / L), n < L; the length-M roots are every second entry
+  // per-pass twiddles, pass p at ptw + poff[p], laid out [r - 1][jm] (r < R, jm < Ns): the entry of tw
+  // that the pass multiplies element r of butterfly jm by, so a warp's loads are contiguous
+  const double2* ptw;
+  int poff[16];
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -212,9 +216,8 @@ __device__ __forceinline__ void dft(double2 (&v)[R]) {
 // does a pass in one round.
 template <int R>
 __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int M, int Ns, unsigned ns_magic,
-                                              int nseq, const double2* tw) {
+                                              int nseq, const double2* ptw) {
   const int nb = M / R;
-  const int tstride = 2 * (M / (Ns * R));  // the length-M roots are every second table entry
   for (int t = threadIdx.x; t < nseq * nb; t += blockDim.x) {
     int sq = 0, j = t;
 #pragma unroll
@@ -227,7 +230,7 @@ __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int 
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = as[j + r * nb];
 #pragma unroll
-    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + jm * tstride * r));
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(ptw + (r - 1) * Ns + jm));
     dft<R>(v);
     double2* bs = b + sq * M + jq * Ns * R + jm;
 #pragma unroll
@@ -240,9 +243,8 @@ __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int 
 // straight out as real samples, so that pass needs no shared-memory round trip and no barrier after it.
 template <int R, typename Src, typename Sink>
 __device__ __forceinline__ void stockham_pass_io(Src src, Sink sink, int M, int Ns, unsigned ns_magic, int nseq,
-                                                 const double2* tw) {
+                                                 const double2* ptw) {
   const int nb = M / R;
-  const int tstride = 2 * (M / (Ns * R));
   for (int t = threadIdx.x; t < nseq * nb; t += blockDim.x) {
     int sq = 0, j = t;
 #pragma unroll
@@ -254,7 +256,7 @@ __device__ __forceinline__ void stockham_pass_io(Src src, Sink sink, int M, int 
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src(sq, j + r * nb);
 #pragma unroll
-    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tw + jm * tstride * r));
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(ptw + (r - 1) * Ns + jm));
     dft<R>(v);
 #pragma unroll
     for (int r = 0; r < R; ++r) sink(sq, jq * Ns * R + jm + r * Ns, v[r]);
@@ -263,16 +265,16 @@ __device__ __forceinline__ void stockham_pass_io(Src src, Sink sink, int M, int 
 
 template <typename Src, typename Sink>
 __device__ __forceinline__ void pass_io(int R, Src src, Sink sink, int M, int Ns, unsigned mg, int nseq,
-                                        const double2* tw) {
+                                        const double2* ptw) {
   switch (R) {
-    case 2: stockham_pass_io<2>(src, sink, M, Ns, mg, nseq, tw); break;
-    case 3: stockham_pass_io<3>(src, sink, M, Ns, mg, nseq, tw); break;
-    case 4: stockham_pass_io<4>(src, sink, M, Ns, mg, nseq, tw); break;
-    case 5: stockham_pass_io<5>(src, sink, M, Ns, mg, nseq, tw); break;
-    case 8: stockham_pass_io<8>(src, sink, M, Ns, mg, nseq, tw); break;
-    case 9: stockham_pass_io<9>(src, sink, M, Ns, mg, nseq, tw); break;
-    case 10: stockham_pass_io<10>(src, sink, M, Ns, mg, nseq, tw); break;
-    default: stockham_pass_io<16>(src, sink, M, Ns, mg, nseq, tw); break;
+    case 2: stockham_pass_io<2>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 3: stockham_pass_io<3>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 4: stockham_pass_io<4>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 5: stockham_pass_io<5>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 8: stockham_pass_io<8>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 9: stockham_pass_io<9>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 10: stockham_pass_io<10>(src, sink, M, Ns, mg, nseq, ptw); break;
+    default: stockham_pass_io<16>(src, sink, M, Ns, mg, nseq, ptw); break;
   }
 }
 
@@ -283,15 +285,16 @@ __device__ __forceinline__ double2* fft_block(double2* a, double2* b, int nseq, 
   for (int p = 0; p < f.nrad; ++p) {
     const int R = f.rad[p];
     const unsigned mg = f.magic[p];
+    const double2* tp = f.ptw + f.poff[p];
     switch (R) {
-      case 2: stockham_pass<2>(a, b, f.M, Ns, mg, nseq, f.tw); break;
-      case 3: stockham_pass<3>(a, b, f.M, Ns, mg, nseq, f.tw); break;
-      case 4: stockham_pass<4>(a, b, f.M, Ns, mg, nseq, f.tw); break;
-      case 5: stockham_pass<5>(a, b, f.M, Ns, mg, nseq, f.tw); break;
-      case 8: stockham_pass<8>(a, b, f.M, Ns, mg, nseq, f.tw); break;
-      case 9: stockham_pass<9>(a, b, f.M, Ns, mg, nseq, f.tw); break;
-      case 10: stockham_pass<10>(a, b, f.M, Ns, mg, nseq, f.tw); break;
-      default: stockham_pass<16>(a, b, f.M, Ns, mg, nseq, f.tw); break;
+      case 2: stockham_pass<2>(a, b, f.M, Ns, mg, nseq, tp); break;
+      case 3: stockham_pass<3>(a, b, f.M, Ns, mg, nseq, tp); break;
+      case 4: stockham_pass<4>(a, b, f.M, Ns, mg, nseq, tp); break;
+      case 5: stockham_pass<5>(a, b, f.M, Ns, mg, nseq, tp); break;
+      case 8: stockham_pass<8>(a, b, f.M, Ns, mg, nseq, tp); break;
+      case 9: stockham_pass<9>(a, b, f.M, Ns, mg, nseq, tp); break;
+      case 10: stockham_pass<10>(a, b, f.M, Ns, mg, nseq, tp); break;
+      default: stockham_pass<16>(a, b, f.M, Ns, mg, nseq, tp); break;
     }
     __syncthreads();
     double2* t = a;
@@ -608,10 +611,11 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(Rs
     const double2* src = a;
     auto from_smem = [src, M](int e, int n) { return src[e * M + n]; };
     if (pass == np - 1) {
-      pass_io(R, from_smem, to_row, M, Ns, mg, nseq, k.f.tw);
+      pass_io(R, from_smem, to_row, M, Ns, mg, nseq, k.f.ptw + k.f.poff[pass]);
     } else {
       double2* dst = b;
-      pass_io(R, from_smem, [dst, M](int e, int n, double2 v) { dst[e * M + n] = v; }, M, Ns, mg, nseq, k.f.tw);
+      pass_io(R, from_smem, [dst, M](int e, int n, double2 v) { dst[e * M + n] = v; }, M, Ns, mg, nseq,
+              k.f.ptw + k.f.poff[pass]);
       __syncthreads();
       double2* t = a;
       a = b;
@@ -697,6 +701,8 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
     ns *= p->rs_rad[i];
   }
   k.f.tw = reinterpret_cast<const double2*>(p->d_rs_tw);
+  k.f.ptw = reinterpret_cast<const double2*>(p->d_rs_ptw);
+  for (int i = 0; i < p->rs_nrad; ++i) k.f.poff[i] = p->rs_poff[i];
   k.planes = a.planes;
   k.plane_stride = a.plane_stride;
   k.slice_stride = a.slice_stride;
@@ -842,11 +848,34 @@ int build_row_spectra(cgef_plan* p) {
     tw[2 * n] = std::cos(ang);
     tw[2 * n + 1] = -std::sin(ang);
   }
+  // per-pass twiddles of the half-length transform: pass p (Ns = the product of the earlier radices)
+  // multiplies element r of butterfly jm by exp(-2 pi i jm r / (Ns R)), entry jm r L / (Ns R) of tw
+  std::vector<double> ptw;
+  int poff[16] = {};
+  {
+    int ns = 1;
+    for (size_t q = 0; q < rad.size(); ++q) {
+      const int R = rad[q];
+      poff[q] = static_cast<int>(ptw.size() / 2);
+      for (int r = 1; r < R; ++r)
+        for (int jm = 0; jm < ns; ++jm) {
+          const int64_t n = static_cast<int64_t>(jm) * r * L / (static_cast<int64_t>(ns) * R);
+          ptw.push_back(tw[2 * n]);
+          ptw.push_back(tw[2 * n + 1]);
+        }
+      ns *= R;
+    }
+  }
   DeviceGuard dg(p->device);
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p->d_rs_tw), tw.size() * sizeof(double));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(row-spectral twiddles)");
   e = cudaMemcpy(p->d_rs_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(row-spectral twiddles)");
+  e = cudaMalloc(reinterpret_cast<void**>(&p->d_rs_ptw), std::max<size_t>(ptw.size(), 2) * sizeof(double));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(row-spectral pass twiddles)");
+  e = cudaMemcpy(p->d_rs_ptw, ptw.data(), ptw.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(row-spectral pass twiddles)");
+  for (size_t q = 0; q < rad.size(); ++q) p->rs_poff[q] = poff[q];
   e = cudaMalloc(reinterpret_cast<void**>(&p->d_rs_k), kbytes);
   if (e == cudaErrorMemoryAllocation) {
     // no room for the kernel spectra: the plan keeps the direct gather only
@@ -854,6 +883,8 @@ int build_row_spectra(cgef_plan* p) {
     p->d_rs_k = nullptr;
     cudaFree(p->d_rs_tw);
     p->d_rs_tw = nullptr;
+    cudaFree(p->d_rs_ptw);
+    p->d_rs_ptw = nullptr;
     return CGEF_OK;
   }
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(row-spectral kernel spectra)");
