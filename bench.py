@@ -7,6 +7,8 @@ Gaussian alpha = 4, l = 100 km, ZeroFill, ~30% land -- one scale x one snapshot 
   sweep24x8 : 24 scales (50-2000 km, log-spaced) x 8 snapshots per step, Pi and E(l)
   cart256   : 256^2 doubly periodic Cartesian, dx = 1 km, l = 8 km (separable engine)
   levels40  : regional 400 x 600 x 40 levels, FP32 storage, 6 scales 25-400 km, one mask per level
+  tophat    : the sphere1 grid and mask with the package's default kernel, the exact top-hat at
+              l = 100 km (the prefix-sum engine)
   closure8  : the learned closure: trained on exact-path pairs of two snapshots at 8 scales
               (50-1000 km, 10^7 points), then Pi of a fresh snapshot at the 8 scales by the closure
               (2% of tiles judged exactly, per-slice fallback above the tolerance) against the plain
@@ -14,9 +16,9 @@ Gaussian alpha = 4, l = 100 km, ZeroFill, ~30% land -- one scale x one snapshot 
 
 `value` times the device-resident path (inputs already in HBM, an L2 flush between steps inside
 the timed region); `e2e` times the host C-ABI call (pinned host inputs copied in, Pi copied out)
-every step.  The default run (sphere1, one rank) adds two sub-records to its line, the metric's
-"plain vs batched/closure": `batched` (the sweep24x8 workload, measured the same way) and `closure`
-(the closure8 workload).  `--impl reference` times the CPU FP64 oracle -- the restated threaded
+every step.  The default run (sphere1, one rank) adds sub-records to its line: the metric's "plain vs
+batched/closure" -- `batched` (the sweep24x8 workload, measured the same way) and `closure` (the
+closure8 workload) -- and `tophat` (the tophat workload).  `--impl reference` times the CPU FP64 oracle -- the restated threaded
 reference path -- on the host's cores instead, with the same `config`.
 """
 from __future__ import annotations
@@ -45,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sphere1", choices=["sphere1", "sweep24x8", "cart256", "levels40", "closure8"])
+    ap.add_argument("--workload", default="sphere1", choices=["sphere1", "sweep24x8", "cart256", "levels40", "closure8", "tophat"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--snapshots", type=int, default=1, help="snapshots per step of the sphere1 workload")
@@ -58,8 +60,8 @@ def parse():
                     help="footprint sums of the banded engine: the autotuner's choice per scale (default), the "
                          "direct gather, or the row-spectral evaluation")
     ap.add_argument("--no-subrecords", action="store_true",
-                    help="sphere1: time the headline only, without the batched (24 scales x 8 snapshots) and "
-                         "closure sub-records")
+                    help="sphere1: time the headline only, without the batched (24 scales x 8 snapshots), "
+                         "closure and top-hat sub-records")
     ap.add_argument("--batched-steps", type=int, default=6, help="timed steps of the batched sub-record")
     ap.add_argument("--clocks-out", default=None,
                     help="directory for the nvidia-smi clock samples (default: a temporary directory)")
@@ -99,6 +101,12 @@ def make_workload(name: str, rank: int, snapshots: int = 1, scale_km=None):
                     kernel=cg.GaussianKernel(4.0),
                     desc="sphere-0.25deg-1440x720-gauss-a4-24scales-50to2000km-x8snapshots-zerofill-30pct-land",
                     dtype="f64")
+    if name == "tophat":
+        g = S.sphere_grid()
+        g = g.with_mask(S.land_mask(g, seed=1))
+        u, v = S.sphere_fields(g, seed=100 + rank)
+        return dict(grid=g, u=u[None], v=v[None], scales=[1e5], slice_masks=None, kernel=cg.TopHatKernel(),
+                    desc="sphere-0.25deg-1440x720-tophat-l100km-zerofill-30pct-land", dtype="f64")
     if name == "cart256":
         g = S.cartesian_grid()
         u, v = S.cartesian_fields(seed=rank)
@@ -164,6 +172,16 @@ def rowspec_bytes(p, grid, nslices, na, nplanes, nout, masked) -> float:
     spec = nslices * grid.ny * na * nk * 16
     return float(nslices * nplanes * N * 8 + 4 * spec + nrows * nk * 8 + 2 * nslices * na * N * 8
                  + nslices * nout * N * 8 + (nslices * N if masked else 0))
+
+
+def prefix_bytes(p, grid, nslices, na, nplanes, nout, masked) -> float:
+    """Compulsory DRAM bytes of one prefix-sum launch: the staged planes read, the prefix sums of every
+    quantity along the tripled (periodic) or single row written once and read once, the outputs
+    written (and the mask read)."""
+    N = grid.nx * grid.ny
+    ne = (3 if grid.periodic[0] else 1) * grid.nx
+    P = nslices * na * grid.ny * (ne + 1) * 8
+    return float(nslices * nplanes * N * 8 + 2 * P + nslices * nout * N * 8 + (nslices * N if masked else 0))
 
 
 def committed_traffic(key: str, nsl: int, scale_km=None):
@@ -275,7 +293,8 @@ def oracle_rate(wl, budget_s: float):
     nthreads = O.max_threads()
     nsl = wl["u"].shape[0]
     scales = list(wl["scales"])
-    alpha = wl["kernel"].alpha
+    alpha = float(getattr(wl["kernel"], "alpha", 0.0))
+    okernel = O.GAUSSIAN if alpha > 0 else O.TOPHAT
     masks = wl["slice_masks"]
 
     def ogrid(mask):
@@ -289,7 +308,7 @@ def oracle_rate(wl, budget_s: float):
         m = mask_of(t)
         return float(g.nx * g.ny if m is None else np.count_nonzero(m))
 
-    entries = [float(O.count_entries(ogrid(None), O.GAUSSIAN, alpha, s)) for s in scales]
+    entries = [float(O.count_entries(ogrid(None), okernel, alpha, s)) for s in scales]
     cost = lambda t, s: active(t) * entries[s]
     # subset: scales spread over the range whose estimated time fits the budget
     order = sorted(range(len(scales)), key=lambda s: entries[s])
@@ -300,7 +319,7 @@ def oracle_rate(wl, budget_s: float):
     def run(t, s):
         key = (t if masks is not None else -1, s)
         if key not in plans:
-            plans[key] = O.Plan(ogrid(mask_of(t)), O.GAUSSIAN, alpha, scales[s], O.ZEROFILL)
+            plans[key] = O.Plan(ogrid(mask_of(t)), okernel, alpha, scales[s], O.ZEROFILL)
         p = plans[key]
         u = np.asarray(wl["u"][t], dtype=np.float64)
         v = np.asarray(wl["v"][t], dtype=np.float64)
@@ -756,7 +775,23 @@ def measure_sweep(args, name, rank, world, local, dist, *, snapshots=1, scale_km
     direct_plans = [p for p in plans if not uses_row_spectral(p)]
     flops_all = algorithmic_flops(plans, g, nsl, wl["slice_masks"])
     masked = g.mask is not None or wl["slice_masks"] is not None
-    if prof["rowspec"][0] >= prof["direct"][0] and spec_plans:
+    if plans[0].engine == "prefixsum":
+        tot, cnt = prof["direct"]
+        per_launch_ms = tot / max(cnt, 1)
+        launches_per_step = max(cnt // steps, 1)
+        na, npl = (9, 3) if g.is_spherical else (5, 2)
+        if isinstance(plans[0].strategy, cg.Deformable):
+            na, npl = na + 1, npl + 1
+        bytes_launch = sum(prefix_bytes(p, g, nsl, na, npl, 5, masked) for p in plans) / launches_per_step
+        peak, peak_source = hbm_peak()
+        achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "traffic_basis": "no capture of this workload",
+                    "kernel": "prefix_scan_kernel + prefix_sweep_kernel (exact top-hat: per-row prefix sums over the "
+                              "tripled periodic row, then interval differences per target and row offset)",
+                    "per_launch_ms": per_launch_ms, "launches": cnt, "algorithmic_bytes_per_launch": bytes_launch,
+                    "peak_source": peak_source}
+    elif prof["rowspec"][0] >= prof["direct"][0] and spec_plans:
         tot, cnt = prof["rowspec"]
         per_launch_ms = tot / max(cnt, 1)
         launches_per_step = max(cnt // steps, 1)
@@ -949,6 +984,9 @@ def main():
             b["speedup_vs_plain"] = b["value"] / line["value"]
             line["batched"] = b
             line["closure"] = run_closure(args, rank, world, local, dist, steps=3)
+            # the package's default kernel (Pipeline.jl:344) on the same grid: the exact top-hat
+            line["tophat"] = measure_sweep(args, "tophat", rank, world, local, dist, steps=50, e2e_steps=20,
+                                           cpu_budget=15.0)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

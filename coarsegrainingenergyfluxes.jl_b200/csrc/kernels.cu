@@ -536,34 +536,68 @@ struct PreK {
   const double* cosphi;
 };
 
-// One thread per (slice, quantity, row): the reference's sequential running sum, in its order
-// (prefixsum_fill_numerator_row!, Filtering.jl:894-907).
+// One block per (slice, row) computes every quantity's running sum along the (tripled, for a periodic
+// axis) row (prefixsum_fill_numerator_row!, Filtering.jl:894-907): the row's staged values are read into
+// shared memory once (when they fit), and warp m scans quantity m -- each chunk of 32 columns forms the
+// quantity of its cells (once per cell), takes a warp-wide inclusive scan of the terms (shuffles), adds the
+// carried sum of the chunks before it and stores the 32 prefix values from consecutive lanes.  The terms
+// and their order along the row are the reference's; only the grouping of the additions differs, so the
+// sums agree with its sequential running sum to FP64 rounding.
 template <int MODE, int NF, bool DEF>
-__global__ void prefix_scan_kernel(PreK a) {
+__global__ void __launch_bounds__(320) prefix_scan_kernel(PreK a, int row_in_smem) {
   using C = Cfg<MODE, NF, DEF>;
-  const int64_t gid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int64_t total = static_cast<int64_t>(a.nslices) * C::NA * a.ny;
-  if (gid >= total) return;
-  const int j = static_cast<int>(gid % a.ny);
-  const int m = static_cast<int>((gid / a.ny) % C::NA);
-  const int s = static_cast<int>(gid / (static_cast<int64_t>(a.ny) * C::NA));
-  const double* row = a.planes + s * a.slice_stride + static_cast<int64_t>(j) * a.pitch + a.halo;
+  extern __shared__ double pre_row[];
+  const int lane = threadIdx.x & 31;
+  const int m = threadIdx.x >> 5;  // the warp's quantity
+  const int j = blockIdx.x;
+  const int s = blockIdx.y;
+  const double* grow = a.planes + s * a.slice_stride + static_cast<int64_t>(j) * a.pitch + a.halo;
+  const double* row = grow;
+  int64_t pstride = a.plane_stride;
+  if (row_in_smem) {
+    for (int t = threadIdx.x; t < C::NP * a.nx; t += blockDim.x) {
+      const int pl = t / a.nx, i = t - pl * a.nx;
+      pre_row[t] = grow[pl * a.plane_stride + i];
+    }
+    __syncthreads();
+    row = pre_row;
+    pstride = a.nx;
+  }
+  if (m >= C::NA) return;
   double* P = a.P + s * a.P_slice + m * a.P_plane + static_cast<int64_t>(j) * (a.ne + 1);
-  double acc = 0.0;
-  P[0] = 0.0;
-  for (int k = 0; k < a.ne; ++k) {
-    const int i = k % a.nx;
-    double v[C::NP];
+  if (lane == 0) P[0] = 0.0;
+  // kChunks chunks of 32 columns per iteration: their scans are independent, only the carry chains them
+  constexpr int kChunks = 4;
+  double carry = 0.0;
+  for (int k0 = 0; k0 < a.ne; k0 += 32 * kChunks) {
+    double x[kChunks];
 #pragma unroll
-    for (int pl = 0; pl < C::NP; ++pl) v[pl] = row[pl * a.plane_stride + i];
-    double q[C::NA];
-    expand<MODE, NF, DEF>(v, q);
-    double qm = 0.0;
+    for (int c = 0; c < kChunks; ++c) {
+      const int k = k0 + 32 * c + lane;
+      x[c] = 0.0;
+      if (k < a.ne) {
+        const int i = k % a.nx;
+        double v[C::NP];
 #pragma unroll
-    for (int mm = 0; mm < C::NA; ++mm)
-      if (mm == m) qm = q[mm];
-    acc = acc + qm * a.wx;
-    P[k + 1] = acc;
+        for (int pl = 0; pl < C::NP; ++pl) v[pl] = row[pl * pstride + i];
+        x[c] = quantity<MODE, NF, DEF>(v, m) * a.wx;
+      }
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+      for (int c = 0; c < kChunks; ++c) {
+        const double y = __shfl_up_sync(0xffffffffu, x[c], d);
+        if (lane >= d) x[c] = x[c] + y;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kChunks; ++c) {
+      const int k = k0 + 32 * c + lane;
+      x[c] = carry + x[c];
+      if (k < a.ne) P[k + 1] = x[c];
+      carry = __shfl_sync(0xffffffffu, x[c], 31);
+    }
   }
 }
 
@@ -1463,9 +1497,22 @@ namespace {
 template <int MODE, int NF, bool DEF>
 int run_prefix(const PreK& a, int nbatch, int nx, int ny, cudaStream_t st) {
   using C = Cfg<MODE, NF, DEF>;
-  const int64_t nthreads = static_cast<int64_t>(C::NA) * ny * nbatch;
+  // the row's staged values in shared memory when they fit (opted in once per device up to 200 KB)
+  const size_t row_bytes = sizeof(double) * C::NP * static_cast<size_t>(nx);
+  const bool in_smem = row_bytes <= (size_t(200) << 10);
+  if (in_smem && row_bytes > (size_t(48) << 10)) {
+    static int opted[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+    if (!opted[dev]) {
+      cudaError_t e = cudaFuncSetAttribute(prefix_scan_kernel<MODE, NF, DEF>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(prefix_scan_kernel)");
+      opted[dev] = 1;
+    }
+  }
   prof_begin(CGEF_KERNEL_PREFIX, st);
-  prefix_scan_kernel<MODE, NF, DEF><<<static_cast<unsigned>((nthreads + 127) / 128), 128, 0, st>>>(a);
+  prefix_scan_kernel<MODE, NF, DEF><<<dim3(ny, nbatch), 32 * C::NA, in_smem ? row_bytes : 0, st>>>(a, in_smem ? 1 : 0);
   int rc = check_launch("prefix_scan_kernel");
   if (rc) return rc;
   dim3 block(128), grid((nx + 127) / 128, ny, nbatch);

@@ -316,40 +316,6 @@ struct RsK {
   double* F;            // [slice][m][row][nx] (aliases Q once the sums are formed)
 };
 
-// Accumulated quantity m of one source cell (the order of expand()): the fields, then (flux modes)
-// their pairwise products, then the mask.
-template <int MODE, int NF, bool DEF>
-__device__ __forceinline__ double quantity(const double (&v)[Cfg<MODE, NF, DEF>::NP], int m) {
-  using C = Cfg<MODE, NF, DEF>;
-  if (DEF && m == C::NA - 1) return v[C::NP - 1];
-  if constexpr (MODE == kModePiSphere) {
-    switch (m) {
-      case 0: return v[0];
-      case 1: return v[1];
-      case 2: return v[2];
-      case 3: return v[0] * v[0];
-      case 4: return v[0] * v[1];
-      case 5: return v[0] * v[2];
-      case 6: return v[1] * v[1];
-      case 7: return v[1] * v[2];
-      default: return v[2] * v[2];
-    }
-  } else if constexpr (MODE == kModePiCart) {
-    switch (m) {
-      case 0: return v[0];
-      case 1: return v[1];
-      case 2: return v[0] * v[0];
-      case 3: return v[0] * v[1];
-      default: return v[1] * v[1];
-    }
-  } else {
-    double r = v[0];
-#pragma unroll
-    for (int f = 1; f < NF; ++f)
-      if (m == f) r = v[f];
-    return r;
-  }
-}
 
 // Real DFTs of up to kRsSeq of the NA accumulated quantities of one source row (slice, row): each
 // row's even and odd samples form one half-length complex sequence z, and with Z = FFT(z) the row's

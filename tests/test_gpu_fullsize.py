@@ -127,3 +127,30 @@ def test_c3_regional_levels_full_shape_fp32(c1):
             sel[rows_cmp] = M[k][rows_cmp]
             err = rel_l2(res[q].Pi[si], ref["Pi"], sel)
             assert err < PI_FP32, (k, s, err)
+
+
+@pytest.mark.parametrize("strat", [cg.ZeroFill(), cg.Deformable()])
+def test_c1_tophat_full_size_matches_oracle(c1, strat):
+    """The package's default kernel on the C1 sphere: the exact top-hat (l = 100 km) by per-row prefix
+    sums, the scan taken by warps in 32-column chunks, against the oracle's sequential running sums
+    (Filtering.jl:894-1078) over every cell.
+
+    The method itself is ill-conditioned in FP64, whoever sums: an interval's sum is the difference of
+    two running sums over the tripled 4320-cell row (the row's magnitude over the window's, ~1e3), and
+    tau = (uu)bar - ubar ubar cancels another ~1e3 on this field.  Two summation orders of the same
+    terms therefore differ by ~1e-13 in ubar but ~1e-10 in tau and ~1e-9 in Pi (Deformable adds the
+    mask's running sum to the denominator).  The bounds are those, with a margin: four orders inside
+    the path's 1e-5 contract for Pi."""
+    g, u, v = c1
+    k = cg.TopHatKernel()
+    plan = cg.plan_filter(g, k, 1e5, mask_strategy=strat)
+    assert plan.engine == "prefixsum"
+    r = cg.compute_Pi_fields(u, v, g, k, 1e5, filter_plan=plan, mask_strategy=strat)
+    st = O.DEFORMABLE if isinstance(strat, cg.Deformable) else O.ZEROFILL
+    ref = O.Plan(oracle_grid(g), O.TOPHAT, 0.0, 1e5, st).compute_pi(u, v, NTH)
+    errs = {key: rel_l2(r[key], ref[key], g.mask) for key in ("Pi", "ubar", "vbar", "tau_xx", "tau_xy", "tau_yy")}
+    assert errs["Pi"] < 1e-8, errs
+    for key in ("ubar", "vbar"):
+        assert errs[key] < 1e-12, errs
+    for key in ("tau_xx", "tau_xy", "tau_yy"):
+        assert errs[key] < 2e-9, errs
