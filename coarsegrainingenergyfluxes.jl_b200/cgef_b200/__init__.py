@@ -12,7 +12,8 @@ from .diagnostics import (AbstractSpectrumPolicy, ForceSpectrum, NoSpectrum, Str
                           gate_spectrum, spectral_density, tau_decomposition)
 from .errors import ArgumentError, DimensionMismatch
 from .filtering import (AbstractMaskStrategy, Deformable, PhysicalFilterPlan, ZeroFill, filter_apply,
-                        filter_apply_batch, filter_apply_batched, filter_field, filter_fields, plan_filter)
+                        filter_apply_batch, filter_apply_batched, filter_field, filter_fields, plan_filter,
+                        set_footprint_build)
 from .grids import Axis, CartesianGeometry, SphericalGeometry, StructuredGrid, axis
 from .kernels import (GaussianKernel, TopHatKernel, check_spectrum_kernel, kernel_radius, kernel_weight,
                       transfer_monotone)

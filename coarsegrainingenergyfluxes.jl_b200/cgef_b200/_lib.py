@@ -20,6 +20,7 @@ CGEF_EUNSUPPORTED = -5
 CGEF_ENODEVICE = -6
 CGEF_ETIMEOUT = -7
 INJECT_CLOSURE_TIMEOUT, INJECT_STALE_QUEUE = 1, 2
+BUILD_AUTO, BUILD_HOST, BUILD_DEVICE = 0, 1, 2
 
 CARTESIAN, SPHERICAL = 0, 1
 TOPHAT, GAUSSIAN = 0, 1
@@ -42,6 +43,7 @@ EXPORTED = [
     "cgef_pipeline_create", "cgef_pipeline_submit", "cgef_pipeline_drain", "cgef_pipeline_destroy",
     "cgef_plan_set_filter_rows", "cgef_plan_get_schedule", "cgef_plan_set_row_spectral",
     "cgef_plan_get_row_spectral", "cgef_build_arch", "cgef_plan_reset_queue", "cgef_debug_inject",
+    "cgef_set_footprint_build", "cgef_plan_get_build",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE, KERNEL_ROWSPEC = (
     0, 1, 2, 3, 4, 5, 6)
@@ -122,6 +124,10 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_plan_reset_queue.restype = i32
     L.cgef_debug_inject.argtypes = [vp, i32]
     L.cgef_debug_inject.restype = i32
+    L.cgef_set_footprint_build.argtypes = [i32]
+    L.cgef_set_footprint_build.restype = i32
+    L.cgef_plan_get_build.argtypes = [vp, C.POINTER(i32)]
+    L.cgef_plan_get_build.restype = i32
     L.cgef_plan_create.argtypes = [C.POINTER(vp), C.POINTER(GridDesc), i32, dbl, dbl, i32, i32]
     L.cgef_plan_create.restype = i32
     L.cgef_plan_destroy.argtypes = [vp]

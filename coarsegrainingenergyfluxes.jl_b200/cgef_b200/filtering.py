@@ -133,6 +133,13 @@ class PhysicalFilterPlan:
         _lib.check(_lib.load().cgef_plan_set_row_spectral(self.handle, 1 if enable else 0))
 
     @property
+    def footprint_build(self) -> str:
+        """Where the plan's footprint weights were computed: "host" or "device" (set_footprint_build)."""
+        w = C.c_int32()
+        _lib.check(_lib.load().cgef_plan_get_build(self.handle, C.byref(w)))
+        return "device" if w.value == _lib.BUILD_DEVICE else "host"
+
+    @property
     def row_spectral(self):
         """(available, enabled, fft_length) of the row-spectral evaluation."""
         a, e, n = C.c_int32(), C.c_int32(), C.c_int32()
@@ -161,6 +168,16 @@ class PhysicalFilterPlan:
     def __repr__(self):
         return (f"PhysicalFilterPlan(engine={self.engine}, kernel={self.kernel!r}, scale={self.scale}, "
                 f"strategy={self.strategy!r})")
+
+
+def set_footprint_build(where: str = "auto") -> None:
+    """Where later plans build large spherical footprints: "auto" (the default: on the device from about
+    2e6 half-row weights), "host" or "device".  The entry set is decided on the host either way; see
+    cgef_set_footprint_build in include/cgef_b200.h."""
+    code = {"auto": _lib.BUILD_AUTO, "host": _lib.BUILD_HOST, "device": _lib.BUILD_DEVICE}.get(where)
+    if code is None:
+        raise ArgumentError("footprint build must be 'auto', 'host' or 'device'")
+    _lib.check(_lib.load().cgef_set_footprint_build(code))
 
 
 def plan_filter(grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,

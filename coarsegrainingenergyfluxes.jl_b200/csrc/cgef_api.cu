@@ -435,6 +435,14 @@ int32_t cgef_version(void) { return CGEF_ABI_VERSION; }
 
 int32_t cgef_build_arch(void) { return 1000; }  // every .cu file refuses any other device target
 
+int32_t cgef_set_footprint_build(int32_t where) { return set_footprint_build(where); }
+
+int32_t cgef_plan_get_build(const cgef_plan* p, int32_t* where) {
+  if (!p) return fail(CGEF_EINVAL, "plan is NULL");
+  if (where) *where = p->built_on_device ? CGEF_BUILD_DEVICE : CGEF_BUILD_HOST;
+  return CGEF_OK;
+}
+
 int32_t cgef_plan_reset_queue(cgef_plan* p) {
   int rc = check_plan(p);
   if (rc) return rc;
@@ -753,15 +761,26 @@ int32_t cgef_plan_get_footprint(const cgef_plan* p, int32_t* di, int32_t* dj, do
   if (p->engine != CGEF_ENGINE_BANDED) return fail(CGEF_EINVAL, "plan has no banded footprint");
   if (ptr) std::memcpy(ptr, p->h_ptr.data(), p->h_ptr.size() * sizeof(int64_t));
   if (di || dj || w) {
+    // a footprint built on the device keeps its weights there only: fetch them for this call
+    std::vector<double> fetched;
+    if (p->built_on_device) {
+      fetched.resize(static_cast<size_t>(std::max<int64_t>(p->nwhalf, 1)));
+      DeviceGuard dg(p->device);
+      cudaError_t e = cudaMemcpy(fetched.data(), p->d_w, sizeof(double) * p->nwhalf, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) return cuda_fail(e, "footprint weights");
+    }
     const int nb = static_cast<int>(p->h_ptr.size()) - 1;
     int64_t k = 0;
     for (int b = 0; b < nb; ++b)
-      for_each_entry(p, b, [&](int ddi, int ddj, double wv) {
-        if (di) di[k] = ddi;
-        if (dj) dj[k] = ddj;
-        if (w) w[k] = wv;
-        ++k;
-      });
+      for_each_entry(
+          p, b,
+          [&](int ddi, int ddj, double wv) {
+            if (di) di[k] = ddi;
+            if (dj) dj[k] = ddj;
+            if (w) w[k] = wv;
+            ++k;
+          },
+          p->built_on_device ? fetched.data() : nullptr);
   }
   return CGEF_OK;
 }

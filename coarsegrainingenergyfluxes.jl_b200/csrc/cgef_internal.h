@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "cgef_b200.h"
@@ -118,7 +119,9 @@ struct cgef_plan {
   // host tables kept for introspection
   std::vector<double> h_x, h_y;
   std::vector<cgef::BandRow> h_rows;  // banded: per (band, row offset) intervals
-  std::vector<double> h_whalf;        // banded: weights by |di|
+  std::vector<double> h_whalf;        // banded: weights by |di| (empty when built on the device)
+  int64_t nwhalf = 0;                 // banded: half-row weights (d_w's length)
+  bool built_on_device = false;       // banded: weights and denominators computed by device_band_tables
   std::vector<int64_t> h_ptr;         // banded: CSR band offsets of the reference's layout
   int64_t nentries = 0;
   int dj_lim = 0, di_max = 0;
@@ -184,6 +187,17 @@ double kernel_radius(int kernel, double alpha, double ell);
 
 // Host plan construction (plan_build.cpp).
 int build_plan_tables(cgef_plan* p);
+// Where later plans build large spherical footprints (CGEF_BUILD_*; process-wide).
+int set_footprint_build(int where);
+
+// Device part of a large spherical footprint build (plan_device.cu): with the plan's rows (a, hi, woff)
+// decided and uploaded (d_rows), computes the half-row weights into d_w (nweights) from the host's row
+// constants -- sdp = sin((phi' - phi) / 2), cc = cos(phi) cos(phi'), area = the row's cell measure, per
+// row -- and sdl[k] = sin(k dlambda / 2); copies the rows the host built itself (woff, weights) over
+// them; then the ZeroFill denominators per band into d_den_zf (periodic x).
+int device_band_tables(cgef_plan* p, const std::vector<double>& sdp, const std::vector<double>& cc,
+                       const std::vector<double>& area, const std::vector<double>& sdl, size_t nweights,
+                       const std::vector<std::pair<int64_t, std::vector<double>>>& host_rows);
 
 // Sets the closure's device error word from the host, as a bounded wait that ran out sets it
 // (cgef_debug_inject; closure.cu).
@@ -217,15 +231,16 @@ void subset_schedule(const cgef_plan* p, const std::vector<std::pair<int, int>>&
                      std::vector<WorkItem>& items, std::vector<SplitGroup>& groups, int& slots);
 
 // Visits band b's footprint entries in the reference's CSR order (row offset ascending, then
-// column offset ascending): f(ddi, ddj, w).
+// column offset ascending): f(ddi, ddj, w).  `whalf`: the half-row weights (default: the host copy).
 template <typename F>
-void for_each_entry(const cgef_plan* p, int b, F f) {
+void for_each_entry(const cgef_plan* p, int b, F f, const double* whalf = nullptr) {
+  const double* wh = whalf ? whalf : p->h_whalf.data();
   const int W = 2 * p->D + 1;
   for (int r = 0; r < W; ++r) {
     const BandRow& br = p->h_rows[static_cast<size_t>(b) * W + r];
     if (br.a < 0) continue;
     for (int di = -br.a; di <= br.hi; ++di) {
-      const double w = p->h_whalf[br.woff + (di < 0 ? -di : di)];
+      const double w = wh[br.woff + (di < 0 ? -di : di)];
       if (w != 0.0) f(di, r - p->D, w);
     }
   }

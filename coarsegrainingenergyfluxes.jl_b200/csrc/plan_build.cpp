@@ -233,7 +233,155 @@ int build_banded(const cgef_plan* p, Banded& B) {
   return CGEF_OK;
 }
 
+// Rows of the spherical banded footprint for the device build (device_band_tables): every inclusion
+// decided here with libm, the weights left to the device.  Per (band, row offset), h -- and so the
+// distance -- grows with |di| over [0, half] (sin^2 increases there and cos(phi) cos(phi') >= 0), so the
+// included offsets are |di| <= a; a is found by bisection over the row's window, then the offsets within
+// four of it are tested one by one, and a row where rounding breaks the order there is built entirely
+// here, as build_banded does, zero weights included.  The rows and entry counts are build_banded's.
+struct DeviceRows {
+  std::vector<double> sdp, cc, area;  // per band row: sin((phi' - phi) / 2), cos(phi) cos(phi'), cell measure
+  std::vector<double> sdl;            // sin(k dlambda / 2), k <= nx / 2
+  std::vector<std::pair<int64_t, std::vector<double>>> host_rows;  // (woff, weights) built here
+  size_t nweights = 0;
+};
+
+int build_banded_sphere_rows(const cgef_plan* p, Banded& B, DeviceRows& dr) {
+  const int nx = p->nx, ny = p->ny;
+  const double rad = p->rad;
+  const int dj_lim = p->dy > 0 ? static_cast<int>(std::ceil(rad / (p->R * p->dy))) : 0;
+  const int half = nx / 2;
+  const int W = 2 * dj_lim + 1;
+  B.D = dj_lim;
+  B.rows.assign(static_cast<size_t>(ny) * W, BandRow{0, -1, -1, 0});
+  dr.sdp.assign(static_cast<size_t>(ny) * W, 0.0);
+  dr.cc.assign(static_cast<size_t>(ny) * W, 0.0);
+  dr.area.assign(static_cast<size_t>(ny) * W, 0.0);
+  dr.sdl.resize(static_cast<size_t>(half) + 1);
+  for (int k = 0; k <= half; ++k) dr.sdl[k] = std::sin((static_cast<double>(k) * p->dx - 0.0) / 2.0);
+  std::vector<int64_t> counts(ny, 0);
+  std::vector<std::vector<std::pair<int, std::vector<double>>>> own(ny);  // per band: (row, weights)
+  parallel_for(ny, [&](int j) {
+    const double phi = coord(p->y0, p->dy, j);
+    bool closed = false;
+    for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
+      int jj = j + ddj;
+      if (jj < 0 || jj >= ny) continue;
+      if (sphere_row_window(p->R, p->dx, phi, coord(p->y0, p->dy, jj), rad, half) >= half) closed = true;
+    }
+    for (int ddj = -dj_lim; ddj <= dj_lim; ++ddj) {
+      int jj = j + ddj;
+      if (jj < 0 || jj >= ny) continue;
+      const size_t r = static_cast<size_t>(j) * W + (ddj + dj_lim);
+      const double phi2 = coord(p->y0, p->dy, jj);
+      const double A = p->R * p->R * std::cos(phi2) * p->dx * p->dy;
+      const int win = closed ? half : sphere_row_window(p->R, p->dx, phi, phi2, rad, half);
+      const int hi = (closed && 2 * half + 1 > nx) ? half - 1 : win;
+      const double sdp = std::sin((phi2 - phi) / 2.0);
+      const double cc = std::cos(phi) * std::cos(phi2);
+      auto dist = [&](int k) {
+        const double sdl = dr.sdl[k];
+        double h = sdp * sdp + cc * sdl * sdl;
+        if (h > 1.0) h = 1.0;
+        return 2.0 * p->R * std::asin(std::sqrt(h));
+      };
+      int amax = -1;
+      if (dist(0) <= rad) {
+        int lo = 0, up = win;
+        while (lo < up) {
+          const int mid = lo + (up - lo + 1) / 2;
+          if (dist(mid) <= rad)
+            lo = mid;
+          else
+            up = mid - 1;
+        }
+        amax = lo;
+      }
+      bool monotone = true;
+      for (int k = std::max(0, amax - 4); k <= std::min(win, amax + 4) && monotone; ++k)
+        monotone = (dist(k) <= rad) == (k <= amax);
+      if (!monotone) {
+        // build_banded's loop over the whole window: inclusion per offset, zero weights in the gaps
+        std::vector<double> wabs(static_cast<size_t>(win) + 1, 0.0);
+        amax = -1;
+        int64_t n = 0;
+        for (int k = 0; k <= win; ++k) {
+          const double d = dist(k);
+          if (d <= rad) {
+            wabs[k] = kernel_weight(p->kernel, p->alpha, d, p->scale) * A;
+            amax = k;
+            n += k == 0 ? 1 : 1 + (k <= hi ? 1 : 0);
+          }
+        }
+        counts[j] += n;
+        if (amax >= 0) {
+          wabs.resize(static_cast<size_t>(amax) + 1);
+          own[j].emplace_back(ddj + dj_lim, std::move(wabs));
+        }
+      } else if (amax >= 0) {
+        counts[j] += 1 + amax + std::min(amax, hi);
+      }
+      if (amax >= 0) {
+        BandRow& br = B.rows[r];
+        br.a = amax;
+        br.hi = std::min(amax, hi);
+        dr.sdp[r] = sdp;
+        dr.cc[r] = cc;
+        dr.area[r] = A;
+      }
+    }
+  });
+  // half-row offsets in band order, then the entry counts of the reference's CSR
+  size_t off = 0;
+  for (size_t r = 0; r < B.rows.size(); ++r) {
+    BandRow& br = B.rows[r];
+    if (br.a < 0) continue;
+    if (off > static_cast<size_t>(INT32_MAX))
+      return fail(CGEF_EINVAL, "footprint too large: more than 2^31 half-row weights (reduce the scale or the grid)");
+    br.woff = static_cast<int32_t>(off);
+    off += static_cast<size_t>(br.a) + 1;
+    B.Amax = std::max(B.Amax, br.a);
+  }
+  if (off > static_cast<size_t>(INT32_MAX))
+    return fail(CGEF_EINVAL, "footprint too large: more than 2^31 half-row weights (reduce the scale or the grid)");
+  dr.nweights = off;
+  for (int j = 0; j < ny; ++j)
+    for (auto& rw : own[j])
+      dr.host_rows.emplace_back(B.rows[static_cast<size_t>(j) * W + rw.first].woff, std::move(rw.second));
+  B.ptr.assign(1, 0);
+  for (int j = 0; j < ny; ++j) B.ptr.push_back(B.ptr.back() + counts[j]);
+  return CGEF_OK;
+}
+
+// Process-wide choice of where large spherical footprints are built (cgef_set_footprint_build).
+std::atomic<int> g_footprint_build{CGEF_BUILD_AUTO};
+
+// The device build applies to the banded engine on a sphere with a periodic longitude (one ZeroFill
+// denominator per band) and a device; AUTO takes it once the footprint holds about 2e6 half-row weights,
+// where the host's distance loop starts to cost tens of milliseconds.
+bool use_device_build(const cgef_plan* p) {
+  if (p->engine != CGEF_ENGINE_BANDED || p->geometry != CGEF_SPHERICAL || !p->periodic_x || p->device < 0) return false;
+  const int mode = g_footprint_build.load();
+  if (mode == CGEF_BUILD_HOST) return false;
+  if (mode == CGEF_BUILD_DEVICE) return true;
+  const int dj_lim = p->dy > 0 ? static_cast<int>(std::ceil(p->rad / (p->R * p->dy))) : 0;
+  double est = 0.0;
+  for (int j = 0; j < p->ny; ++j) {
+    const double c = std::fabs(std::cos(coord(p->y0, p->dy, j)));
+    const double cells = c > 0.0 ? p->rad / (p->R * c * p->dx) : p->nx / 2.0;
+    est += (2.0 * dj_lim + 1.0) * (std::min(cells, p->nx / 2.0) + 1.0);
+  }
+  return est > 2e6;
+}
+
 }  // namespace
+
+int set_footprint_build(int where) {
+  if (where != CGEF_BUILD_AUTO && where != CGEF_BUILD_HOST && where != CGEF_BUILD_DEVICE)
+    return fail(CGEF_EINVAL, "footprint build must be CGEF_BUILD_AUTO, CGEF_BUILD_HOST or CGEF_BUILD_DEVICE");
+  g_footprint_build.store(where);
+  return CGEF_OK;
+}
 
 #ifndef CGEF_PAIRED
 #define CGEF_PAIRED 1
@@ -410,7 +558,11 @@ int build_plan_tables(cgef_plan* p) {
   std::vector<PrefixRow> prows;
 
   if (p->engine == CGEF_ENGINE_BANDED) {
-    if (int rc = build_banded(p, B)) return rc;
+    const bool on_device = use_device_build(p);
+    DeviceRows dr;
+    if (int rc = on_device ? build_banded_sphere_rows(p, B, dr) : build_banded(p, B)) return rc;
+    p->built_on_device = on_device;
+    p->nwhalf = on_device ? static_cast<int64_t>(dr.nweights) : static_cast<int64_t>(B.w.size());
     p->D = B.D;
     p->Amax = B.Amax;
     p->dj_lim = B.D;
@@ -422,7 +574,9 @@ int build_plan_tables(cgef_plan* p) {
     // ZeroFill denominator: the footprint mass over in-domain entries, in CSR order
     // (Filtering.jl:2574-2582 accumulate w for every in-domain entry).
     const int64_t W = 2 * B.D + 1;
-    if (p->periodic_x) {
+    if (on_device) {
+      // the denominators come from the device weights (device_band_tables)
+    } else if (p->periodic_x) {
       p->den_zf_2d = 0;
       den_zf.assign(ny, 0.0);
       parallel_for(ny, [&](int j) {
@@ -468,11 +622,16 @@ int build_plan_tables(cgef_plan* p) {
     p->H = std::max(B.Amax, 1);
     int rc;
     if ((rc = upload(p, &p->d_rows, p->h_rows.data(), p->h_rows.size())) != CGEF_OK) return rc;
-    const double no_weights = 0.0;  // a footprint without entries still gets a one-element table
-    if ((rc = upload(p, &p->d_w, p->h_whalf.empty() ? &no_weights : p->h_whalf.data(),
-                     std::max<size_t>(p->h_whalf.size(), 1))) != CGEF_OK)
-      return rc;
-    if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
+    if (on_device) {
+      if ((rc = device_band_tables(p, dr.sdp, dr.cc, dr.area, dr.sdl, dr.nweights, dr.host_rows)) != CGEF_OK)
+        return rc;
+    } else {
+      const double no_weights = 0.0;  // a footprint without entries still gets a one-element table
+      if ((rc = upload(p, &p->d_w, p->h_whalf.empty() ? &no_weights : p->h_whalf.data(),
+                       std::max<size_t>(p->h_whalf.size(), 1))) != CGEF_OK)
+        return rc;
+      if ((rc = upload(p, &p->d_den_zf, den_zf.data(), den_zf.size())) != CGEF_OK) return rc;
+    }
     const unsigned long long queue0[2] = {0, 0};
     if ((rc = upload(p, &p->d_queue, queue0, 2)) != CGEF_OK) return rc;
     if ((rc = rebuild_schedule(p, CGEF_SPLIT_WAVES, 0)) != CGEF_OK) return rc;

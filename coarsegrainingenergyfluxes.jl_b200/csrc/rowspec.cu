@@ -606,24 +606,48 @@ __global__ void __launch_bounds__(128) rs_finish_kernel(BandedK a, const double*
 }
 
 // K_{row}(q) / L for every band row: w_0 + 2 sum_{d=1..min(a,hi)} w_d cos(2 pi q d / L), plus
-// w_a cos(2 pi q a / L) for a ring-closing row (its column -a), with the cosines read from the
-// twiddle table at (q d) mod L.
-__global__ void rs_kspec_kernel(const BandRow* rows, int64_t nrows, const double* w, const double2* tw, int L, int nk,
-                                int nkp, double* kspec) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t r = blockIdx.y + static_cast<int64_t>(blockIdx.z) * gridDim.y;
-  if (q >= nkp || r >= nrows) return;
-  const BandRow br = rows[r];
-  double sum = 0.0;
-  if (br.a >= 0 && q < nk) {
-    const double* wr = w + br.woff;
-    const int sym = min(br.a, br.hi);
-    sum = wr[0];
-    for (int d = 1; d <= sym; ++d)
-      sum = fma(2.0 * wr[d], __ldg(&tw[static_cast<int64_t>(q) * d % L].x), sum);
-    if (br.hi < br.a) sum = fma(wr[br.a], __ldg(&tw[static_cast<int64_t>(q) * br.a % L].x), sum);
+// w_a cos(2 pi q a / L) for a ring-closing row (its column -a) -- the real DFT of the row's weights laid
+// out on the ring (w_|d| at d mod L for every visited d in [-a, hi]), taken like a source row's (a
+// half-length Stockham FFT in shared memory, then the real split), kRsSeq rows per block.  O(L log L) a
+// row instead of a cosine sum over every offset for every bin.
+__global__ void __launch_bounds__(kRsThreads, kRsMinBlocks)
+    rs_kspec_kernel(Fft f, const BandRow* rows, int64_t nrows, const double* w, double* kspec) {
+  extern __shared__ double2 rs_smem[];
+  const int M = f.M, L = f.L;
+  double2* a = rs_smem;
+  double2* b = rs_smem + kRsSeq * M;
+  const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kRsSeq;
+  const int nseq = static_cast<int>(min(static_cast<int64_t>(kRsSeq), nrows - r0));
+  double* ad = reinterpret_cast<double*>(a);
+  for (int e = 0; e < nseq; ++e) {
+    const BandRow br = rows[r0 + e];
+    const double* wr = w + (br.a >= 0 ? br.woff : 0);
+    for (int n = threadIdx.x; n < L; n += blockDim.x) {
+      // every visited offset d in [-a, hi] lands on ring position d mod L (a footprint wider than a
+      // periodic domain wraps it more than once)
+      double x = 0.0;
+      if (br.a >= 0) {
+        for (int d = n; d <= br.hi; d += L) x += wr[d];
+        for (int d = L - n; d <= br.a; d += L) x += wr[d];
+      }
+      ad[e * L + n] = x;
+    }
   }
-  kspec[r * nkp + q] = sum / L;
+  __syncthreads();
+  const double2* z = fft_block(a, b, nseq, f);
+  const double inv_l = 1.0 / static_cast<double>(L);
+  for (int t = threadIdx.x; t < nseq * f.nkp; t += blockDim.x) {
+    const int e = t / f.nkp, q = t - e * f.nkp;
+    double v = 0.0;
+    if (q < f.nk) {
+      const double2 zq = z[e * M + (q == M ? 0 : q)];
+      const double2 zc = conj2(z[e * M + (q == 0 ? 0 : M - q)]);
+      const double2 E = make_double2(0.5 * (zq.x + zc.x), 0.5 * (zq.y + zc.y));
+      const double2 O = make_double2(0.5 * (zq.y - zc.y), -0.5 * (zq.x - zc.x));  // (zq - zc) / 2i
+      v = cadd(E, cmul(__ldg(f.tw + q), O)).x * inv_l;
+    }
+    kspec[(r0 + e) * f.nkp + q] = v;
+  }
 }
 
 int rs_check(const char* what) {
@@ -649,6 +673,25 @@ int rs_smem_attr(const void* kernel) {
   return CGEF_OK;
 }
 
+// The plan's transform description for the kernels.
+Fft make_fft(const cgef_plan* p) {
+  Fft f{};
+  f.L = p->rs_L;
+  f.M = p->rs_L / 2;
+  f.nk = p->rs_nk;
+  f.nkp = p->rs_nkp;
+  f.nrad = p->rs_nrad;
+  for (int i = 0, ns = 1; i < p->rs_nrad; ++i) {
+    f.rad[i] = p->rs_rad[i];
+    f.magic[i] = ns == 1 ? 0u : static_cast<unsigned>(((uint64_t(1) << 32) + ns - 1) / ns);
+    f.poff[i] = p->rs_poff[i];
+    ns *= p->rs_rad[i];
+  }
+  f.tw = reinterpret_cast<const double2*>(p->d_rs_tw);
+  f.ptw = reinterpret_cast<const double2*>(p->d_rs_ptw);
+  return f;
+}
+
 template <int MODE, int NF, bool DEF>
 int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsShare& share, bool leave_raw,
                 cudaStream_t st) {
@@ -656,19 +699,7 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
   constexpr int NA = C::NA;
   constexpr int NC = (NA + kRsSeq - 1) / kRsSeq;
   RsK k{};
-  k.f.L = p->rs_L;
-  k.f.M = p->rs_L / 2;
-  k.f.nk = p->rs_nk;
-  k.f.nkp = p->rs_nkp;
-  k.f.nrad = p->rs_nrad;
-  for (int i = 0, ns = 1; i < p->rs_nrad; ++i) {
-    k.f.rad[i] = p->rs_rad[i];
-    k.f.magic[i] = ns == 1 ? 0u : static_cast<unsigned>(((uint64_t(1) << 32) + ns - 1) / ns);
-    ns *= p->rs_rad[i];
-  }
-  k.f.tw = reinterpret_cast<const double2*>(p->d_rs_tw);
-  k.f.ptw = reinterpret_cast<const double2*>(p->d_rs_ptw);
-  for (int i = 0; i < p->rs_nrad; ++i) k.f.poff[i] = p->rs_poff[i];
+  k.f = make_fft(p);
   k.planes = a.planes;
   k.plane_stride = a.plane_stride;
   k.slice_stride = a.slice_stride;
@@ -854,17 +885,25 @@ int build_row_spectra(cgef_plan* p) {
     return CGEF_OK;
   }
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(row-spectral kernel spectra)");
-  const int64_t zchunks = (nrows + 65534) / 65535;
-  const dim3 g((nkp + 127) / 128, static_cast<unsigned>(std::min<int64_t>(nrows, 65535)), static_cast<unsigned>(zchunks));
-  rs_kspec_kernel<<<g, 128>>>(p->d_rows, nrows, p->d_w, reinterpret_cast<const double2*>(p->d_rs_tw), L, nk, nkp,
-                               p->d_rs_k);
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "rs_kspec_kernel");
-  if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cuda_fail(e, "rs_kspec_kernel");
   p->rs_L = L;
   p->rs_nk = nk;
   p->rs_nkp = nkp;
   p->rs_nrad = static_cast<int>(rad.size());
   for (size_t i = 0; i < rad.size(); ++i) p->rs_rad[i] = rad[i];
+  int rc = rs_smem_attr(reinterpret_cast<const void*>(rs_kspec_kernel));
+  if (rc == CGEF_OK) {
+    const int smem = 2 * kRsSeq * static_cast<int>(sizeof(double2)) * (L / 2);
+    rs_kspec_kernel<<<static_cast<unsigned>((nrows + kRsSeq - 1) / kRsSeq), kRsThreads, smem>>>(
+        make_fft(p), p->d_rows, nrows, p->d_w, p->d_rs_k);
+    if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaDeviceSynchronize()) != cudaSuccess)
+      rc = cuda_fail(e, "rs_kspec_kernel");
+    else
+      count_launch();
+  }
+  if (rc != CGEF_OK) {
+    p->rs_L = 0;
+    return rc;
+  }
   p->rs_on = true;
   return CGEF_OK;
 }

@@ -137,6 +137,21 @@ int32_t cgef_plan_reset_queue(cgef_plan* plan);
 /* Plan statistics. */
 int32_t cgef_plan_get_info(const cgef_plan* plan, cgef_plan_info* info);
 
+/* Where the banded engine builds a spherical footprint on a periodic longitude axis (no counterpart in
+ * the reference, which builds on the CPU, Filtering.jl:675-731).  The host always decides the entry
+ * set with its libm, as the reference's loop does: per (band, row offset) the great-circle distance
+ * grows with |di|, so it bisects for the last included offset and tests the four either side of it
+ * (a row where rounding breaks that order is built entirely on the host).  With the device build, the
+ * weights of those entries (one exp per |di|, from the host's row constants) and the ZeroFill
+ * denominators are computed on the GPU: the same entries as a host build, weights within a few ulps
+ * of it, denominators summed in another order.  CGEF_BUILD_AUTO (the default) takes the device build
+ * once a footprint holds about 2e6 half-row weights.  Applies to plans created afterwards, from any
+ * thread. */
+enum { CGEF_BUILD_AUTO = 0, CGEF_BUILD_HOST = 1, CGEF_BUILD_DEVICE = 2 };
+int32_t cgef_set_footprint_build(int32_t where);
+/* CGEF_BUILD_DEVICE if the plan's footprint weights were computed on the device, else CGEF_BUILD_HOST. */
+int32_t cgef_plan_get_build(const cgef_plan* plan, int32_t* where);
+
 /* Schedule autotuner of the banded engine (no counterpart in the reference, whose loops have no
  * schedule).  Times the flux's footprint sums on this plan's grid and mask (zero-valued inputs; their
  * cost depends on the footprint and the mask, not on the values): first the row-spectral evaluation
