@@ -160,18 +160,21 @@ def uses_row_spectral(p) -> bool:
     return p.engine == "banded" and p.row_spectral[1]
 
 
-def rowspec_bytes(p, grid, nslices, na, nplanes, nout, masked) -> float:
+def rowspec_bytes(p, grid, nslices, na, nplanes, nout, masked, raw=False) -> float:
     """Compulsory DRAM bytes of one row-spectral launch: the staged planes read, the source spectra
-    written and read once, the kernel spectra read, the summed spectra written and read, the
-    unnormalised sums written and read, the outputs written (and the mask read)."""
+    written and read once, the kernel spectra read, the summed spectra written and read, then either
+    (raw: the flux, whose strain pass finishes the sums) the unnormalised sums written once, or (a
+    filter) the unnormalised sums written and read, the outputs written and the mask read."""
     L = p.row_spectral[2]
     nk = L // 2 + 1
     D = p.info.dj_lim
     nrows = (grid.ny if grid.is_spherical else 1) * (2 * D + 1)
     N = grid.nx * grid.ny
     spec = nslices * grid.ny * na * nk * 16
-    return float(nslices * nplanes * N * 8 + 4 * spec + nrows * nk * 8 + 2 * nslices * na * N * 8
-                 + nslices * nout * N * 8 + (nslices * N if masked else 0))
+    base = nslices * nplanes * N * 8 + 4 * spec + nrows * nk * 8
+    if raw:
+        return float(base + nslices * na * N * 8)
+    return float(base + 2 * nslices * na * N * 8 + nslices * nout * N * 8 + (nslices * N if masked else 0))
 
 
 def prefix_bytes(p, grid, nslices, na, nplanes, nout, masked) -> float:
@@ -798,7 +801,7 @@ def measure_sweep(args, name, rank, world, local, dist, *, snapshots=1, scale_km
         na, npl = (9, 3) if g.is_spherical else (5, 2)
         if isinstance(plans[0].strategy, cg.Deformable):  # the mask is one more quantity and plane
             na, npl = na + 1, npl + 1
-        bytes_step = sum(rowspec_bytes(p, g, nsl, na, npl, 5, masked) for p in spec_plans)
+        bytes_step = sum(rowspec_bytes(p, g, nsl, na, npl, 0, masked, raw=True) for p in spec_plans)
         # a sweep transforms the source rows once for all row-spectral scales of one FFT length: the
         # other scales read those spectra but neither read the staged planes nor write spectra
         L0 = spec_plans[0].row_spectral[2]
@@ -812,8 +815,9 @@ def measure_sweep(args, name, rank, world, local, dist, *, snapshots=1, scale_km
         traffic, traffic_basis, traffic_one = committed_traffic(f"{name}:rowspec", nsl, scale_km)
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": traffic, "traffic_basis": traffic_basis, "traffic_one_snapshot": traffic_one,
-                    "kernel": "rs_forward_kernel + rs_accumulate_kernel + rs_inverse_kernel + rs_finish_kernel "
-                              "(row-spectral footprint sums: FFTs along x, banded spectral sums, inverse FFTs)",
+                    "kernel": "rs_forward_kernel + rs_accumulate_kernel + rs_inverse_kernel (row-spectral footprint "
+                              "sums: FFTs along x, banded spectral sums, inverse FFTs; the epilogue runs in the strain "
+                              "pass)",
                     "per_launch_ms": per_launch_ms, "launches": cnt, "algorithmic_bytes_per_launch": bytes_launch,
                     "direct_sum_equivalent_tflops": flops_all / launches_per_step / (per_launch_ms * 1e-3) / 1e12
                     if not direct_plans else None,

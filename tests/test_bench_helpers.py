@@ -31,18 +31,20 @@ def test_row_spectral_compulsory_bytes_at_quarter_degree_100_km(bench):
     # the plan as the device builds it: a 1440-point ring, so 721 bins per row
     stub = types.SimpleNamespace(row_spectral=(True, True, 1440), info=p.info)
     N, nk, na = 1440 * 720, 721, 9
+    kspec = 720 * (2 * D + 1) * nk * 8      # kernel spectra
+    # the flux: the strain pass finishes the unnormalised sums, so the launch writes them once
     want = (3 * N * 8                       # staged planes (3 planetary velocities)
             + 4 * 720 * na * nk * 16        # source and summed spectra, each written and read
-            + 720 * (2 * D + 1) * nk * 8    # kernel spectra
-            + 2 * na * N * 8                # unnormalised sums written and read
-            + 5 * N * 8                     # outputs
-            + N)                            # mask
-    assert want == 594_610_560
-    assert bench.rowspec_bytes(stub, g.with_mask(S.land_mask(g)), 1, na, 3, 5, True) == want
+            + kspec
+            + na * N * 8)                   # unnormalised sums, written
+    assert want == 477_452_160
+    assert bench.rowspec_bytes(stub, g.with_mask(S.land_mask(g)), 1, na, 3, 0, True, raw=True) == want
     # eight snapshots per launch move eight times the per-snapshot bytes; the kernel spectra are read
     # once per launch whatever the snapshot count
-    kspec = 720 * (2 * D + 1) * nk * 8
-    assert bench.rowspec_bytes(stub, g, 8, na, 3, 5, False) == 8 * (want - N - kspec) + kspec
+    assert bench.rowspec_bytes(stub, g, 8, na, 3, 0, False, raw=True) == 8 * (want - kspec) + kspec
+    # a filter of three fields: the sums written and read, the outputs written, the mask read
+    f3 = bench.rowspec_bytes(stub, g.with_mask(S.land_mask(g)), 1, 3, 3, 3, True)
+    assert f3 == 3 * N * 8 + 4 * 720 * 3 * nk * 16 + kspec + 2 * 3 * N * 8 + 3 * N * 8 + N
 
 
 def test_committed_traffic_only_where_a_capture_exists(bench):

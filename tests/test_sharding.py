@@ -2,8 +2,10 @@
 
 The assignment and result assembly run as world-size-2 `gloo` ranks with an injected compute
 function standing in for the GPU sweep; the checks are that every (slice, scale) unit is computed
-exactly once, that the loads balance, and that the assembled result equals one rank's.
+exactly once, that the loads balance on the cost of the evaluation each scale runs, and that the
+assembled result (sent to rank 0 as tensors) equals one rank's.
 """
+import math
 import os
 import socket
 
@@ -68,7 +70,7 @@ def _worker(rank, world, port, nslices, nscales, q):
             calls.append((tuple(sl), tuple(scl)))
             return base(sl, scl)
 
-        out = SH.run_sharded(rank, world, nslices, nscales, a, compute, SH.torch_gather())
+        out = SH.run_sharded(rank, world, nslices, nscales, a, compute, SH.torch_collect(a, (3, 4)))
         q.put((rank, calls, None if out is None else (out[0].tolist(), out[1].shape)))
     finally:
         dist.destroy_process_group()
@@ -102,3 +104,39 @@ def test_two_gloo_ranks_assemble_the_single_rank_result(nslices, nscales):
     ref, _ = SH.run_sharded(0, 1, nslices, nscales, SH.assign([1.0] * nscales, [1.0] * nslices, 1), fake_compute())
     assert np.array_equal(np.array(E), ref)
     assert tuple(pishape) == (nslices, nscales, 3, 4)
+
+
+def test_cost_model_follows_the_evaluation_each_scale_runs():
+    # 0.25 degree sphere: 2000 km has 168k entries per target and 347 row offsets; 100 km 873 and 19
+    nx = 1440
+    direct_2000 = SH.scale_cost("banded", nx=nx, entries_per_target=168_388.0, dj_lim=173)
+    spectral_2000 = SH.scale_cost("banded", nx=nx, entries_per_target=168_388.0, dj_lim=173, fft_length=1440)
+    direct_100 = SH.scale_cost("banded", nx=nx, entries_per_target=873.0, dj_lim=9)
+    spectral_100 = SH.scale_cost("banded", nx=nx, entries_per_target=873.0, dj_lim=9, fft_length=1440)
+    assert direct_2000 / spectral_2000 > 50           # measured on the device: ~109 (one snapshot)
+    assert 0.5 < direct_100 / spectral_100 < 5       # comparable near the autotuner's switch (~80 km)
+    assert SH.scale_cost("banded", nx=nx, dj_lim=173, fft_length=1440) < 2 * SH.scale_cost(
+        "banded", nx=nx, dj_lim=9, fft_length=1440) * 173 / 9
+
+
+def test_scales_mode_balances_a_mixed_direct_and_spectral_set():
+    # C2's 24 scales on 2 ranks with one snapshot ("scales" mode): the small ones direct, the rest
+    # row-spectral, costed by what they run
+    nx = 1440
+    ells = [50e3 * 40.0 ** (s / 23.0) for s in range(24)]
+    costs = []
+    for ell in ells:
+        dj = math.ceil(ell * 2.399 / 27_798.0)
+        entries = 873.0 * (ell / 1e5) ** 2
+        costs.append(SH.scale_cost("banded", nx=nx, entries_per_target=entries, dj_lim=dj,
+                                   fft_length=0 if ell < 80e3 else 1440))
+    a = SH.assign(costs, [1.0], 2)
+    assert a.mode == "scales"
+    per = [c * 1.0 for c in costs]
+    assert max(a.loads) <= sum(per) / 2 + max(per) + 1e-9
+    # the direct-sum model (entries per target) balances its own numbers, not the device's: under the
+    # costs of what each scale runs, its split is further from even
+    naive = SH.assign([873.0 * (ell / 1e5) ** 2 for ell in ells], [1.0], 2)
+    true_loads = [sum(per[s] for _, s in part) for part in naive.units]
+    assert max(a.loads) / (sum(per) / 2) < 1.1
+    assert max(a.loads) <= max(true_loads)
