@@ -43,7 +43,7 @@ EXPORTED = [
     "cgef_pipeline_create", "cgef_pipeline_submit", "cgef_pipeline_drain", "cgef_pipeline_destroy",
     "cgef_plan_set_filter_rows", "cgef_plan_get_schedule", "cgef_plan_set_row_spectral",
     "cgef_plan_get_row_spectral", "cgef_build_arch", "cgef_plan_reset_queue", "cgef_debug_inject",
-    "cgef_set_footprint_build", "cgef_plan_get_build",
+    "cgef_set_footprint_build", "cgef_plan_get_build", "cgef_compute_pi_w", "cgef_compute_pi_w_device",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE, KERNEL_ROWSPEC = (
     0, 1, 2, 3, 4, 5, 6)
@@ -64,6 +64,12 @@ class PlanInfo(C.Structure):
         ("engine", C.c_int32), ("nbands", C.c_int32), ("nentries", C.c_int64), ("dj_lim", C.c_int32),
         ("di_max", C.c_int32), ("kernel_radius", C.c_double), ("active_area", C.c_double),
     ]
+
+
+class PiWOutputs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in
+                ("pi", "ubar", "vbar", "wbar", "tau_xx", "tau_xy", "tau_yy", "tau_xz", "tau_yz", "tau_zz",
+                 "s_xx", "s_xy", "s_yy", "s_xz", "s_yz", "energy")]
 
 
 class PiOutputs(C.Structure):
@@ -124,6 +130,10 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_plan_reset_queue.restype = i32
     L.cgef_debug_inject.argtypes = [vp, i32]
     L.cgef_debug_inject.restype = i32
+    L.cgef_compute_pi_w.argtypes = [vp, i32, vp, vp, vp, i64, vp, C.POINTER(PiWOutputs)]
+    L.cgef_compute_pi_w.restype = i32
+    L.cgef_compute_pi_w_device.argtypes = [vp, i32, vp, vp, vp, i64, vp, C.POINTER(PiWOutputs), vp]
+    L.cgef_compute_pi_w_device.restype = i32
     L.cgef_set_footprint_build.argtypes = [i32]
     L.cgef_set_footprint_build.restype = i32
     L.cgef_plan_get_build.argtypes = [vp, C.POINTER(i32)]

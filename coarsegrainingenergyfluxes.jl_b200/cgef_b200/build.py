@@ -21,8 +21,8 @@ INCLUDE = os.path.join(REPO_ROOT, "include")
 LIB_PATH = os.path.join(HERE, "libcgef_b200.so")
 PEAK_LIB_PATH = os.path.join(HERE, "libcgef_peak.so")
 SOURCES = ["kernels.cu", "rowspec.cu", "cgef_api.cu", "noalloc.cu", "closure.cu", "decomposition.cu", "pipeline.cu",
-           "plan_build.cpp", "plan_device.cu"]
-HEADERS = ["cgef_internal.h", "banded_common.cuh"]
+           "plan_build.cpp", "plan_device.cu", "pi_w.cu"]
+HEADERS = ["cgef_internal.h", "banded_common.cuh", "stencil.cuh"]
 
 
 def _nvcc() -> str:

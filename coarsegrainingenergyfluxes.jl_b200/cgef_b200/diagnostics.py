@@ -23,6 +23,9 @@ from .kernels import AbstractFilterKernel, check_spectrum_kernel, transfer_monot
 PI_OUTPUTS = ("Pi", "ubar", "vbar", "tau_xx", "tau_xy", "tau_yy", "S_xx", "S_xy", "S_yy")
 _FIELD = {"Pi": "pi", "ubar": "ubar", "vbar": "vbar", "tau_xx": "tau_xx", "tau_xy": "tau_xy", "tau_yy": "tau_yy",
           "S_xx": "s_xx", "S_xy": "s_xy", "S_yy": "s_yy"}
+# the 2.5-D flux (compute_Pi with w): the vertical velocity and the stress and strain terms it adds
+PI_W_OUTPUTS = ("Pi", "ubar", "vbar", "wbar", "tau_xx", "tau_xy", "tau_yy", "tau_xz", "tau_yz", "tau_zz",
+                "S_xx", "S_xy", "S_yy", "S_xz", "S_yz")
 
 
 # ------------------------------------------------------------------------------------------
@@ -102,7 +105,8 @@ def compute_Pi(Pi, u, v, w, grid: StructuredGrid, kernel: AbstractFilterKernel, 
     CUDA tensors through the stream-ordered device entry point.
     """
     if w is not None:
-        raise ArgumentError("the vertical velocity w (2.5-D path) is outside the supported path; pass None")
+        return _compute_Pi_w(Pi, u, v, w, grid, kernel, scale, filter_plan=filter_plan, mask_strategy=mask_strategy,
+                             outputs=outputs, energy=energy, slice_masks=slice_masks)
     bs = _batch_shape(u, grid, "u")
     if _batch_shape(v, grid, "v") != bs:
         raise DimensionMismatch("v's batch axes do not match u's")
@@ -145,18 +149,57 @@ def compute_Pi(Pi, u, v, w, grid: StructuredGrid, kernel: AbstractFilterKernel, 
 compute_Π = compute_Pi
 
 
+def _compute_Pi_w(Pi, u, v, w, grid, kernel, scale, *, filter_plan, mask_strategy, outputs, energy, slice_masks):
+    """compute_Π! with the vertical velocity (Diagnostics.jl:254-260, 483-681): cgef_compute_pi_w."""
+    bs = _batch_shape(u, grid, "u")
+    if _batch_shape(v, grid, "v") != bs or _batch_shape(w, grid, "w") != bs:
+        raise DimensionMismatch("v's and w's batch axes must match u's")
+    nb = _nbatch(bs)
+    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy)
+    if Pi is None:
+        Pi = A.empty_like(u)
+    if tuple(Pi.shape) != tuple(u.shape):
+        raise DimensionMismatch(f"Pi {tuple(Pi.shape)} does not match u {tuple(u.shape)}")
+    dt = A.dtype_code(u)
+    if A.dtype_code(v) != dt or A.dtype_code(w) != dt or A.dtype_code(Pi) != dt:
+        raise ArgumentError("u, v, w and Pi must share a dtype")
+    outs = _lib.PiWOutputs()
+    outs.pi = A.ptr(Pi)
+    for k, arr in (outputs or {}).items():
+        if k not in PI_W_OUTPUTS or k == "Pi":
+            raise ArgumentError(f"unknown output {k!r}; choose from {PI_W_OUTPUTS[1:]}")
+        if tuple(arr.shape) != tuple(u.shape) or A.dtype_code(arr) != dt:
+            raise DimensionMismatch(f"output {k} must match u's shape and dtype")
+        setattr(outs, k.lower() if k.startswith("S_") else k, A.ptr(arr))
+    if energy is not None:
+        if int(np.prod(energy.shape)) != nb:
+            raise DimensionMismatch("energy needs one entry per slice")
+        outs.energy = A.ptr(energy)
+    L = _lib.load()
+    m = _slice_masks(slice_masks, u, nb, grid)
+    if A.is_device(u):
+        _lib.check(L.cgef_compute_pi_w_device(plan.handle, dt, A.ptr(u), A.ptr(v), A.ptr(w), nb,
+                                              None if m is None else A.ptr(m), C.byref(outs), A.stream_of(u)))
+    else:
+        u, v, w = (np.ascontiguousarray(x) for x in (u, v, w))
+        _lib.check(L.cgef_compute_pi_w(plan.handle, dt, A.ptr(u), A.ptr(v), A.ptr(w), nb,
+                                       None if m is None else A.ptr(m), C.byref(outs)))
+    return Pi
+
+
 def compute_Pi_fields(u, v, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
                       mask_strategy: AbstractMaskStrategy = ZeroFill(),
-                      filter_plan: Optional[PhysicalFilterPlan] = None, slice_masks=None) -> Dict[str, object]:
-    """compute_Π! returning every intermediate (the reference's ΠWorkspace contents) and E."""
-    outs = {k: A.empty_like(u) for k in PI_OUTPUTS[1:]}
+                      filter_plan: Optional[PhysicalFilterPlan] = None, slice_masks=None, w=None) -> Dict[str, object]:
+    """compute_Π! returning every intermediate (the reference's ΠWorkspace contents) and E; with the
+    vertical velocity w, the 2.5-D path's as well (wbar, tau_xz, tau_yz, tau_zz, S_xz, S_yz)."""
+    outs = {k: A.empty_like(u) for k in (PI_OUTPUTS if w is None else PI_W_OUTPUTS)[1:]}
     nb = _nbatch(tuple(u.shape[:-2]))
     if A.is_device(u):
         import torch
         energy = torch.empty(nb, dtype=torch.float64, device=u.device)
     else:
         energy = np.empty(nb, dtype=np.float64)
-    Pi = compute_Pi(None, u, v, None, grid, kernel, scale, filter_plan=filter_plan, mask_strategy=mask_strategy,
+    Pi = compute_Pi(None, u, v, w, grid, kernel, scale, filter_plan=filter_plan, mask_strategy=mask_strategy,
                     outputs=outs, energy=energy, slice_masks=slice_masks)
     outs["Pi"] = Pi
     outs["energy"] = energy

@@ -856,6 +856,63 @@ int32_t cgef_compute_pi_device(cgef_plan* p, int32_t dtype, const void* u, const
   return compute_pi_device(p, dtype, u, v, nbatch, slice_masks, out, static_cast<cudaStream_t>(stream));
 }
 
+int32_t cgef_compute_pi_w_device(cgef_plan* p, int32_t dtype, const void* u, const void* v, const void* w,
+                                 int64_t nbatch, const uint8_t* slice_masks, const cgef_pi_w_outputs* out,
+                                 void* stream) {
+  int rc = check_plan(p);
+  if (rc) return rc;
+  DeviceGuard dg(p->device);
+  return compute_pi_w_device(p, dtype, u, v, w, nbatch, slice_masks, out, static_cast<cudaStream_t>(stream));
+}
+
+int32_t cgef_compute_pi_w(cgef_plan* p, int32_t dtype, const void* u, const void* v, const void* w, int64_t nbatch,
+                          const uint8_t* slice_masks, const cgef_pi_w_outputs* out) {
+  int rc;
+  if ((rc = check_plan(p)) || (rc = check_dtype(dtype))) return rc;
+  if (!u || !v || !w) return fail(CGEF_EINVAL, "u, v and w must be non-NULL");
+  if (nbatch < 1 || nbatch > 65535) return fail(CGEF_EINVAL, "nbatch must be in 1..65535");
+  DeviceGuard dg(p->device);
+  const int64_t N = static_cast<int64_t>(p->nx) * p->ny;
+  const size_t fb = dsize(dtype) * N * nbatch;
+  void* din = nullptr;
+  if ((rc = ensure_ws(p, kSlotIn, 3 * fb, &din))) return rc;
+  cudaError_t e = cudaMemcpyAsync(din, u, fb, cudaMemcpyHostToDevice, p->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(static_cast<char*>(din) + fb, v, fb, cudaMemcpyHostToDevice, p->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(static_cast<char*>(din) + 2 * fb, w, fb, cudaMemcpyHostToDevice, p->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(H2D)");
+  const uint8_t* dmask = nullptr;
+  if (slice_masks) {
+    void* dm = nullptr;
+    if ((rc = h2d(p, kSlotMask, slice_masks, static_cast<size_t>(N) * nbatch, &dm))) return rc;
+    dmask = static_cast<const uint8_t*>(dm);
+  }
+  cgef_pi_w_outputs none{};
+  const cgef_pi_w_outputs* o = out ? out : &none;
+  void* const hosts[15] = {o->pi,     o->ubar,   o->vbar,   o->wbar, o->tau_xx, o->tau_xy, o->tau_yy, o->tau_xz,
+                           o->tau_yz, o->tau_zz, o->s_xx,   o->s_xy, o->s_yy,   o->s_xz,   o->s_yz};
+  int nreq = 0;
+  for (void* h : hosts)
+    if (h) ++nreq;
+  void* dout = nullptr;
+  const size_t fba = (fb + 255) / 256 * 256;
+  if ((rc = ensure_ws(p, kSlotOut, fba * (nreq > 0 ? nreq : 1) + sizeof(double) * nbatch, &dout))) return rc;
+  cgef_pi_w_outputs dev{};
+  void** devs[15] = {&dev.pi,     &dev.ubar,   &dev.vbar, &dev.wbar, &dev.tau_xx, &dev.tau_xy, &dev.tau_yy, &dev.tau_xz,
+                     &dev.tau_yz, &dev.tau_zz, &dev.s_xx, &dev.s_xy, &dev.s_yy,   &dev.s_xz,   &dev.s_yz};
+  int slot = 0;
+  for (int m = 0; m < 15; ++m)
+    if (hosts[m]) *devs[m] = static_cast<char*>(dout) + fba * slot++;
+  double* denergy = reinterpret_cast<double*>(static_cast<char*>(dout) + fba * (nreq > 0 ? nreq : 1));
+  if (o->energy) dev.energy = denergy;
+  if ((rc = compute_pi_w_device(p, dtype, din, static_cast<char*>(din) + fb, static_cast<char*>(din) + 2 * fb, nbatch,
+                                dmask, &dev, p->stream)))
+    return rc;
+  for (int m = 0; m < 15; ++m)
+    if (hosts[m] && (rc = d2h(p, hosts[m], *devs[m], fb))) return rc;
+  if (o->energy && (rc = d2h(p, o->energy, denergy, sizeof(double) * nbatch))) return rc;
+  return sync(p);
+}
+
 int32_t cgef_compute_pi(cgef_plan* p, int32_t dtype, const void* u, const void* v, int64_t nbatch,
                         const uint8_t* slice_masks, const cgef_pi_outputs* out) {
   int rc;

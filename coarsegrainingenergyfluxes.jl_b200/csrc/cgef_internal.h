@@ -172,7 +172,7 @@ struct cgef_plan {
   cgef::PrefixRow* d_prows = nullptr;  // ny * nb
   // execution
   cudaStream_t stream = nullptr;
-  cgef::DeviceBuffer ws[12];  // workspace slots (cgef::WsSlot), grown on demand
+  cgef::DeviceBuffer ws[13];  // workspace slots (cgef::WsSlot), grown on demand
   unsigned long long* d_queue = nullptr;  // banded work queue: [next unit, warps finished], zero between launches
 };
 
@@ -449,7 +449,8 @@ enum WsSlot {
   kSlotVel = 9,
   kSlotDecomp = 10,
   kSlotSpectra = 11,  // a sweep's shared source spectra (row-spectral evaluation)
-  kNumSlots = 12,
+  kSlotW = 12,        // the 2.5-D flux: the velocities and products before and after filtering
+  kNumSlots = 13,
 };
 
 struct DeviceGuard {
@@ -482,6 +483,9 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
               const double** raw_out = nullptr);
 int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int64_t nbatch64,
                       const uint8_t* slice_masks, const cgef_pi_outputs* out, cudaStream_t st);
+// The 2.5-D flux (pi_w.cu): u, v, w device buffers of dtype.
+int compute_pi_w_device(cgef_plan* p, int dtype, const void* u, const void* v, const void* w, int64_t nbatch64,
+                        const uint8_t* slice_masks, const cgef_pi_w_outputs* out, cudaStream_t st);
 // The sweep over plans (one grid) for nbatch slices on stream st: Pi [nbatch][nscales][N] (dtype) and
 // E [nbatch][nscales], either may be nullptr.
 int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u, const void* v, int64_t nbatch64,

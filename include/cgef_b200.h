@@ -215,6 +215,39 @@ int32_t cgef_filter_batch(cgef_plan* plan, int32_t dtype, const void* const* fie
 int32_t cgef_compute_pi(cgef_plan* plan, int32_t dtype, const void* u, const void* v, int64_t nbatch,
                         const uint8_t* slice_masks, const cgef_pi_outputs* out);
 
+/* Diagnostics.compute_Π! with the vertical velocity w (the 2.5-D path: `w::AbstractArray` in
+ * Diagnostics.jl:389-416, its terms at 254-260 and 483-681).  u, v, w: nbatch*ny*nx values of dtype.
+ * The plane filters u, v, w and the products uu, uv, vv, uw, vw, ww; the sphere takes w along the local
+ * up vector into the planetary velocity (vector_to_cartesian), filters its 3 components and 6
+ * products, and rotates back to east/north/up in full.  tau gains its xz, yz, zz (east-up, north-up,
+ * up-up) components; the strain S_xz = 1/2 dwbar/dx, S_yz = 1/2 dwbar/dy and S_zz = 0 (layers flat in
+ * the vertical, no curvature terms); Pi = -(Sxx txx + 2 Sxy txy + Syy tyy + 2 Sxz txz + 2 Syz tyz +
+ * Szz tzz) on active cells.  E = 1/2 <ubar^2 + vbar^2 + wbar^2>.  Every non-NULL output holds
+ * nbatch*ny*nx values of dtype (energy: nbatch doubles).  slice_masks as in cgef_compute_pi. */
+typedef struct cgef_pi_w_outputs {
+  void* pi;
+  void* ubar;
+  void* vbar;
+  void* wbar;
+  void* tau_xx;
+  void* tau_xy;
+  void* tau_yy;
+  void* tau_xz;
+  void* tau_yz;
+  void* tau_zz;
+  void* s_xx;
+  void* s_xy;
+  void* s_yy;
+  void* s_xz;
+  void* s_yz;
+  double* energy;
+} cgef_pi_w_outputs;
+int32_t cgef_compute_pi_w(cgef_plan* plan, int32_t dtype, const void* u, const void* v, const void* w, int64_t nbatch,
+                          const uint8_t* slice_masks, const cgef_pi_w_outputs* out);
+int32_t cgef_compute_pi_w_device(cgef_plan* plan, int32_t dtype, const void* u, const void* v, const void* w,
+                                 int64_t nbatch, const uint8_t* slice_masks, const cgef_pi_w_outputs* out,
+                                 void* stream);
+
 /* Diagnostics.cumulative_energy! (Diagnostics.jl:1144-1217): u, v (ny*nx, dtype) filtered as
  * scalars at every plan's scale; spectrum[s] = 1/2 <|ubar|^2>.  All plans share one grid. */
 int32_t cgef_cumulative_energy(cgef_plan* const* plans, int32_t nscales, int32_t dtype, const void* u,

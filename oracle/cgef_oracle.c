@@ -917,6 +917,149 @@ int orc_compute_pi(const orc_plan* p, const double* u, const double* v, double* 
 }
 
 /* ------------------------------------------------------------------------------------
+ * compute_Pi! with the vertical velocity w (the 2.5-D path, Diagnostics.jl:254-260, 483-681).
+ * Cartesian: u, v, w and the products uu, uv, vv, uw, vw, ww are filtered; tau_xz, tau_yz, tau_zz
+ * follow; S_xz = 1/2 dwbar/dx, S_yz = 1/2 dwbar/dy, S_zz = 0 (Diagnostics.jl:540-548).  Sphere: the
+ * planetary velocity includes w along the local up vector (vector_to_cartesian), the local filtered
+ * velocity gains wbar = up . Ubar (vector_from_cartesian), tau is rotated to east/north/up in full
+ * (tau_er, tau_nr, tau_rr too) and S_er = 1/2 dwbar/dx, S_nr = 1/2 dwbar/dy, S_rr = 0, with the metric
+ * division of the derivatives but no curvature terms (Diagnostics.jl:658-667).
+ * Pi = -(Sxx txx + 2 Sxy txy + Syy tyy + 2 Sxz txz + 2 Syz tyz + Szz tzz) on active cells
+ * (Diagnostics.jl:463-465, 689-699).  outs (each n values, NULL skips one): ubar, vbar, wbar, txx,
+ * txy, tyy, txz, tyz, tzz, sxx, sxy, syy, sxz, syz.
+ * ------------------------------------------------------------------------------------ */
+int orc_compute_pi_w(const orc_plan* p, const double* u, const double* v, const double* w, double* Pi,
+                     double* const* outs, int nthreads) {
+  const orc_grid* g = &p->g;
+  int nx = g->nx, ny = g->ny;
+  int64_t n = (int64_t)nx * ny;
+  double* in[9];
+  double* f[9];
+  for (int q = 0; q < 9; ++q) {
+    in[q] = (double*)calloc((size_t)n, sizeof(double));
+    f[q] = (double*)calloc((size_t)n, sizeof(double));
+  }
+  double* loc = (double*)calloc((size_t)n * 14, sizeof(double));
+  double *ub = loc, *vb = loc + n, *wb = loc + 2 * n, *txx = loc + 3 * n, *txy = loc + 4 * n, *tyy = loc + 5 * n,
+         *txz = loc + 6 * n, *tyz = loc + 7 * n, *tzz = loc + 8 * n, *sxx = loc + 9 * n, *sxy = loc + 10 * n,
+         *syy = loc + 11 * n, *sxz = loc + 12 * n, *syz = loc + 13 * n;
+  double* scr = (double*)calloc((size_t)n, sizeof(double));
+  int sphere = g->geometry == ORC_SPHERE;
+  /* the three velocity components: (u, v, w) on the plane, planetary (X, Y, Z) on the sphere */
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      int64_t k = (int64_t)j * nx + i;
+      if (!is_active(g, i, j)) continue;
+      if (sphere) {
+        double lam = gx_coord(g, i), phi = gy_coord(g, j);
+        double sl = sin(lam), cl = cos(lam), sp = sin(phi), cp = cos(phi);
+        in[0][k] = -sl * u[k] - sp * cl * v[k] + cp * cl * w[k];
+        in[1][k] = cl * u[k] - sp * sl * v[k] + cp * sl * w[k];
+        in[2][k] = cp * v[k] + sp * w[k];
+      } else {
+        in[0][k] = u[k];
+        in[1][k] = v[k];
+        in[2][k] = w[k];
+      }
+    }
+  /* products: 00, 01, 02, 11, 12, 22 */
+  for (int64_t k = 0; k < n; ++k) {
+    in[3][k] = in[0][k] * in[0][k];
+    in[4][k] = in[0][k] * in[1][k];
+    in[5][k] = in[0][k] * in[2][k];
+    in[6][k] = in[1][k] * in[1][k];
+    in[7][k] = in[1][k] * in[2][k];
+    in[8][k] = in[2][k] * in[2][k];
+  }
+  orc_filter_batch(p, 3, (const double* const*)in, f, nthreads);
+  orc_filter_batch(p, 6, (const double* const*)(in + 3), f + 3, nthreads);
+  for (int j = 0; j < ny; ++j) {
+    double phi = gy_coord(g, j), sp = sin(phi), cp = cos(phi);
+    for (int i = 0; i < nx; ++i) {
+      int64_t k = (int64_t)j * nx + i;
+      if (!is_active(g, i, j)) continue;
+      double U[3] = {f[0][k], f[1][k], f[2][k]};
+      double T[3][3];
+      T[0][0] = f[3][k] - U[0] * U[0];
+      T[0][1] = T[1][0] = f[4][k] - U[0] * U[1];
+      T[0][2] = T[2][0] = f[5][k] - U[0] * U[2];
+      T[1][1] = f[6][k] - U[1] * U[1];
+      T[1][2] = T[2][1] = f[7][k] - U[1] * U[2];
+      T[2][2] = f[8][k] - U[2] * U[2];
+      if (!sphere) {
+        ub[k] = U[0];
+        vb[k] = U[1];
+        wb[k] = U[2];
+        txx[k] = T[0][0];
+        txy[k] = T[0][1];
+        tyy[k] = T[1][1];
+        txz[k] = T[0][2];
+        tyz[k] = T[1][2];
+        tzz[k] = T[2][2];
+        continue;
+      }
+      double lam = gx_coord(g, i), sl = sin(lam), cl = cos(lam);
+      double e[3] = {-sl, cl, 0.0};
+      double nn[3] = {-sp * cl, -sp * sl, cp};
+      double r[3] = {cp * cl, cp * sl, sp};
+      ub[k] = e[0] * U[0] + e[1] * U[1] + e[2] * U[2];
+      vb[k] = nn[0] * U[0] + nn[1] * U[1] + nn[2] * U[2];
+      wb[k] = r[0] * U[0] + r[1] * U[1] + r[2] * U[2];
+      double te[3], tn[3], tr[3];
+      for (int a = 0; a < 3; ++a) {
+        te[a] = T[a][0] * e[0] + T[a][1] * e[1] + T[a][2] * e[2];
+        tn[a] = T[a][0] * nn[0] + T[a][1] * nn[1] + T[a][2] * nn[2];
+        tr[a] = T[a][0] * r[0] + T[a][1] * r[1] + T[a][2] * r[2];
+      }
+      txx[k] = e[0] * te[0] + e[1] * te[1] + e[2] * te[2];
+      txy[k] = e[0] * tn[0] + e[1] * tn[1] + e[2] * tn[2];
+      tyy[k] = nn[0] * tn[0] + nn[1] * tn[1] + nn[2] * tn[2];
+      txz[k] = e[0] * tr[0] + e[1] * tr[1] + e[2] * tr[2];
+      tyz[k] = nn[0] * tr[0] + nn[1] * tr[1] + nn[2] * tr[2];
+      tzz[k] = r[0] * tr[0] + r[1] * tr[1] + r[2] * tr[2];
+    }
+  }
+  orc_ddx_grid(g, ub, sxx);
+  orc_ddy_grid(g, ub, sxy);
+  orc_ddx_grid(g, vb, scr);
+  orc_ddy_grid(g, vb, syy);
+  orc_ddx_grid(g, wb, sxz);
+  orc_ddy_grid(g, wb, syz);
+  for (int j = 0; j < ny; ++j) {
+    double phi = gy_coord(g, j), sp = sin(phi), cp = cos(phi);
+    double tan_fact = sphere && fabs(cp) > 1e-12 ? sp / (g->R * cp) : 0.0;
+    for (int i = 0; i < nx; ++i) {
+      int64_t k = (int64_t)j * nx + i;
+      if (!is_active(g, i, j)) {
+        Pi[k] = 0.0;
+        continue;
+      }
+      if (sphere) {
+        sxx[k] -= vb[k] * tan_fact;
+        sxy[k] = 0.5 * (sxy[k] + scr[k] + ub[k] * tan_fact);
+      } else {
+        sxy[k] = 0.5 * (sxy[k] + scr[k]);
+      }
+      sxz[k] = 0.5 * sxz[k];
+      syz[k] = 0.5 * syz[k];
+      double szz = 0.0;
+      Pi[k] = -(sxx[k] * txx[k] + 2.0 * sxy[k] * txy[k] + syy[k] * tyy[k] + 2.0 * sxz[k] * txz[k] +
+                2.0 * syz[k] * tyz[k] + szz * tzz[k]);
+    }
+  }
+  double* src[14] = {ub, vb, wb, txx, txy, tyy, txz, tyz, tzz, sxx, sxy, syy, sxz, syz};
+  for (int q = 0; q < 14; ++q)
+    if (outs && outs[q]) memcpy(outs[q], src[q], sizeof(double) * n);
+  for (int q = 0; q < 9; ++q) {
+    free(in[q]);
+    free(f[q]);
+  }
+  free(loc);
+  free(scr);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------------------
  * Energies (Diagnostics.jl:1051-1059 active_area, 1086-1134 energy_from_filtered,
  * 1144-1217 cumulative_energy!, 1319-1333 spectral_density!).
  * ------------------------------------------------------------------------------------ */

@@ -59,6 +59,7 @@ def lib():
         L.orc_ddx.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_ddy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_compute_pi.argtypes = [C.c_void_p] + [C.c_void_p] * 11 + [C.c_int]
+        L.orc_compute_pi_w.argtypes = [C.c_void_p] * 6 + [C.c_int]
         L.orc_active_area.argtypes = [C.c_void_p]
         L.orc_active_area.restype = C.c_double
         L.orc_energy_from_filtered.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]
@@ -192,6 +193,17 @@ class Plan:
         names = ["Pi", "ubar", "vbar", "tau_xx", "tau_xy", "tau_yy", "S_xx", "S_xy", "S_yy"]
         out = {k: np.zeros_like(u) for k in names}
         lib().orc_compute_pi(self.h, _ptr(u), _ptr(v), *[_ptr(out[k]) for k in names], nthreads)
+        return out
+
+    W_OUTPUTS = ["ubar", "vbar", "wbar", "tau_xx", "tau_xy", "tau_yy", "tau_xz", "tau_yz", "tau_zz",
+                 "S_xx", "S_xy", "S_yy", "S_xz", "S_yz"]
+
+    def compute_pi_w(self, u: np.ndarray, v: np.ndarray, w: np.ndarray, nthreads: int = 1) -> dict:
+        """compute_Pi! with the vertical velocity (the 2.5-D path): Pi and the 14 local fields."""
+        u, v, w = _f64(u), _f64(v), _f64(w)
+        out = {k: np.zeros_like(u) for k in ["Pi"] + self.W_OUTPUTS}
+        arr = (C.c_void_p * 14)(*[out[k].ctypes.data for k in self.W_OUTPUTS])
+        lib().orc_compute_pi_w(self.h, _ptr(u), _ptr(v), _ptr(w), _ptr(out["Pi"]), arr, nthreads)
         return out
 
     def active_area(self) -> float:

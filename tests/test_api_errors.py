@@ -70,8 +70,14 @@ def test_compute_pi_batch_errors():
     with pytest.raises(cg.DimensionMismatch):
         cg.compute_Pi(None, np.zeros((Nb, N, N)), np.zeros((Nb, N, N)), None, g, k, 4e3,
                       slice_masks=np.ones((Nb + 1, N, N), bool))
+    # the vertical velocity (2.5-D path) must match u's batch and dtype too
+    with pytest.raises(cg.DimensionMismatch):
+        cg.compute_Pi(None, np.zeros((Nb, N, N)), np.zeros((Nb, N, N)), np.zeros((Nb + 1, N, N)), g, k, 4e3)
     with pytest.raises(cg.ArgumentError):
-        cg.compute_Pi(None, np.zeros((N, N)), np.zeros((N, N)), np.zeros((N, N)), g, k, 4e3)
+        cg.compute_Pi(None, np.zeros((N, N)), np.zeros((N, N)), np.zeros((N, N), np.float32), g, k, 4e3)
+    with pytest.raises(cg.ArgumentError):
+        cg.compute_Pi(None, np.zeros((N, N)), np.zeros((N, N)), np.zeros((N, N)), g, k, 4e3,
+                      outputs={"tau_ww": np.zeros((N, N))})
     with pytest.raises(cg.ArgumentError):
         cg.compute_Pi(None, np.zeros((N, N)), np.zeros((N, N), np.float32), None, g, k, 4e3)
     with pytest.raises(cg.ArgumentError):
