@@ -11,8 +11,9 @@ from .diagnostics import (AbstractSpectrumPolicy, ForceSpectrum, NoSpectrum, Str
                           compute_Π_strain_convergence, cumulative_energy, ddx, ddy, filtering_spectrum,
                           gate_spectrum, spectral_density, tau_decomposition)
 from .errors import ArgumentError, DimensionMismatch
-from .filtering import (AbstractMaskStrategy, Deformable, PhysicalFilterPlan, ZeroFill, filter_apply,
-                        filter_apply_batch, filter_apply_batched, filter_field, filter_fields, plan_filter,
+from .filtering import (AbstractFilterMethod, AbstractMaskStrategy, AutoMethod, Deformable, PhysicalFilterPlan,
+                        RealSpace, Spectral, SpectralFilterPlan, ZeroFill, filter_apply, filter_apply_batch,
+                        filter_apply_batched, filter_field, filter_fields, plan_filter, resolve_method,
                         set_footprint_build)
 from .grids import Axis, CartesianGeometry, SphericalGeometry, StructuredGrid, axis
 from .kernels import (GaussianKernel, TopHatKernel, check_spectrum_kernel, kernel_radius, kernel_weight,

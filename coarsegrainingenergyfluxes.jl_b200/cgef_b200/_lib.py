@@ -25,7 +25,7 @@ BUILD_AUTO, BUILD_HOST, BUILD_DEVICE = 0, 1, 2
 CARTESIAN, SPHERICAL = 0, 1
 TOPHAT, GAUSSIAN = 0, 1
 ZEROFILL, DEFORMABLE = 0, 1
-ENGINE_AUTO, ENGINE_BANDED, ENGINE_SEPARABLE, ENGINE_PREFIXSUM = 0, 1, 2, 3
+ENGINE_AUTO, ENGINE_BANDED, ENGINE_SEPARABLE, ENGINE_PREFIXSUM, ENGINE_SPECTRAL = 0, 1, 2, 3, 4
 F64, F32 = 0, 1
 
 # Every symbol include/cgef_b200.h declares.
@@ -44,6 +44,7 @@ EXPORTED = [
     "cgef_plan_set_filter_rows", "cgef_plan_get_schedule", "cgef_plan_set_row_spectral",
     "cgef_plan_get_row_spectral", "cgef_build_arch", "cgef_plan_reset_queue", "cgef_debug_inject",
     "cgef_set_footprint_build", "cgef_plan_get_build", "cgef_compute_pi_w", "cgef_compute_pi_w_device",
+    "cgef_plan_get_transfer",
 ]
 KERNEL_STAGE, KERNEL_BANDED, KERNEL_SEPARABLE, KERNEL_PREFIX, KERNEL_STRAIN, KERNEL_CLOSURE, KERNEL_ROWSPEC = (
     0, 1, 2, 3, 4, 5, 6)
@@ -207,6 +208,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     L.cgef_plan_set_row_spectral.restype = i32
     L.cgef_plan_get_row_spectral.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
     L.cgef_plan_get_row_spectral.restype = i32
+    L.cgef_plan_get_transfer.argtypes = [vp, vp]
+    L.cgef_plan_get_transfer.restype = i32
     L.cgef_closure_create.argtypes = [C.POINTER(vp), C.c_uint64]
     L.cgef_closure_destroy.argtypes = [vp]
     L.cgef_closure_get_params.argtypes = [vp, vp]

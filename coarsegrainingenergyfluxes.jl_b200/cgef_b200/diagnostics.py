@@ -217,25 +217,36 @@ def active_area(grid: StructuredGrid) -> float:
 
 def cumulative_energy(u, v, w, grid: StructuredGrid, kernel: AbstractFilterKernel, scales: Sequence[float], *,
                       mask_strategy: AbstractMaskStrategy = ZeroFill(),
-                      filter_plans: Optional[Sequence[PhysicalFilterPlan]] = None) -> np.ndarray:
-    """Diagnostics.cumulative_energy (Diagnostics.jl:1144-1251): E(l) = 1/2 <|ubar_l|^2> with u, v
-    filtered as scalars at every scale (host arrays)."""
-    if w is not None:
-        raise ArgumentError("the vertical velocity w is outside the supported path; pass None")
+                      filter_plans: Optional[Sequence[PhysicalFilterPlan]] = None, method=None) -> np.ndarray:
+    """Diagnostics.cumulative_energy (Diagnostics.jl:1144-1251): E(l) = 1/2 <|ubar_l|^2> with u, v (and
+    w, whose wbar^2 joins the sum, Diagnostics.jl:1203-1211) filtered as scalars at every scale (host
+    arrays).  `method` as for plan_filter."""
     if tuple(u.shape) != grid.shape or tuple(v.shape) != grid.shape:
         raise DimensionMismatch(f"u and v must have the grid's shape {grid.shape}")
+    if w is not None and tuple(w.shape) != grid.shape:
+        raise DimensionMismatch(f"w must have the grid's shape {grid.shape}")
     active_area(grid)
     plans = list(filter_plans) if filter_plans is not None else [
-        plan_filter(grid, kernel, float(s), mask_strategy=mask_strategy) for s in scales]
+        plan_filter(grid, kernel, float(s), mask_strategy=mask_strategy, method=method) for s in scales]
     if len(plans) != len(scales):
         raise DimensionMismatch("one plan per scale")
     dt = A.dtype_code(u)
-    hu = np.ascontiguousarray(A.host(u))
-    hv = np.ascontiguousarray(A.host(v))
-    spec = np.zeros(len(plans), dtype=np.float64)
+    if A.dtype_code(v) != dt or (w is not None and A.dtype_code(w) != dt):
+        raise ArgumentError("u, v and w must share a dtype")
     arr = (C.c_void_p * len(plans))(*[p.handle.value for p in plans])
-    _lib.check(_lib.load().cgef_cumulative_energy(arr, len(plans), dt, hu.ctypes.data, hv.ctypes.data,
-                                                  spec.ctypes.data))
+
+    def half_energy(a, b):
+        ha = np.ascontiguousarray(A.host(a))
+        hb = np.ascontiguousarray(A.host(b))
+        e = np.zeros(len(plans), dtype=np.float64)
+        _lib.check(_lib.load().cgef_cumulative_energy(arr, len(plans), dt, ha.ctypes.data, hb.ctypes.data,
+                                                      e.ctypes.data))
+        return e
+
+    spec = half_energy(u, v)
+    if w is not None:
+        hw = A.host(w)
+        spec = spec + half_energy(hw, np.zeros_like(hw))
     return spec
 
 
@@ -258,10 +269,10 @@ def spectral_density(Cv, k) -> np.ndarray:
 
 def filtering_spectrum(u, v, w, grid: StructuredGrid, kernel: AbstractFilterKernel, scales, *, L: float = 1.0,
                        mask_strategy: AbstractMaskStrategy = ZeroFill(),
-                       policy: AbstractSpectrumPolicy = StrictSpectrum()):
+                       policy: AbstractSpectrumPolicy = StrictSpectrum(), method=None):
     """Diagnostics.filtering_spectrum (Diagnostics.jl:1292-1310) -> (k_l, dE/dk_l)."""
     compute = gate_spectrum(kernel, policy)
-    cum = cumulative_energy(u, v, w, grid, kernel, scales, mask_strategy=mask_strategy)
+    cum = cumulative_energy(u, v, w, grid, kernel, scales, mask_strategy=mask_strategy, method=method)
     kl = float(L) / np.asarray(scales, dtype=np.float64)
     if not compute:
         return kl, np.full(len(kl), np.nan)

@@ -46,6 +46,71 @@ class Deformable(AbstractMaskStrategy):
 _ENGINES = {"auto": _lib.ENGINE_AUTO, "banded": _lib.ENGINE_BANDED, "separable": _lib.ENGINE_SEPARABLE,
             "prefixsum": _lib.ENGINE_PREFIXSUM}
 _ENGINE_NAMES = {v: k for k, v in _ENGINES.items()}
+_ENGINE_NAMES[_lib.ENGINE_SPECTRAL] = "spectral"
+
+
+class AbstractFilterMethod:
+    """How the convolution is evaluated (Filtering.jl:52-85)."""
+
+    def __eq__(self, other):
+        return type(self) is type(other)
+
+    def __hash__(self):
+        return hash(type(self))
+
+    def __repr__(self):
+        return f"{type(self).__name__}()"
+
+
+class RealSpace(AbstractFilterMethod):
+    """The physical-space footprint sum, any grid and mask (Filtering.jl:58-65): the banded, separable and
+    prefix-sum engines."""
+
+
+class Spectral(AbstractFilterMethod):
+    """A periodic convolution by the kernel's transfer function (Filtering.jl:66-74, FFTWExt.jl:121-206):
+    a doubly-periodic Cartesian grid only; the output is defined on masked cells too."""
+
+
+class AutoMethod(AbstractFilterMethod):
+    """Spectral where it is the exact filter -- a Cartesian grid periodic along both axes, with transform
+    lengths the spectral engine covers -- else RealSpace (Filtering.jl:3008-3019)."""
+
+
+def _smooth(n: int) -> bool:
+    for r in (2, 3, 5):
+        while n > 1 and n % r == 0:
+            n //= r
+    return n == 1
+
+
+def spectral_exact(grid: StructuredGrid) -> bool:
+    """Filtering._spectral_exact (Filtering.jl:2996-3004): Cartesian and periodic along both axes (the
+    axes are uniform ranges by construction here)."""
+    return (not grid.is_spherical) and bool(grid.periodic[0]) and bool(grid.periodic[1])
+
+
+def spectral_sizes_ok(grid: StructuredGrid) -> bool:
+    """The transform lengths the spectral engine covers: nx even, nx/2 and ny with prime factors 2, 3 and 5
+    only, both at most 4096."""
+    nx, ny = grid.nx, grid.ny
+    return nx % 2 == 0 and nx <= 4096 and ny <= 4096 and _smooth(nx // 2) and _smooth(ny)
+
+
+def resolve_method(grid: StructuredGrid, kernel: AbstractFilterKernel, method) -> AbstractFilterMethod:
+    """Filtering._resolve_method (Filtering.jl:3012-3019); also accepts "realspace", "spectral", "auto"."""
+    if method is None:
+        return RealSpace()
+    if isinstance(method, str):
+        named = {"realspace": RealSpace(), "spectral": Spectral(), "auto": AutoMethod()}.get(method.lower())
+        if named is None:
+            raise ArgumentError("method must be RealSpace(), Spectral() or AutoMethod()")
+        method = named
+    if not isinstance(method, AbstractFilterMethod):
+        raise ArgumentError("method must be RealSpace(), Spectral() or AutoMethod()")
+    if isinstance(method, AutoMethod):
+        return Spectral() if spectral_exact(grid) and spectral_sizes_ok(grid) else RealSpace()
+    return method
 
 
 def _validate_scale(scale: float) -> None:
@@ -57,6 +122,8 @@ def _validate_scale(scale: float) -> None:
 class PhysicalFilterPlan:
     """A prebuilt, device-resident filter (Filtering.jl:2894-2901)."""
 
+    _engine_code = None  # set by subclasses that fix the engine
+
     def __init__(self, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float,
                  mask_strategy: AbstractMaskStrategy = ZeroFill(), engine: str = "auto"):
         if not isinstance(grid, StructuredGrid):
@@ -64,14 +131,15 @@ class PhysicalFilterPlan:
         if not isinstance(kernel, (TopHatKernel, GaussianKernel)):
             raise ArgumentError(f"{type(kernel).__name__} is outside the supported path (TopHat, Gaussian)")
         _validate_scale(float(scale))
-        if engine not in _ENGINES:
+        if self._engine_code is None and engine not in _ENGINES:
             raise ArgumentError(f"engine must be one of {sorted(_ENGINES)}")
+        code = self._engine_code if self._engine_code is not None else _ENGINES[engine]
         L = _lib.load()
         keep: list = []
         desc = grid._desc(keep)
         h = C.c_void_p()
         _lib.check(L.cgef_plan_create(C.byref(h), C.byref(desc), kernel.code, float(kernel.alpha), float(scale),
-                                      mask_strategy.code, _ENGINES[engine]))
+                                      mask_strategy.code, code))
         self._h = h
         self.grid = grid
         self.kernel = kernel
@@ -170,6 +238,29 @@ class PhysicalFilterPlan:
                 f"strategy={self.strategy!r})")
 
 
+class SpectralFilterPlan(PhysicalFilterPlan):
+    """A spectral-method plan (the FFTW extension's FFTWFilterPlan, FFTWExt.jl:19-49): the transforms and
+    the transfer function Ghat(|k|, l) on the rfft grid, resident on the GPU.  Applies through the same
+    calls as a real-space plan; its output is defined on masked cells too."""
+
+    _engine_code = _lib.ENGINE_SPECTRAL
+
+    def __init__(self, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float,
+                 mask_strategy: AbstractMaskStrategy = ZeroFill()):
+        if not spectral_exact(grid):
+            # FFTWExt.jl:130-135
+            raise ArgumentError("Spectral FFT filtering requires a doubly-periodic Cartesian grid; build it with "
+                                "periodic=(True, True)")
+        super().__init__(grid, kernel, scale, mask_strategy)
+
+    def transfer(self) -> np.ndarray:
+        """Ghat(|k|, l) on the rfft grid, (ny, nx // 2 + 1), as the host computed it for the device."""
+        ny, nk = self.grid.ny, self.grid.nx // 2 + 1
+        out = np.zeros((ny, nk), np.float64)
+        _lib.check(_lib.load().cgef_plan_get_transfer(self.handle, out.ctypes.data))
+        return out
+
+
 def set_footprint_build(where: str = "auto") -> None:
     """Where later plans build large spherical footprints: "auto" (the default: on the device from about
     2e6 half-row weights), "host" or "device".  The entry set is decided on the host either way; see
@@ -181,9 +272,18 @@ def set_footprint_build(where: str = "auto") -> None:
 
 
 def plan_filter(grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
-                mask_strategy: AbstractMaskStrategy = ZeroFill(), engine: str = "auto") -> PhysicalFilterPlan:
-    """Filtering.plan_filter: engine dispatched as the reference does (Gaussian on the plane ->
-    separable, top-hat -> prefix sum, Gaussian on the sphere -> banded footprint)."""
+                mask_strategy: AbstractMaskStrategy = ZeroFill(), engine: str = "auto",
+                method=None) -> PhysicalFilterPlan:
+    """Filtering.plan_filter (Filtering.jl:2931-2954): `method` RealSpace() (the default) dispatches the
+    engine as the reference does (Gaussian on the plane -> separable, top-hat -> prefix sum, Gaussian on
+    the sphere -> banded footprint); Spectral() builds a SpectralFilterPlan; AutoMethod() picks Spectral()
+    where it is the exact filter."""
+    m = resolve_method(grid, kernel, method)
+    if isinstance(m, Spectral):
+        if engine != "auto":
+            raise ArgumentError("engine selects a real-space engine; it cannot be combined with Spectral()")
+        _validate_scale(float(scale))
+        return SpectralFilterPlan(grid, kernel, scale, mask_strategy)
     return PhysicalFilterPlan(grid, kernel, scale, mask_strategy, engine)
 
 
@@ -253,14 +353,18 @@ def filter_apply_batch(outs: Optional[Sequence], fields: Sequence, plan: Physica
 
 
 def filter_field(out, field, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
-                 mask_strategy: AbstractMaskStrategy = ZeroFill(), filter_plan: Optional[PhysicalFilterPlan] = None):
-    """Filtering.filter_field! (Filtering.jl:168-217): plan (unless given) then apply."""
-    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy)
+                 mask_strategy: AbstractMaskStrategy = ZeroFill(), filter_plan: Optional[PhysicalFilterPlan] = None,
+                 method=None):
+    """Filtering.filter_field! (Filtering.jl:168-217, 276-290): plan (unless given) then apply."""
+    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy,
+                                                                   method=method)
     return filter_apply(out, field, plan)
 
 
 def filter_fields(outs, fields, grid: StructuredGrid, kernel: AbstractFilterKernel, scale: float, *,
-                  mask_strategy: AbstractMaskStrategy = ZeroFill(), filter_plan: Optional[PhysicalFilterPlan] = None):
+                  mask_strategy: AbstractMaskStrategy = ZeroFill(), filter_plan: Optional[PhysicalFilterPlan] = None,
+                  method=None):
     """Filtering.filter_fields!: several fields sharing one plan."""
-    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy)
+    plan = filter_plan if filter_plan is not None else plan_filter(grid, kernel, scale, mask_strategy=mask_strategy,
+                                                                   method=method)
     return filter_apply_batch(outs, fields, plan)

@@ -64,13 +64,30 @@ class CoarseGrainBatchResult:
         return out
 
 
-def _plans(grid, kernel, scales, mask_strategy, filter_plans):
+def _plans(grid, kernel, scales, mask_strategy, filter_plans, method=None):
     if filter_plans is not None:
         plans = list(filter_plans)
         if len(plans) != len(scales):
             raise DimensionMismatch("filter_plans must hold one plan per scale")
         return plans
-    return [plan_filter(grid, kernel, float(s), mask_strategy=mask_strategy) for s in scales]
+    return [plan_filter(grid, kernel, float(s), mask_strategy=mask_strategy, method=method) for s in scales]
+
+
+def _sweep_w(u, v, w, grid, plans, nb, slice_masks, want_pi=True):
+    """The sweep with the vertical velocity: compute_Pi with w per scale (cgef_compute_pi_w) over the
+    whole batch; E includes wbar^2 (Diagnostics.jl:1125-1134)."""
+    from .diagnostics import compute_Pi
+
+    ns = len(plans)
+    ny, nx = grid.shape
+    Pi = np.empty((nb, ns, ny, nx), dtype=np.asarray(u).dtype)
+    E = np.empty((nb, ns), dtype=np.float64)
+    e = np.empty(nb, dtype=np.float64)
+    for q, p in enumerate(plans):
+        Pi[:, q] = compute_Pi(None, u, v, w, grid, p.kernel, p.scale, filter_plan=p, energy=e,
+                              slice_masks=slice_masks)
+        E[:, q] = e
+    return (Pi if want_pi else None), E
 
 
 def _sweep(u, v, grid, plans, nb, slice_masks, want_pi=True):
@@ -108,16 +125,20 @@ def _spectrum(E, k, spectrum):
 def coarse_grain(u, v, grid: StructuredGrid, *, scales: Sequence[float], w=None,
                  kernel: AbstractFilterKernel = TopHatKernel(), mask_strategy: AbstractMaskStrategy = ZeroFill(),
                  filter_plans: Optional[Sequence[PhysicalFilterPlan]] = None, L: float = 1.0,
-                 spectrum: AbstractSpectrumPolicy = StrictSpectrum()) -> CoarseGrainResult:
-    """Pipeline.coarse_grain (Pipeline.jl:342-360, 412-468) for one (ny, nx) slice."""
-    if w is not None:
-        raise ArgumentError("the vertical velocity w is outside the supported path; pass None")
+                 spectrum: AbstractSpectrumPolicy = StrictSpectrum(), method=None) -> CoarseGrainResult:
+    """Pipeline.coarse_grain (Pipeline.jl:342-360, 412-468) for one (ny, nx) slice; `w` (the vertical
+    velocity) runs the 2.5-D flux, `method` is plan_filter's."""
     if tuple(u.shape) != grid.shape or tuple(v.shape) != grid.shape:
         raise DimensionMismatch(f"u and v must have the grid's shape {grid.shape}")
+    if w is not None and tuple(w.shape) != grid.shape:
+        raise DimensionMismatch(f"w must have the grid's shape {grid.shape}")
     gate_spectrum(kernel, spectrum)
     scales = np.asarray(scales, dtype=np.float64)
-    plans = _plans(grid, kernel, scales, mask_strategy, filter_plans)
-    Pi, E = _sweep(u, v, grid, plans, 1, None)
+    plans = _plans(grid, kernel, scales, mask_strategy, filter_plans, method)
+    if w is not None:
+        Pi, E = _sweep_w(np.asarray(u)[None], np.asarray(v)[None], np.asarray(w)[None], grid, plans, 1, None)
+    else:
+        Pi, E = _sweep(u, v, grid, plans, 1, None)
     k = float(L) / scales
     return CoarseGrainResult(scales.copy(), Pi[0], E[0], k, _spectrum(E[0], k, spectrum))
 
@@ -126,21 +147,27 @@ def coarse_grain_batch(u, v, grid: StructuredGrid, *, scales: Sequence[float], w
                        kernel: AbstractFilterKernel = TopHatKernel(),
                        mask_strategy: AbstractMaskStrategy = ZeroFill(),
                        filter_plans: Optional[Sequence[PhysicalFilterPlan]] = None, L: float = 1.0,
-                       spectrum: AbstractSpectrumPolicy = StrictSpectrum(), slice_masks=None) -> CoarseGrainBatchResult:
-    """Pipeline.coarse_grain_batch! (Pipeline.jl:686-717): u, v of shape (batch..., ny, nx) share the
-    grid; the whole batch runs batch-native, one fused pass per scale (the GPU driver,
+                       spectrum: AbstractSpectrumPolicy = StrictSpectrum(), slice_masks=None,
+                       method=None) -> CoarseGrainBatchResult:
+    """Pipeline.coarse_grain_batch! (Pipeline.jl:686-717): u, v (and w) of shape (batch..., ny, nx) share
+    the grid; the whole batch runs batch-native, one fused pass per scale (the GPU driver,
     Pipeline.jl:519-563).  `slice_masks` (batch..., ny, nx) gives every slice its own mask."""
-    if w is not None:
-        raise ArgumentError("the vertical velocity w is outside the supported path; pass None")
     shp = tuple(u.shape)
     if len(shp) < 3 or shp[-2:] != grid.shape or tuple(v.shape) != shp:
         raise DimensionMismatch(f"u and v must be (batch..., {grid.ny}, {grid.nx}) and equal")
+    if w is not None and tuple(w.shape) != shp:
+        raise DimensionMismatch("w must match u's shape")
     bsz = shp[:-2]
     nb = int(np.prod(bsz))
     gate_spectrum(kernel, spectrum)
     scales = np.asarray(scales, dtype=np.float64)
-    plans = _plans(grid, kernel, scales, mask_strategy, filter_plans)
-    Pi, E = _sweep(u.reshape((nb,) + grid.shape), v.reshape((nb,) + grid.shape), grid, plans, nb, slice_masks)
+    plans = _plans(grid, kernel, scales, mask_strategy, filter_plans, method)
+    if w is not None:
+        Pi, E = _sweep_w(u.reshape((nb,) + grid.shape), v.reshape((nb,) + grid.shape), w.reshape((nb,) + grid.shape),
+                         grid, plans, nb, None if slice_masks is None else np.asarray(slice_masks).reshape(
+                             (nb,) + grid.shape))
+    else:
+        Pi, E = _sweep(u.reshape((nb,) + grid.shape), v.reshape((nb,) + grid.shape), grid, plans, nb, slice_masks)
     ns = len(scales)
     k = float(L) / scales
     spec = np.stack([_spectrum(E[t], k, spectrum) for t in range(nb)])
@@ -157,7 +184,7 @@ def coarse_grain_profile(u, v, grid: StructuredGrid, **kw) -> CoarseGrainBatchRe
 def coarse_grain_slices(us: Sequence, vs: Sequence, grids: Sequence[StructuredGrid], *, scales: Sequence[float],
                         kernel: AbstractFilterKernel = TopHatKernel(),
                         mask_strategy: AbstractMaskStrategy = ZeroFill(), L: float = 1.0,
-                        spectrum: AbstractSpectrumPolicy = StrictSpectrum()) -> List[CoarseGrainResult]:
+                        spectrum: AbstractSpectrumPolicy = StrictSpectrum(), method=None) -> List[CoarseGrainResult]:
     """Pipeline.coarse_grain_slices! (Pipeline.jl:866-904): each slice brings its own grid.  Slices whose
     grids differ only in their masks (levels under bathymetry) run as one batched sweep with a mask
     per slice; any other group runs per grid."""
@@ -178,7 +205,7 @@ def coarse_grain_slices(us: Sequence, vs: Sequence, grids: Sequence[StructuredGr
     k = float(L) / scales
     for g in groups:
         base = grids[g[0]].with_mask(None)
-        plans = _plans(base, kernel, scales, mask_strategy, None)
+        plans = _plans(base, kernel, scales, mask_strategy, None, method)
         masks = np.stack([np.ones(base.shape, np.uint8) if grids[t].mask is None else grids[t].mask.astype(np.uint8)
                           for t in g])
         u = np.stack([np.asarray(us[t]) for t in g])

@@ -151,6 +151,14 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
     return launch_banded(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(part), go, st,
                          true);
   }
+  if (p->engine == CGEF_ENGINE_SPECTRAL) {
+    const int na = 5 + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
+    void* sc = nullptr;
+    int rc = ensure_ws(p, kSlotSplit, spectral_scratch_bytes(p, na, nbatch), &sc);
+    if (rc) return rc;
+    return launch_spectral(p, mode, 0, planes, pitch, np, nbatch, mstride != 0 || p->masked, static_cast<double*>(sc),
+                           go, st);
+  }
   if (p->engine == CGEF_ENGINE_SEPARABLE) {
     const int na = 5 + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
     void* rb = nullptr;
@@ -275,6 +283,12 @@ int filter_fields_device(cgef_plan* p, int dtype, const void* const* fields, int
     void* rb = nullptr;
     if ((rc = ensure_ws(p, kSlotAux, sizeof(double) * (nf + 1) * N * nbatch, &rb))) return rc;
     return launch_separable(p, kModeFields, nf, pl, pitch, np, nbatch, mask, mstride, static_cast<double*>(rb), go, st);
+  }
+  if (p->engine == CGEF_ENGINE_SPECTRAL) {
+    void* sc = nullptr;
+    if ((rc = ensure_ws(p, kSlotSplit, spectral_scratch_bytes(p, np, nbatch), &sc))) return rc;
+    return launch_spectral(p, kModeFields, nf, pl, pitch, np, nbatch, mstride != 0 || p->masked,
+                           static_cast<double*>(sc), go, st);
   }
   void* pre = nullptr;
   if ((rc = ensure_ws(p, kSlotAux, sizeof(double) * (nf + 1) * static_cast<int64_t>(p->ny) * (p->pre_ne + 1) * nbatch,
@@ -523,7 +537,11 @@ int32_t cgef_plan_create(cgef_plan** out, const cgef_grid_desc* g, int32_t kerne
     return fail(CGEF_EUNSUPPORTED, "the separable engine needs a Gaussian kernel on a Cartesian grid");
   if (eng == CGEF_ENGINE_PREFIXSUM && kernel != CGEF_TOPHAT)
     return fail(CGEF_EUNSUPPORTED, "the prefix-sum engine needs the top-hat kernel");
-  if (eng < CGEF_ENGINE_BANDED || eng > CGEF_ENGINE_PREFIXSUM) return fail(CGEF_EINVAL, "unknown engine");
+  // FFTWExt.jl:130-135 and Filtering.jl:2998-3004: a periodic transform is the filter only on a
+  // Cartesian grid that wraps along both axes
+  if (eng == CGEF_ENGINE_SPECTRAL && (g->geometry != CGEF_CARTESIAN || !g->periodic_x || !g->periodic_y))
+    return fail(CGEF_EINVAL, "spectral FFT filtering requires a doubly-periodic Cartesian grid");
+  if (eng < CGEF_ENGINE_BANDED || eng > CGEF_ENGINE_SPECTRAL) return fail(CGEF_EINVAL, "unknown engine");
 
   cgef_plan* p = new (std::nothrow) cgef_plan();
   if (!p) return fail(CGEF_ENOMEM, "host allocation failed");
@@ -579,7 +597,8 @@ int32_t cgef_plan_destroy(cgef_plan* p) {
     void* ptrs[] = {p->d_mask, p->d_x, p->d_sinlam, p->d_coslam, p->d_sinphi, p->d_cosphi, p->d_area, p->d_xscale,
                     p->d_tanfac, p->d_rows, p->d_w, p->d_den_zf, p->sched[0].d_items, p->sched[0].d_groups,
                     p->sched[1].d_items, p->sched[1].d_groups, p->d_gx, p->d_gy, p->d_px, p->d_py, p->d_xe,
-                    p->d_prefix_wx, p->d_prows, p->d_queue, p->d_rs_tw, p->d_rs_k, p->d_rs_ptw};
+                    p->d_prefix_wx, p->d_prows, p->d_queue, p->d_rs_tw, p->d_rs_k, p->d_rs_ptw,
+                    p->d_sp_ptw, p->d_sp_T};
     for (void* q : ptrs)
       if (q) cudaFree(q);
     for (auto& b : p->ws)
@@ -627,7 +646,7 @@ int32_t cgef_plan_set_filter_rows(cgef_plan* p, int32_t rows) {
 int32_t cgef_plan_set_row_spectral(cgef_plan* p, int32_t enable) {
   int rc = check_plan(p);
   if (rc) return rc;
-  if (enable && p->rs_L == 0)
+  if (enable && (p->rs_L == 0 || p->engine != CGEF_ENGINE_BANDED))
     return fail(CGEF_EINVAL, "row-spectral evaluation is not available for this plan (banded engine on a periodic "
                              "x axis or with symmetric rows, and an even FFT length whose half has factors 2, 3, 5 "
                              "only)");
@@ -637,9 +656,17 @@ int32_t cgef_plan_set_row_spectral(cgef_plan* p, int32_t enable) {
 
 int32_t cgef_plan_get_row_spectral(const cgef_plan* p, int32_t* available, int32_t* enabled, int32_t* fft_length) {
   if (!p) return fail(CGEF_EINVAL, "plan is NULL");
-  if (available) *available = p->rs_L > 0;
-  if (enabled) *enabled = p->rs_on;
-  if (fft_length) *fft_length = p->rs_L;
+  const bool banded = p->engine == CGEF_ENGINE_BANDED;
+  if (available) *available = banded && p->rs_L > 0;
+  if (enabled) *enabled = banded && p->rs_on;
+  if (fft_length) *fft_length = banded ? p->rs_L : 0;
+  return CGEF_OK;
+}
+
+int32_t cgef_plan_get_transfer(const cgef_plan* p, double* transfer) {
+  if (!p || !transfer) return fail(CGEF_EINVAL, "plan and transfer must be non-NULL");
+  if (p->engine != CGEF_ENGINE_SPECTRAL) return fail(CGEF_EINVAL, "plan is not a spectral-method plan");
+  std::copy(p->h_sp_T.begin(), p->h_sp_T.end(), transfer);
   return CGEF_OK;
 }
 

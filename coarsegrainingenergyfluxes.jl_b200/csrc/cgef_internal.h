@@ -158,6 +158,14 @@ struct cgef_plan {
   double* d_rs_ptw = nullptr;   // per-pass twiddles, pass p at rs_poff[p] (complex), [r - 1][jm]
   int rs_poff[16] = {};
   bool rs_on = false;           // full-grid banded launches use the row-spectral evaluation
+  // spectral method (CGEF_ENGINE_SPECTRAL): the x transforms are the row-spectral ones above with
+  // rs_L = nx (no kernel spectra); the y transforms are complex FFTs of length ny over the bins
+  int sp_nrad = 0;
+  int sp_rad[16] = {};
+  int sp_poff[16] = {};
+  double* d_sp_ptw = nullptr;   // per-pass twiddles of the length-ny FFT, pass p at sp_poff[p]
+  double* d_sp_T = nullptr;     // transfer function / (nx ny): [ky row][rs_nkp bins], zero past rs_nk
+  std::vector<double> h_sp_T;   // the transfer function itself, [ky row][rs_nk bins]
   // separable engine
   int di_lim = 0, sep_dj_lim = 0;
   double* d_gx = nullptr;
@@ -321,6 +329,20 @@ struct RsShare {
 int launch_rowspec(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
                    const uint8_t* mask, int64_t mask_slice_stride, double* scratch, const GatherOut& out,
                    cudaStream_t st, const RsShare& share = RsShare{}, bool leave_raw = false);
+
+// The spectral method (CGEF_ENGINE_SPECTRAL) over staged planes: the row transforms of the row-spectral
+// evaluation (L = nx), a column pass per bin that transforms along y, multiplies by the transfer
+// function and transforms back, the inverse row transforms, and an epilogue that applies Deformable's
+// renormalisation (`renorm`) and forms tau in the flux mode.  Every cell gets a value.  `scratch`
+// holds spectral_scratch_bytes().
+int launch_spectral(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                    bool renorm, double* scratch, const GatherOut& out, cudaStream_t st);
+inline size_t spectral_scratch_bytes(const cgef_plan* p, int na, int nbatch) {
+  return 2 * 2 * sizeof(double) * static_cast<size_t>(nbatch) * p->ny * na * p->rs_nkp;
+}
+// Builds the spectral method's transforms and transfer function (CGEF_EUNSUPPORTED for lengths the
+// transforms do not cover).
+int build_spectral(cgef_plan* p);
 
 // Bytes of one sweep's shared source spectra: `na` quantities over `nbatch` slices.
 inline size_t rowspec_spectra_bytes(const cgef_plan* p, int na, int nbatch) {

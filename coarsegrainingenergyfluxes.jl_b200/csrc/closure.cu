@@ -1057,6 +1057,7 @@ int32_t cgef_closure_pairs_device(cgef_plan* p, int32_t dtype, const void* u, co
                                   const uint8_t* slice_masks, float* features, float* targets, void* stream) {
   int rc;
   if ((rc = check_plan(p)) || (rc = check_dtype(dtype))) return rc;
+  if (p->engine == CGEF_ENGINE_SPECTRAL) return fail(CGEF_EUNSUPPORTED, "the learned closure runs on real-space plans");
   if (!u || !v || !features || !targets) return fail(CGEF_EINVAL, "u, v, features and targets must be non-NULL");
   if (nbatch64 < 1 || nbatch64 > 65535) return fail(CGEF_EINVAL, "nbatch must be in 1..65535");
   DeviceGuard dg(p->device);
@@ -1099,6 +1100,7 @@ int32_t cgef_closure_pi_device(cgef_closure* c, cgef_plan* p, int32_t dtype, con
                                double tol, void* pi, cgef_closure_report* report, void* stream) {
   int rc;
   if ((rc = check_closure(c)) || (rc = check_plan(p)) || (rc = check_dtype(dtype))) return rc;
+  if (p->engine == CGEF_ENGINE_SPECTRAL) return fail(CGEF_EUNSUPPORTED, "the learned closure runs on real-space plans");
   if (!u || !v || !pi) return fail(CGEF_EINVAL, "u, v and pi must be non-NULL");
   if (nbatch64 < 1 || nbatch64 > 65535) return fail(CGEF_EINVAL, "nbatch must be in 1..65535");
   if (!(judge_fraction >= 0.0 && judge_fraction <= 1.0)) return fail(CGEF_EINVAL, "judge_fraction must be in [0, 1]");

@@ -78,6 +78,7 @@ extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const
   if (p->engine == CGEF_ENGINE_PREFIXSUM)
     engine_b = round256(sizeof(double) * 2 * static_cast<size_t>(p->ny) * (p->pre_ne + 1) * nbatch);
   if (p->engine == CGEF_ENGINE_BANDED) engine_b = round256(banded_partials_bytes(p, np, nbatch, kModeFields));
+  if (p->engine == CGEF_ENGINE_SPECTRAL) engine_b = round256(spectral_scratch_bytes(p, np, nbatch));
   const size_t result_b = dtype == CGEF_F64 ? 0 : round256(sizeof(double) * static_cast<size_t>(N) * nbatch);
   const size_t need = planes_b + engine_b + result_b;
   if (need > kNoallocScratchBytes)
@@ -115,6 +116,8 @@ extern "C" int32_t cgef_filter_device_noalloc(cgef_plan* p, int32_t dtype, const
                           true);
       else if (p->engine == CGEF_ENGINE_SEPARABLE)
         rc = launch_separable(p, kModeFields, 1, planes, pitch, np, nbatch, p->d_mask, 0, aux, go, st);
+      else if (p->engine == CGEF_ENGINE_SPECTRAL)
+        rc = launch_spectral(p, kModeFields, 1, planes, pitch, np, nbatch, p->masked, aux, go, st);
       else
         rc = launch_prefix(p, kModeFields, 1, planes, pitch, np, nbatch, p->d_mask, 0, aux, go, st);
     }

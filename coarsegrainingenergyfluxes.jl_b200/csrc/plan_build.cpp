@@ -672,6 +672,10 @@ int build_plan_tables(cgef_plan* p) {
     if ((rc = upload(p, &p->d_gy, gy.data(), gy.size())) != CGEF_OK) return rc;
     if ((rc = upload(p, &p->d_px, px.data(), px.size())) != CGEF_OK) return rc;
     if ((rc = upload(p, &p->d_py, py.data(), py.size())) != CGEF_OK) return rc;
+  } else if (p->engine == CGEF_ENGINE_SPECTRAL) {
+    // FFTWExt.jl:121-181: the transforms and the transfer function on the rfft grid
+    p->H = 1;
+    if (int rc = build_spectral(p)) return rc;
   } else {
     // Prefix-sum top-hat (Filtering.jl:833-907): measure factors, the tripled periodic axis,
     // the row band and per (row, band slot) the support half-width (Filtering.jl:990-1005).

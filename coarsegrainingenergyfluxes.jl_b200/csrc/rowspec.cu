@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <mutex>
 #include <set>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -798,6 +799,274 @@ int smooth_length(int n) {
   }
 }
 
+bool is_smooth(int n) { return n >= 1 && smooth_length(n) == n; }
+
+// exp(-2 pi i n / L), n < L, as (re, im) pairs.
+std::vector<double> roots_table(int L) {
+  std::vector<double> tw(2 * static_cast<size_t>(L));
+  for (int n = 0; n < L; ++n) {
+    const double ang = 2.0 * 3.14159265358979323846 * (static_cast<double>(n) / L);
+    tw[2 * n] = std::cos(ang);
+    tw[2 * n + 1] = -std::sin(ang);
+  }
+  return tw;
+}
+
+// Per-pass twiddles of a Stockham plan with radices `rad` whose roots are those of `tw` (length L): pass
+// p (Ns = the product of the earlier radices) multiplies element r of butterfly jm by exp(-2 pi i jm r /
+// (Ns R)), entry jm r L / (Ns R) of tw; laid out [r - 1][jm] from poff[p].
+std::vector<double> pass_twiddles(const std::vector<int>& rad, const std::vector<double>& tw, int L, int* poff) {
+  std::vector<double> ptw;
+  int ns = 1;
+  for (size_t q = 0; q < rad.size(); ++q) {
+    const int R = rad[q];
+    poff[q] = static_cast<int>(ptw.size() / 2);
+    for (int r = 1; r < R; ++r)
+      for (int jm = 0; jm < ns; ++jm) {
+        const int64_t n = static_cast<int64_t>(jm) * r * L / (static_cast<int64_t>(ns) * R);
+        ptw.push_back(tw[2 * n]);
+        ptw.push_back(tw[2 * n + 1]);
+      }
+    ns *= R;
+  }
+  return ptw;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// The spectral method (CGEF_ENGINE_SPECTRAL; ext/CoarseGrainingEnergyFluxesFFTWExt.jl:121-206): a
+// 2-D real DFT as the row transforms above (L = nx), then per spectrum bin a complex DFT along y, the
+// transfer function and the inverse along y (sp_column_kernel, in place), the inverse row transforms,
+// and sp_finish_kernel.
+// ---------------------------------------------------------------------------------------------------
+constexpr int kSpThreads = 256;
+constexpr int kSpMaxN = 4096;                 // longest y transform
+constexpr int kSpSmemMax = 200 * 1024;        // shared memory the column kernel may use
+constexpr int kSpSmemTarget = 96 * 1024;      // what it aims for (two blocks an SM)
+
+struct SpK {
+  double2* Q;       // [slice][row][m][bin]: the rows' spectra in, the filtered spectra out
+  const double* T;  // transfer / (nx ny): [ky row][nkp]
+  int ny, na, nk, nkp, cb;
+  int nrad;
+  int rad[16];
+  unsigned magic[16];
+  int poff[16];
+  const double2* ptw;
+};
+
+// One Stockham pass (as stockham_pass) of a length-n complex FFT over nseq sequences `ss` elements apart.
+template <int R>
+__device__ __forceinline__ void col_pass(const double2* a, double2* b, int n, int ss, int Ns, unsigned ns_magic,
+                                         int nseq, const double2* ptw) {
+  const int nb = n / R;
+  for (int t = threadIdx.x; t < nseq * nb; t += blockDim.x) {
+    const int sq = t / nb, j = t - sq * nb;
+    const double2* as = a + sq * ss;
+    const int jq = Ns == 1 ? j : static_cast<int>(__umulhi(static_cast<unsigned>(j), ns_magic));
+    const int jm = j - jq * Ns;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = as[j + r * nb];
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(ptw + (r - 1) * Ns + jm));
+    dft<R>(v);
+    double2* bs = b + sq * ss + jq * Ns * R + jm;
+#pragma unroll
+    for (int r = 0; r < R; ++r) bs[r * Ns] = v[r];
+  }
+}
+
+// Forward DFTs of nseq length-ny sequences in `a` (shared memory, `ss` apart), `b` as scratch; returns
+// the buffer holding them.  Every thread of the block must call it.
+__device__ __forceinline__ double2* col_fft(double2* a, double2* b, int nseq, int ss, const SpK& k) {
+  int Ns = 1;
+  for (int p = 0; p < k.nrad; ++p) {
+    const int R = k.rad[p];
+    const unsigned mg = k.magic[p];
+    const double2* tp = k.ptw + k.poff[p];
+    switch (R) {
+      case 2: col_pass<2>(a, b, k.ny, ss, Ns, mg, nseq, tp); break;
+      case 3: col_pass<3>(a, b, k.ny, ss, Ns, mg, nseq, tp); break;
+      case 4: col_pass<4>(a, b, k.ny, ss, Ns, mg, nseq, tp); break;
+      case 5: col_pass<5>(a, b, k.ny, ss, Ns, mg, nseq, tp); break;
+      case 8: col_pass<8>(a, b, k.ny, ss, Ns, mg, nseq, tp); break;
+      case 9: col_pass<9>(a, b, k.ny, ss, Ns, mg, nseq, tp); break;
+      case 10: col_pass<10>(a, b, k.ny, ss, Ns, mg, nseq, tp); break;
+      default: col_pass<16>(a, b, k.ny, ss, Ns, mg, nseq, tp); break;
+    }
+    __syncthreads();
+    double2* t = a;
+    a = b;
+    b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
+// One block per (cb bins, quantity, slice): the bins' columns of row spectra (coalesced: a row's cb
+// bins are adjacent), DFT along y, times Ghat(|k|) / (nx ny), inverse DFT along y as conj(DFT(conj)),
+// stored back in place.  Sequences sit ny + 1 elements apart in shared memory (no bank aliasing of the
+// transposing loads and stores).
+__global__ void __launch_bounds__(kSpThreads) sp_column_kernel(SpK k) {
+  extern __shared__ double2 rs_smem[];
+  const int q0 = blockIdx.x * k.cb, m = blockIdx.y, s = blockIdx.z;
+  const int nseq = min(k.cb, k.nk - q0);
+  const int ny = k.ny, ss = ny + 1;
+  double2* a = rs_smem;
+  double2* b = rs_smem + k.cb * ss;
+  const int64_t rstride = static_cast<int64_t>(k.na) * k.nkp;
+  double2* base = k.Q + static_cast<int64_t>(s) * ny * rstride + static_cast<int64_t>(m) * k.nkp + q0;
+  for (int t = threadIdx.x; t < nseq * ny; t += blockDim.x) {
+    const int r = t / nseq, e = t - r * nseq;
+    a[e * ss + r] = base[r * rstride + e];
+  }
+  __syncthreads();
+  double2* x = col_fft(a, b, nseq, ss, k);
+  for (int t = threadIdx.x; t < nseq * ny; t += blockDim.x) {
+    const int e = t / ny, r = t - e * ny;
+    const double g = __ldg(k.T + static_cast<int64_t>(r) * k.nkp + q0 + e);
+    const double2 v = x[e * ss + r];
+    x[e * ss + r] = make_double2(v.x * g, -(v.y * g));  // conj(X g)
+  }
+  __syncthreads();
+  double2* y = col_fft(x, x == a ? b : a, nseq, ss, k);
+  for (int t = threadIdx.x; t < nseq * ny; t += blockDim.x) {
+    const int r = t / nseq, e = t - r * nseq;
+    const double2 v = y[e * ss + r];
+    base[r * rstride + e] = make_double2(v.x, -v.y);
+  }
+}
+
+struct SpFin {
+  const double* F;  // [slice][m][row][nx], the filtered quantities
+  int nx, ny, renorm;
+  GatherOut go;
+};
+
+// Per cell: Deformable's renormalisation, 1 / filter(mask) where |filter(mask)| >= 0.01 and 0 elsewhere
+// (FFTWExt.jl:163-173, 201), applied to every filtered quantity; the flux mode then forms
+// tau_ij = (u_i u_j)bar - ubar_i ubar_j (Diagnostics.jl:525-535).  Every cell is written.
+template <int MODE, int NF, bool DEF>
+__global__ void __launch_bounds__(128) sp_finish_kernel(SpFin f) {
+  using C = Cfg<MODE, NF, DEF>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, s = blockIdx.z;
+  if (i >= f.nx) return;
+  const int64_t plane = static_cast<int64_t>(f.ny) * f.nx;
+  const int64_t pix = static_cast<int64_t>(j) * f.nx + i;
+  const double* src = f.F + static_cast<int64_t>(s) * C::NA * plane + pix;
+  double v[C::NA];
+#pragma unroll
+  for (int m = 0; m < C::NA; ++m) v[m] = src[m * plane];
+  double ir = 1.0;
+  if (DEF && f.renorm) {
+    const double r = v[C::NA - 1];
+    ir = fabs(r) >= 0.01 ? 1.0 / r : 0.0;
+  }
+  const int64_t o = static_cast<int64_t>(s) * f.go.slice_stride + pix;
+  if constexpr (MODE == kModePiCart) {
+    const double ub = v[0] * ir, vb = v[1] * ir;
+    f.go.o[0][o] = ub;
+    f.go.o[1][o] = vb;
+    f.go.o[2][o] = v[2] * ir - ub * ub;
+    f.go.o[3][o] = v[3] * ir - ub * vb;
+    f.go.o[4][o] = v[4] * ir - vb * vb;
+  } else {
+#pragma unroll
+    for (int m = 0; m < NF; ++m) f.go.o[m][o] = v[m] * ir;
+  }
+}
+
+int sp_smem_attr() {
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(dev)) return CGEF_OK;
+  cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(sp_column_kernel),
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSpSmemMax);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(spectral column kernel)");
+  done.insert(dev);
+  return CGEF_OK;
+}
+
+// Bins a column block takes: the most (16 at most) whose two buffers fit kSpSmemTarget, else one.
+int spectral_cb(int ny) {
+  for (int cb = 16; cb > 1; cb /= 2)
+    if (2 * cb * (ny + 1) * static_cast<int>(sizeof(double2)) <= kSpSmemTarget) return cb;
+  return 1;
+}
+
+template <int MODE, int NF, bool DEF>
+int run_spectral(const cgef_plan* p, const double* planes, int pitch, int np, int nbatch, bool renorm, double* scratch,
+                 const GatherOut& go, cudaStream_t st) {
+  using C = Cfg<MODE, NF, DEF>;
+  constexpr int NA = C::NA;
+  constexpr int NC = (NA + kRsSeq - 1) / kRsSeq;
+  RsK k{};
+  k.f = make_fft(p);
+  k.planes = planes;
+  k.plane_stride = static_cast<int64_t>(p->ny) * pitch;
+  k.slice_stride = np * k.plane_stride;
+  k.pitch = pitch;
+  k.halo = p->H;
+  k.nx = p->nx;
+  k.ny = p->ny;
+  k.periodic_y = 1;
+  k.nslices = nbatch;
+  const size_t spec = static_cast<size_t>(nbatch) * p->ny * NA * p->rs_nkp;  // complex bins
+  k.Q = reinterpret_cast<double2*>(scratch);
+  k.S = k.Q;              // the column pass filters the row spectra in place
+  k.F = scratch + 2 * spec;
+  SpK c{};
+  c.Q = k.Q;
+  c.T = p->d_sp_T;
+  c.ny = p->ny;
+  c.na = NA;
+  c.nk = p->rs_nk;
+  c.nkp = p->rs_nkp;
+  c.cb = spectral_cb(p->ny);
+  c.nrad = p->sp_nrad;
+  for (int i = 0, ns = 1; i < p->sp_nrad; ++i) {
+    c.rad[i] = p->sp_rad[i];
+    c.magic[i] = ns == 1 ? 0u : static_cast<unsigned>(((uint64_t(1) << 32) + ns - 1) / ns);
+    c.poff[i] = p->sp_poff[i];
+    ns *= p->sp_rad[i];
+  }
+  c.ptw = reinterpret_cast<const double2*>(p->d_sp_ptw);
+  SpFin fin{};
+  fin.F = k.F;
+  fin.nx = p->nx;
+  fin.ny = p->ny;
+  fin.renorm = renorm ? 1 : 0;
+  fin.go = go;
+  const int smem = 2 * kRsSeq * static_cast<int>(sizeof(double2)) * (p->rs_L / 2);
+  const int csmem = 2 * c.cb * (p->ny + 1) * static_cast<int>(sizeof(double2));
+  int rc;
+  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_forward_kernel<MODE, NF, DEF>))) != CGEF_OK) return rc;
+  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_inverse_kernel<NA>))) != CGEF_OK) return rc;
+  if ((rc = sp_smem_attr()) != CGEF_OK) return rc;
+  prof_begin(CGEF_KERNEL_ROWSPEC, st);
+  const dim3 rows(NC, p->ny, nbatch);
+  rs_forward_kernel<MODE, NF, DEF><<<rows, kRsThreads, smem, st>>>(k);
+  rc = rs_check("rs_forward_kernel");
+  if (rc == CGEF_OK) {
+    sp_column_kernel<<<dim3((c.nk + c.cb - 1) / c.cb, NA, nbatch), kSpThreads, csmem, st>>>(c);
+    rc = rs_check("sp_column_kernel");
+  }
+  if (rc == CGEF_OK) {
+    rs_inverse_kernel<NA><<<rows, kRsThreads, smem, st>>>(k);
+    rc = rs_check("rs_inverse_kernel");
+  }
+  if (rc == CGEF_OK) {
+    sp_finish_kernel<MODE, NF, DEF><<<dim3((p->nx + 127) / 128, p->ny, nbatch), 128, 0, st>>>(fin);
+    rc = rs_check("sp_finish_kernel");
+  }
+  prof_end(CGEF_KERNEL_ROWSPEC, st);
+  return rc;
+}
+
 }  // namespace
 
 int launch_rowspec(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
@@ -839,30 +1108,10 @@ int build_row_spectra(cgef_plan* p) {
   const size_t kbytes = sizeof(double) * static_cast<size_t>(nrows) * nkp;
   if (kbytes > (size_t(8) << 30)) return CGEF_OK;
 
-  std::vector<double> tw(2 * static_cast<size_t>(L));
-  for (int n = 0; n < L; ++n) {
-    const double ang = 2.0 * 3.14159265358979323846 * (static_cast<double>(n) / L);
-    tw[2 * n] = std::cos(ang);
-    tw[2 * n + 1] = -std::sin(ang);
-  }
-  // per-pass twiddles of the half-length transform: pass p (Ns = the product of the earlier radices)
-  // multiplies element r of butterfly jm by exp(-2 pi i jm r / (Ns R)), entry jm r L / (Ns R) of tw
-  std::vector<double> ptw;
+  const std::vector<double> tw = roots_table(L);
+  // per-pass twiddles of the half-length transform
   int poff[16] = {};
-  {
-    int ns = 1;
-    for (size_t q = 0; q < rad.size(); ++q) {
-      const int R = rad[q];
-      poff[q] = static_cast<int>(ptw.size() / 2);
-      for (int r = 1; r < R; ++r)
-        for (int jm = 0; jm < ns; ++jm) {
-          const int64_t n = static_cast<int64_t>(jm) * r * L / (static_cast<int64_t>(ns) * R);
-          ptw.push_back(tw[2 * n]);
-          ptw.push_back(tw[2 * n + 1]);
-        }
-      ns *= R;
-    }
-  }
+  const std::vector<double> ptw = pass_twiddles(rad, tw, L, poff);
   DeviceGuard dg(p->device);
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p->d_rs_tw), tw.size() * sizeof(double));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(row-spectral twiddles)");
@@ -905,6 +1154,90 @@ int build_row_spectra(cgef_plan* p) {
     return rc;
   }
   p->rs_on = true;
+  return CGEF_OK;
+}
+
+int launch_spectral(const cgef_plan* p, int mode, int nf, const double* planes, int pitch, int np, int nbatch,
+                    bool renorm, double* scratch, const GatherOut& out, cudaStream_t st) {
+  if (p->engine != CGEF_ENGINE_SPECTRAL || p->d_sp_T == nullptr)
+    return fail(CGEF_EINVAL, "spectral method not built for this plan");
+  if (scratch == nullptr) return fail(CGEF_EINVAL, "spectral method needs its scratch buffer");
+  const bool def = p->strategy == CGEF_DEFORMABLE;
+  if (mode == kModePiCart)
+    return def ? run_spectral<kModePiCart, 1, true>(p, planes, pitch, np, nbatch, renorm, scratch, out, st)
+               : run_spectral<kModePiCart, 1, false>(p, planes, pitch, np, nbatch, renorm, scratch, out, st);
+  if (mode != kModeFields) return fail(CGEF_EUNSUPPORTED, "the spectral method is defined on the plane only");
+  switch (nf) {
+    case 1: return def ? run_spectral<kModeFields, 1, true>(p, planes, pitch, np, nbatch, renorm, scratch, out, st)
+                       : run_spectral<kModeFields, 1, false>(p, planes, pitch, np, nbatch, renorm, scratch, out, st);
+    case 2: return def ? run_spectral<kModeFields, 2, true>(p, planes, pitch, np, nbatch, renorm, scratch, out, st)
+                       : run_spectral<kModeFields, 2, false>(p, planes, pitch, np, nbatch, renorm, scratch, out, st);
+    case 3: return def ? run_spectral<kModeFields, 3, true>(p, planes, pitch, np, nbatch, renorm, scratch, out, st)
+                       : run_spectral<kModeFields, 3, false>(p, planes, pitch, np, nbatch, renorm, scratch, out, st);
+    case 4: return def ? run_spectral<kModeFields, 4, true>(p, planes, pitch, np, nbatch, renorm, scratch, out, st)
+                       : run_spectral<kModeFields, 4, false>(p, planes, pitch, np, nbatch, renorm, scratch, out, st);
+    default: return fail(CGEF_EINVAL, "spectral method: 1..4 fields per pass");
+  }
+}
+
+// FFTWExt.jl:121-181: the transforms' tables and Ghat(|k|, l) on the rfft grid (Kernels.jl:394-406;
+// the top-hat's Bessel form, SpecialFunctionsExt.jl:10-17, through std::cyl_bessel_j), divided by
+// nx ny so the unnormalised transforms there and back give the filter.
+int build_spectral(cgef_plan* p) {
+  const int nx = p->nx, ny = p->ny;
+  if (nx % 2 != 0 || nx > kRsMaxL || ny > kSpMaxN || !is_smooth(nx / 2) || !is_smooth(ny))
+    return fail(CGEF_EUNSUPPORTED, "the spectral method needs an even nx with nx / 2 and ny free of prime factors "
+                                   "above 5, both at most 4096 (got nx = " + std::to_string(nx) +
+                                   ", ny = " + std::to_string(ny) + ")");
+  const std::vector<int> radx = fft_radices(nx / 2), rady = fft_radices(ny);
+  if (radx.size() > 16 || rady.size() > 16) return fail(CGEF_EUNSUPPORTED, "spectral method: too many FFT passes");
+  const int nk = nx / 2 + 1;
+  const int nkp = (nk + 31) / 32 * 32;
+  std::vector<double> T(static_cast<size_t>(ny) * nkp, 0.0);
+  p->h_sp_T.assign(static_cast<size_t>(ny) * nk, 0.0);
+  const double pi2 = 2.0 * 3.14159265358979323846;
+  const double norm = 1.0 / (static_cast<double>(nx) * ny);
+  for (int r = 0; r < ny; ++r) {
+    const int mr = r < (ny + 1) / 2 ? r : r - ny;  // fftfreq order
+    const double ky = pi2 * (static_cast<double>(mr) / (ny * p->dy));
+    for (int q = 0; q < nk; ++q) {
+      const double kx = pi2 * (static_cast<double>(q) / (nx * p->dx));
+      const double k = std::sqrt(kx * kx + ky * ky);
+      double g;
+      if (p->kernel == CGEF_GAUSSIAN) {
+        g = std::exp(-(k * k) * (p->scale * p->scale) / (4.0 * p->alpha));
+      } else {
+        const double x = k * (p->scale / 2.0);
+        g = x == 0.0 ? 1.0 : 2.0 * std::cyl_bessel_j(1.0, x) / x;
+      }
+      p->h_sp_T[static_cast<size_t>(r) * nk + q] = g;
+      T[static_cast<size_t>(r) * nkp + q] = g * norm;
+    }
+  }
+  p->rs_L = nx;
+  p->rs_nk = nk;
+  p->rs_nkp = nkp;
+  p->rs_nrad = static_cast<int>(radx.size());
+  for (size_t i = 0; i < radx.size(); ++i) p->rs_rad[i] = radx[i];
+  p->sp_nrad = static_cast<int>(rady.size());
+  for (size_t i = 0; i < rady.size(); ++i) p->sp_rad[i] = rady[i];
+  p->rs_on = false;
+  if (p->device < 0) return CGEF_OK;
+  const std::vector<double> twx = roots_table(nx), twy = roots_table(ny);
+  const std::vector<double> ptwx = pass_twiddles(radx, twx, nx, p->rs_poff);
+  const std::vector<double> ptwy = pass_twiddles(rady, twy, ny, p->sp_poff);
+  DeviceGuard dg(p->device);
+  auto put = [](double** dst, const std::vector<double>& v, const char* what) {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), std::max<size_t>(v.size(), 2) * sizeof(double));
+    if (e == cudaSuccess && !v.empty())
+      e = cudaMemcpy(*dst, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? CGEF_OK : cuda_fail(e, what);
+  };
+  int rc;
+  if ((rc = put(&p->d_rs_tw, twx, "spectral method: x roots")) != CGEF_OK) return rc;
+  if ((rc = put(&p->d_rs_ptw, ptwx, "spectral method: x pass twiddles")) != CGEF_OK) return rc;
+  if ((rc = put(&p->d_sp_ptw, ptwy, "spectral method: y pass twiddles")) != CGEF_OK) return rc;
+  if ((rc = put(&p->d_sp_T, T, "spectral method: transfer function")) != CGEF_OK) return rc;
   return CGEF_OK;
 }
 

@@ -55,8 +55,20 @@ enum { CGEF_TOPHAT = 0, CGEF_GAUSSIAN = 1 };
 /* Mask strategies (Filtering.jl:36-48 ZeroFill, :50-57 Deformable). */
 enum { CGEF_ZEROFILL = 0, CGEF_DEFORMABLE = 1 };
 /* Engines: AUTO dispatches as the reference does (Filtering.jl:636-749, 1121-1141, 1533-1561):
- * Gaussian on Cartesian -> SEPARABLE, top-hat -> PREFIXSUM, otherwise BANDED. */
-enum { CGEF_ENGINE_AUTO = 0, CGEF_ENGINE_BANDED = 1, CGEF_ENGINE_SEPARABLE = 2, CGEF_ENGINE_PREFIXSUM = 3 };
+ * Gaussian on Cartesian -> SEPARABLE, top-hat -> PREFIXSUM, otherwise BANDED.
+ * SPECTRAL is the reference's `method = Spectral()` (plan_filter, Filtering.jl:2944-2946, with the FFTW
+ * extension's plan, ext/CoarseGrainingEnergyFluxesFFTWExt.jl:121-206): a periodic convolution by the
+ * kernel's isotropic transfer function, so only on a Cartesian grid periodic along both axes
+ * (CGEF_EINVAL otherwise, Filtering.jl:2998-3004).  A field f filters to
+ *     IDFT2(Ghat(|k|, l) * DFT2(mask * f)),  Ghat = exp(-k^2 l^2 / (4 alpha)) (Gaussian),
+ *                                            2 J1(k l / 2) / (k l / 2) (top-hat, 1 at k = 0),
+ * with kx = 2 pi m / (nx dx), ky = 2 pi m' / (ny dy) on the rfft / fft frequency grids (Kernels.jl:394-406).
+ * ZeroFill stops there; Deformable multiplies by 1 / filter(mask) where |filter(mask)| >= 0.01 and by 0
+ * elsewhere (FFTWExt.jl:163-173), on a grid with masked cells.  Unlike the real-space engines the output
+ * is defined on every cell, masked ones too (FFTWExt.jl:184-206).  CGEF_EUNSUPPORTED unless nx is even,
+ * nx / 2 and ny have no prime factor above 5, and both are at most 4096. */
+enum { CGEF_ENGINE_AUTO = 0, CGEF_ENGINE_BANDED = 1, CGEF_ENGINE_SEPARABLE = 2, CGEF_ENGINE_PREFIXSUM = 3,
+       CGEF_ENGINE_SPECTRAL = 4 };
 /* Storage types of caller buffers. */
 enum { CGEF_F64 = 0, CGEF_F32 = 1 };
 
@@ -194,6 +206,11 @@ int32_t cgef_plan_set_row_spectral(cgef_plan* plan, int32_t enable);
  * along x (0 when unavailable).  Any pointer may be NULL. */
 int32_t cgef_plan_get_row_spectral(const cgef_plan* plan, int32_t* available, int32_t* enabled,
                                    int32_t* fft_length);
+
+/* A spectral-method plan's transfer function Ghat(|k|, l) on the rfft grid, the FFTW plan's `transfer`
+ * array (FFTWExt.jl:146): transfer[ky * (nx/2 + 1) + kx], ny * (nx/2 + 1) values, ky in fftfreq order.
+ * CGEF_EINVAL for a real-space plan. */
+int32_t cgef_plan_get_transfer(const cgef_plan* plan, double* transfer);
 
 /* Banded footprint of the plan in the reference's CSR form (FilterFootprint, Filtering.jl:327-336):
  * di/dj/w have nentries entries, ptr has nbands+1 (0-based offsets).  Any pointer may be NULL. */
