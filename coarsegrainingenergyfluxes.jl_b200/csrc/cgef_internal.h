@@ -451,6 +451,10 @@ int launch_convert(const double* src, int64_t src_stride, void* dst, int64_t dst
                    int nbatch, cudaStream_t st);
 
 // Energy of `fields` (ubar, vbar planes) per slice.
+// energy[s * energy_stride] = factor * sum_k partials[s][k][0] / sum_k partials[s][k][1] (0 when the
+// weight is 0), one block per slice, the partials summed in a fixed order: the energies' last step.
+int launch_energy_finish(const double* partials, int64_t nblk, int nbatch, double* energy, int64_t energy_stride,
+                         double factor, cudaStream_t st);
 int launch_energy(const cgef_plan* p, const double* ubar, const double* vbar, int64_t slice_stride,
                   const uint8_t* mask, int64_t mask_slice_stride, int nbatch, double* partials, double* energy,
                   int64_t energy_stride, cudaStream_t st);

@@ -752,35 +752,44 @@ struct RawFlux {
   static constexpr int NV = MODE == kModePiSphere ? 3 : 2;
 };
 
-template <int MODE, bool DEF>
-__device__ __forceinline__ bool raw_zero(const StrainK& a, const double* Fs, int64_t plane, int64_t pix, int j,
-                                         bool act, double& den) {
-  if (DEF)
-    den = Fs[(RawFlux<MODE, DEF>::NA - 1) * plane + pix];
-  else
-    den = a.den_zf_2d ? a.den_zf[pix] : a.den_zf[j];
-  return !act || !(den > kNormEps);
-}
+// The raw sums one finished value needs at a cell, with its activity and denominator, loaded together:
+// whether the cell is zero is decided after the loads, so a cell costs one round trip of memory latency
+// (every cell of the raw planes is written, masked ones too).
+template <int NQ>
+struct RawCell {
+  double F[NQ];
+  double den;
+  bool act;
+};
 
-// Finished local velocity at (j, i) of the slice whose raw sums start at Fs.
-template <int MODE, bool DEF>
-__device__ __forceinline__ void raw_velocity(const StrainK& a, const double* Fs, const uint8_t* mk, int j, int i,
-                                             double& u, double& v) {
-  using R = RawFlux<MODE, DEF>;
+template <int MODE, bool DEF, int NQ>
+__device__ __forceinline__ void raw_load(const StrainK& a, const double* Fs, const uint8_t* mk, int j, int i,
+                                         RawCell<NQ>& c) {
   const int64_t plane = static_cast<int64_t>(a.nx) * a.ny;
   const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
-  const bool act = mk == nullptr || mk[pix] != 0;
-  double den;
-  const bool zero = raw_zero<MODE, DEF>(a, Fs, plane, pix, j, act, den);
-  if (zero) {
+  c.act = mk == nullptr || mk[pix] != 0;
+  if (DEF)
+    c.den = Fs[(RawFlux<MODE, DEF>::NA - 1) * plane + pix];
+  else
+    c.den = a.den_zf_2d ? a.den_zf[pix] : a.den_zf[j];
+#pragma unroll
+  for (int m = 0; m < NQ; ++m) c.F[m] = Fs[m * plane + pix];
+}
+
+// Finished local velocity at (j, i) from its loaded raw sums.
+template <int MODE, bool DEF>
+__device__ __forceinline__ void raw_velocity(const StrainK& a, const RawCell<RawFlux<MODE, DEF>::NV>& c, int j, int i,
+                                             double& u, double& v) {
+  using R = RawFlux<MODE, DEF>;
+  if (!c.act || !(c.den > kNormEps)) {
     u = 0.0;
     v = 0.0;
     return;
   }
-  const double inv = 1.0 / den;
+  const double inv = 1.0 / c.den;
   double F[R::NV];
 #pragma unroll
-  for (int m = 0; m < R::NV; ++m) F[m] = Fs[m * plane + pix] * inv;
+  for (int m = 0; m < R::NV; ++m) F[m] = c.F[m] * inv;
   if constexpr (MODE == kModePiSphere) {
     local_velocity(F[0], F[1], F[2], a.sinlam[i], a.coslam[i], a.sinphi[j], a.cosphi[j], u, v);
   } else {
@@ -789,24 +798,19 @@ __device__ __forceinline__ void raw_velocity(const StrainK& a, const double* Fs,
   }
 }
 
-// Finished local velocity and stress at target (j, i).
+// Finished local velocity and stress at target (j, i) from its loaded raw sums.
 template <int MODE, bool DEF>
-__device__ __forceinline__ void raw_target(const StrainK& a, const double* Fs, const uint8_t* mk, int j, int i,
+__device__ __forceinline__ void raw_target(const StrainK& a, const RawCell<RawFlux<MODE, DEF>::NA0>& c, int j, int i,
                                            double& u, double& v, double& txx, double& txy, double& tyy) {
   using R = RawFlux<MODE, DEF>;
-  const int64_t plane = static_cast<int64_t>(a.nx) * a.ny;
-  const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
-  const bool act = mk == nullptr || mk[pix] != 0;
-  double den;
-  const bool zero = raw_zero<MODE, DEF>(a, Fs, plane, pix, j, act, den);
-  if (zero) {
+  if (!c.act || !(c.den > kNormEps)) {
     u = v = txx = txy = tyy = 0.0;
     return;
   }
-  const double inv = 1.0 / den;
+  const double inv = 1.0 / c.den;
   double F[R::NA0];
 #pragma unroll
-  for (int m = 0; m < R::NA0; ++m) F[m] = Fs[m * plane + pix] * inv;
+  for (int m = 0; m < R::NA0; ++m) F[m] = c.F[m] * inv;
   if constexpr (MODE == kModePiSphere) {
     const double sl = a.sinlam[i], cl = a.coslam[i], sp = a.sinphi[j], cp = a.cosphi[j];
     local_velocity(F[0], F[1], F[2], sl, cl, sp, cp, u, v);
@@ -884,10 +888,36 @@ __global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a
   const double* ub = RAW ? nullptr : a.ub + s * a.in_stride;
   const double* vb = RAW ? nullptr : a.vb + s * a.in_stride;
   const double* Fs = RAW ? a.raw + s * static_cast<int64_t>(RawFlux<MODE, DEF>::NA) * a.nx * a.ny : nullptr;
-  for (int c = threadIdx.y * kStrainBX + threadIdx.x; c < TW * TH; c += kStrainBX * kStrainBY) {
+  using R = RawFlux<MODE, DEF>;
+  const int i = x0 + threadIdx.x;
+  const int j = y0 + threadIdx.y;
+  const bool target = i < a.nx && j < a.ny;
+  const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+  // the target's own loads first, so that they overlap the tile's
+  RawCell<R::NA0> cen{};
+  double ctxx = 0.0, ctxy = 0.0, ctyy = 0.0;
+  if (target) {
+    if (RAW) {
+      raw_load<MODE, DEF, R::NA0>(a, Fs, mk, j, i, cen);
+    } else {
+      ctxx = a.txx ? a.txx[s * a.in_stride + pix] : 0.0;
+      ctxy = a.txy ? a.txy[s * a.in_stride + pix] : 0.0;
+      ctyy = a.tyy ? a.tyy[s * a.in_stride + pix] : 0.0;
+    }
+  }
+  // the tile: every thread's cells are loaded before any of them is finished
+  constexpr int kThreads = kStrainBX * kStrainBY, kPer = (TW * TH + kThreads - 1) / kThreads;
+  const int tid = threadIdx.y * kStrainBX + threadIdx.x;
+  RawCell<R::NV> rc[kPer];
+  double lu[kPer], lv[kPer];
+  int cj[kPer], ci[kPer];
+  bool cin[kPer];
+#pragma unroll
+  for (int it = 0; it < kPer; ++it) {
+    const int c = tid + it * kThreads;
     const int r = c / TW, q = c - r * TW;
     int jj = y0 - kStrainHalo + r, ii = x0 - kStrainHalo + q;
-    bool inside = true;
+    bool inside = c < TW * TH;
     if (jj < 0 || jj >= a.ny) {
       if (a.periodic_y)
         jj = wrap(jj, a.ny);
@@ -900,42 +930,51 @@ __global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a
       else
         inside = false;
     }
-    double u = 0.0, v = 0.0;
-    unsigned char am = 0;
+    cj[it] = jj;
+    ci[it] = ii;
+    cin[it] = inside;
+    rc[it].act = false;
+    lu[it] = lv[it] = 0.0;
     if (inside) {
-      am = mk == nullptr || mk[static_cast<int64_t>(jj) * a.nx + ii] != 0;
       if (RAW) {
-        raw_velocity<MODE, DEF>(a, Fs, mk, jj, ii, u, v);
+        raw_load<MODE, DEF, R::NV>(a, Fs, mk, jj, ii, rc[it]);
       } else {
         const int64_t k = static_cast<int64_t>(jj) * a.nx + ii;
-        u = ub[k];
-        v = vb[k];
+        rc[it].act = mk == nullptr || mk[k] != 0;
+        lu[it] = ub[k];
+        lv[it] = vb[k];
       }
     }
-    tu[r][q] = u;
-    tv[r][q] = v;
-    tm[r][q] = am;
+  }
+#pragma unroll
+  for (int it = 0; it < kPer; ++it) {
+    const int c = tid + it * kThreads;
+    if (c < TW * TH) {
+      const int r = c / TW, q = c - r * TW;
+      double u = lu[it], v = lv[it];
+      if (RAW && cin[it]) raw_velocity<MODE, DEF>(a, rc[it], cj[it], ci[it], u, v);
+      tu[r][q] = cin[it] ? u : 0.0;
+      tv[r][q] = cin[it] ? v : 0.0;
+      tm[r][q] = cin[it] && rc[it].act ? 1 : 0;
+    }
   }
   __syncthreads();
-  const int i = x0 + threadIdx.x;
-  const int j = y0 + threadIdx.y;
   const int cx0 = threadIdx.x + kStrainHalo, cy0 = threadIdx.y + kStrainHalo;
   double e_num = 0.0, e_area = 0.0, g_sum = 0.0, g_cnt = 0.0;
-  if (i < a.nx && j < a.ny) {
-    const int64_t pix = static_cast<int64_t>(j) * a.nx + i;
+  if (target) {
     const int64_t o = s * a.out_stride + pix;
     const bool act = mk == nullptr || mk[pix] != 0;
     double sxx = 0.0, sxy = 0.0, syy = 0.0, pi = 0.0;
     double g1 = 0.0, g2 = 0.0;  // du/dy and dv/dx + u t (the two halves of 2 S_en)
     double u0, v0, txx, txy, tyy;
     if (RAW) {
-      raw_target<MODE, DEF>(a, Fs, mk, j, i, u0, v0, txx, txy, tyy);
+      raw_target<MODE, DEF>(a, cen, j, i, u0, v0, txx, txy, tyy);
     } else {
       u0 = tu[cy0][cx0];
       v0 = tv[cy0][cx0];
-      txx = a.txx ? a.txx[s * a.in_stride + pix] : 0.0;
-      txy = a.txy ? a.txy[s * a.in_stride + pix] : 0.0;
-      tyy = a.tyy ? a.tyy[s * a.in_stride + pix] : 0.0;
+      txx = ctxx;
+      txy = ctxy;
+      tyy = ctyy;
     }
     if (act) {
       const StencilCase cx = tile_case(tm[cy0][cx0 - 1], tm[cy0][cx0 + 1], tm[cy0][cx0 - 2], tm[cy0][cx0 + 2]);
@@ -1065,15 +1104,29 @@ __global__ void energy_partial_kernel(EnergyK a) {
 }
 
 // One block per slice: sums the block partials in a fixed order; out = factor * sum / weight
-// (E = 1/2 sum / area with factor 1/2).
-__global__ void energy_finish_kernel(const double* partials, int64_t nblk, double* energy, int64_t estride,
-                                     double factor) {
-  __shared__ double sa[256], sb[256];
+// (E = 1/2 sum / area with factor 1/2).  Thread t adds partials t, t + 256, ... in that order; its loads
+// are issued eight at a time before any is added (a missing one adds an exact zero), so the sum costs a
+// few round trips of memory latency instead of one per partial.
+constexpr int kFinishThreads = 256, kFinishBatch = 8;
+__global__ void __launch_bounds__(kFinishThreads) energy_finish_kernel(const double* partials, int64_t nblk,
+                                                                       double* energy, int64_t estride, double factor) {
+  __shared__ double sa[kFinishThreads], sb[kFinishThreads];
   const int s = blockIdx.x;
   double a = 0.0, b = 0.0;
-  for (int64_t k = threadIdx.x; k < nblk; k += blockDim.x) {
-    a += partials[(s * nblk + k) * 2];
-    b += partials[(s * nblk + k) * 2 + 1];
+  const double* ps = partials + s * nblk * 2;
+  for (int64_t k0 = threadIdx.x; k0 < nblk; k0 += kFinishBatch * kFinishThreads) {
+    double va[kFinishBatch], vb[kFinishBatch];
+#pragma unroll
+    for (int u = 0; u < kFinishBatch; ++u) {
+      const int64_t k = k0 + static_cast<int64_t>(u) * kFinishThreads;
+      va[u] = k < nblk ? ps[k * 2] : 0.0;
+      vb[u] = k < nblk ? ps[k * 2 + 1] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kFinishBatch; ++u) {
+      a += va[u];
+      b += vb[u];
+    }
   }
   sa[threadIdx.x] = a;
   sb[threadIdx.x] = b;
@@ -1564,11 +1617,17 @@ int launch_strain(const cgef_plan* p, const StrainArgs& s, cudaStream_t st) {
   if (rc) return rc;
   const int64_t nblk = static_cast<int64_t>(grid.x) * grid.y;
   if (s.grad_mean) {
-    energy_finish_kernel<<<s.nbatch, 256, 0, st>>>(s.grad_partials, nblk, s.grad_mean, 1, 1.0);
+    energy_finish_kernel<<<s.nbatch, kFinishThreads, 0, st>>>(s.grad_partials, nblk, s.grad_mean, 1, 1.0);
     if ((rc = check_launch("energy_finish_kernel"))) return rc;
   }
   if (!s.energy) return CGEF_OK;
-  energy_finish_kernel<<<s.nbatch, 256, 0, st>>>(s.partials, nblk, s.energy, s.energy_stride, 0.5);
+  energy_finish_kernel<<<s.nbatch, kFinishThreads, 0, st>>>(s.partials, nblk, s.energy, s.energy_stride, 0.5);
+  return check_launch("energy_finish_kernel");
+}
+
+int launch_energy_finish(const double* partials, int64_t nblk, int nbatch, double* energy, int64_t energy_stride,
+                         double factor, cudaStream_t st) {
+  energy_finish_kernel<<<nbatch, kFinishThreads, 0, st>>>(partials, nblk, energy, energy_stride, factor);
   return check_launch("energy_finish_kernel");
 }
 
@@ -1582,7 +1641,7 @@ int launch_energy(const cgef_plan* p, const double* ubar, const double* vbar, in
   int rc = check_launch("energy_partial_kernel");
   if (rc) return rc;
   const int64_t nblk = static_cast<int64_t>(grid.x) * grid.y;
-  energy_finish_kernel<<<nbatch, 256, 0, st>>>(partials, nblk, energy, energy_stride, 0.5);
+  energy_finish_kernel<<<nbatch, kFinishThreads, 0, st>>>(partials, nblk, energy, energy_stride, 0.5);
   return check_launch("energy_finish_kernel");
 }
 

@@ -253,28 +253,6 @@ __global__ void __launch_bounds__(kWBX * kWBY) pi_w_kernel(PiWK a) {
   }
 }
 
-// E of each slice from its blocks' partials, in a fixed order: 1/2 sum / area.
-__global__ void w_energy_finish_kernel(const double* partials, int64_t nblk, double* energy) {
-  __shared__ double sa[256], sb[256];
-  const int s = blockIdx.x;
-  double x = 0.0, y = 0.0;
-  for (int64_t k = threadIdx.x; k < nblk; k += blockDim.x) {
-    x += partials[(s * nblk + k) * 2];
-    y += partials[(s * nblk + k) * 2 + 1];
-  }
-  sa[threadIdx.x] = x;
-  sb[threadIdx.x] = y;
-  __syncthreads();
-  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-    if (static_cast<int>(threadIdx.x) < h) {
-      sa[threadIdx.x] += sa[threadIdx.x + h];
-      sb[threadIdx.x] += sb[threadIdx.x + h];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) energy[s] = sb[0] > 0.0 ? 0.5 * sa[0] / sb[0] : 0.0;
-}
-
 int w_check(const char* what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, what);
@@ -348,8 +326,7 @@ int compute_pi_w_device(cgef_plan* p, int dtype, const void* u, const void* v, c
   pi_w_kernel<<<grid, dim3(kWBX, kWBY), 0, st>>>(a);
   if ((rc = w_check("pi_w_kernel"))) return rc;
   if (o->energy) {
-    w_energy_finish_kernel<<<nbatch, 256, 0, st>>>(a.partials, nblk, o->energy);
-    if ((rc = w_check("w_energy_finish_kernel"))) return rc;
+    if ((rc = launch_energy_finish(a.partials, nblk, nbatch, o->energy, 1, 0.5, st))) return rc;
   }
   return CGEF_OK;
 }

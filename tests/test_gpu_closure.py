@@ -193,6 +193,48 @@ def test_trained_closure_beats_the_untrained_one(torch):
     assert all(e1 < e0 for e0, e1 in zip(errs0, errs1)), (errs0, errs1)
 
 
+def test_trained_closure_beats_the_gradient_model_on_held_out_data(torch):
+    """What the network gains over the closure without it: trained on two snapshots, evaluated on a third
+    it never saw, its Pi must be closer to the exact flux than the classical nonlinear gradient model's,
+    tau_ij = l^2 / (2 alpha) A_ik A_jk (A the filtered velocity gradient, curvature terms included; for a
+    Gaussian of second moment l^2 / (2 alpha)), at every scale."""
+    g = S.sphere_grid(360, 180)
+    g = g.with_mask(S.land_mask(g, seed=21))
+    scales = [3e5, 6e5, 1.2e6]
+    plans = [cg.plan_filter(g, cg.GaussianKernel(4.0), ell) for ell in scales]
+    m = torch.from_numpy(g.mask.reshape(-1)).cuda()
+    xs, ts = [], []
+    for seed in (31, 32):
+        u, v = S.sphere_fields(g, seed=seed, lmax=120)
+        ud, vd = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+        for plan in plans:
+            f, t = CL.training_pairs(plan, ud, vd)
+            xs.append(f[0][:, m].T.contiguous())
+            ts.append(t[0][:, m].T.contiguous())
+    x, t = torch.cat(xs), torch.cat(ts)
+    perm = torch.randperm(x.shape[0], generator=torch.Generator().manual_seed(1)).cuda()
+    x, t = x[perm].contiguous(), t[perm].contiguous()
+    c = CL.Closure(seed=5)
+    c.train(x, t, batch=4096, steps=1200, lr=2e-3, weight_decay=1e-4)
+    c.train(x, t, batch=4096, steps=600, lr=4e-4, weight_decay=1e-4)
+    u, v = S.sphere_fields(g, seed=33, lmax=120)  # held out
+    ud, vd = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+    for plan in plans:
+        exact = _plain_pi(torch, plan, ud, vd).cpu().numpy()
+        err_net = rel_l2(c.pi(plan, ud, vd, judge_fraction=0.0)[0].cpu().numpy(), exact, g.mask)
+        # the gradient model in the closure's normalised units: x = l^2 A / n, y = tau l^2 / n^2, so
+        # y_model = (x0^2 + x1^2, x0 x2 + x1 x3, x2^2 + x3^2) / (2 alpha), and Pi is proportional, with one
+        # positive factor per slice, to -(x0 y0 + (x1 + x2) y1 + x3 y2)
+        f, tt = CL.training_pairs(plan, ud, vd)
+        xx, yy = f[0].double()[:, m], tt[0].double()[:, m]
+        ym = torch.stack([xx[0] ** 2 + xx[1] ** 2, xx[0] * xx[2] + xx[1] * xx[3], xx[2] ** 2 + xx[3] ** 2]) / 8.0
+        pi_of = lambda y: -(xx[0] * y[0] + (xx[1] + xx[2]) * y[1] + xx[3] * y[2])
+        ex = pi_of(yy)
+        err_gm = float(torch.linalg.norm(pi_of(ym) - ex) / torch.linalg.norm(ex))
+        assert err_net < err_gm, (plan.scale, err_net, err_gm)
+        assert err_net < 0.6, (plan.scale, err_net)
+
+
 @pytest.mark.parametrize("case", ["sphere-tophat", "sphere-deformable", "plane-tophat"])
 def test_closure_paths_of_every_engine_fall_back_exactly(torch, case):
     if case.startswith("sphere"):
