@@ -37,6 +37,7 @@ struct BandedK {
   const uint8_t* mask;
   int64_t mask_stride;
   int nx, ny, periodic_y;
+  int periodic_x;  // the zero-weight-skipping gather wraps (or zeroes) its own columns: it needs no halo
   const double* sinlam;
   const double* coslam;
   const double* sinphi;
@@ -274,6 +275,7 @@ inline BandedK make_banded_args(const cgef_plan* p, int mode, const double* plan
   a.nx = p->nx;
   a.ny = p->ny;
   a.periodic_y = p->periodic_y;
+  a.periodic_x = p->periodic_x;
   const bool sph = mode == kModePiSphere;
   a.sinlam = sph ? p->d_sinlam : nullptr;
   a.coslam = sph ? p->d_coslam : nullptr;

@@ -173,6 +173,11 @@ int pi_gather(cgef_plan* p, const double* planes, int pitch, int halo, int np, i
   return launch_prefix(p, mode, 0, planes, pitch, np, nbatch, mask, mstride, static_cast<double*>(pre), go, st);
 }
 
+// Column halo the flux's staged planes need for plan q: the direct gather reads up to H columns past either
+// end of a row, while the row-spectral evaluation reads the row alone (its non-finite re-sum wraps or zeroes
+// its own columns), so it is staged without one -- half the stage pass's writes on the 0.25-degree sphere.
+int stage_halo(const cgef_plan* q) { return q->engine == CGEF_ENGINE_BANDED && q->rs_on ? 0 : q->H; }
+
 int stage_pi(cgef_plan* p, int dtype, const void* u, const void* v, int nbatch, const uint8_t* mask, int64_t mstride,
              int halo, double** planes_out, int* pitch_out, int* np_out, cudaStream_t st) {
   const bool def = p->strategy == CGEF_DEFORMABLE;
@@ -210,12 +215,18 @@ int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int
   const int64_t mstride = slice_masks ? N : 0;
   double* planes = nullptr;
   int pitch = 0, np = 0;
-  if ((rc = stage_pi(p, dtype, u, v, nbatch, mask, mstride, p->H, &planes, &pitch, &np, st))) return rc;
+  const int halo = stage_halo(p);
+  if ((rc = stage_pi(p, dtype, u, v, nbatch, mask, mstride, halo, &planes, &pitch, &np, st))) return rc;
   void* gather = nullptr;
   if ((rc = ensure_ws(p, kSlotGather, sizeof(double) * 5 * N * nbatch, &gather))) return rc;
   double* g = static_cast<double*>(gather);
   const double* raw = nullptr;
-  if ((rc = pi_gather(p, planes, pitch, p->H, np, nbatch, mask, mstride, g, st, RsShare{}, &raw))) return rc;
+  // the engine reads the planes with the halo they were staged with
+  const int saveH = p->H;
+  p->H = halo;
+  rc = pi_gather(p, planes, pitch, halo, np, nbatch, mask, mstride, g, st, RsShare{}, &raw);
+  p->H = saveH;
+  if (rc) return rc;
   StrainArgs sa{};
   sa.raw = raw;
   sa.ubar = g;
@@ -335,7 +346,7 @@ int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u,
   cgef_plan* p0 = plans[0];
   if ((rc = check_plan(p0)) || (rc = check_dtype(dtype))) return rc;
   if (nbatch64 < 1 || nbatch64 > 65535) return fail(CGEF_EINVAL, "nbatch must be in 1..65535");
-  int halo = 1;
+  int halo = 0;
   for (int s = 0; s < nscales; ++s) {
     const cgef_plan* q = plans[s];
     if ((rc = check_plan(q))) return rc;
@@ -343,7 +354,7 @@ int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u,
         q->strategy != p0->strategy || q->periodic_x != p0->periodic_x || q->periodic_y != p0->periodic_y ||
         q->dx != p0->dx || q->dy != p0->dy || q->x0 != p0->x0 || q->y0 != p0->y0 || q->h_mask != p0->h_mask)
       return fail(CGEF_EINVAL, "all plans of a sweep must share one grid, engine and mask strategy");
-    halo = std::max(halo, q->H);
+    halo = std::max(halo, stage_halo(q));
   }
   const int nbatch = static_cast<int>(nbatch64);
   const int64_t N = static_cast<int64_t>(p0->nx) * p0->ny;

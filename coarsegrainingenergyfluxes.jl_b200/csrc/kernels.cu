@@ -48,6 +48,13 @@ __device__ __forceinline__ int wrap(int a, int n) {
   return r < 0 ? r + n : r;
 }
 
+// Column c of a source row as the halo would hold it: itself inside the row, wrapped on a periodic axis,
+// -1 (a zero value) off a bounded one.
+__device__ __forceinline__ int source_col(int c, int nx, int periodic) {
+  if (c >= 0 && c < nx) return c;
+  return periodic ? wrap(c, nx) : -1;
+}
+
 template <typename T>
 __device__ __forceinline__ double ld(const void* p, int64_t k) {
   return static_cast<double>(static_cast<const T*>(p)[k]);
@@ -221,6 +228,7 @@ __device__ __forceinline__ void banded_unit(const BandedK& a, int64_t gid, doubl
       continue;
     }
     const double* src = base + static_cast<int64_t>(jj) * a.pitch;
+    const double* rowp = src - col;  // column 0 of the source row (the SAFE gather indexes it itself)
     if constexpr (PAIR) {
       // offsets d = 0 .. A, the pair (c + d, c - d) per step
       for (int d0 = 0; d0 <= A; d0 += 32) {
@@ -243,10 +251,20 @@ __device__ __forceinline__ void banded_unit(const BandedK& a, int64_t gid, doubl
 #pragma unroll kBandedUnroll
         for (int kk = 0; kk < cn; ++kk) {
           double v1[C::NP], v2[C::NP];
+          if constexpr (SAFE) {
+            const int c1 = source_col(col + d0 + kk, a.nx, a.periodic_x);
+            const int c2 = source_col(col - d0 - kk, a.nx, a.periodic_x);
 #pragma unroll
-          for (int pl = 0; pl < C::NP; ++pl) {
-            v1[pl] = __ldg(sp + pl * a.plane_stride + kk);
-            v2[pl] = __ldg(sm + pl * a.plane_stride - kk);
+            for (int pl = 0; pl < C::NP; ++pl) {
+              v1[pl] = c1 >= 0 ? __ldg(rowp + pl * a.plane_stride + c1) : 0.0;
+              v2[pl] = c2 >= 0 ? __ldg(rowp + pl * a.plane_stride + c2) : 0.0;
+            }
+          } else {
+#pragma unroll
+            for (int pl = 0; pl < C::NP; ++pl) {
+              v1[pl] = __ldg(sp + pl * a.plane_stride + kk);
+              v2[pl] = __ldg(sm + pl * a.plane_stride - kk);
+            }
           }
           double q[C::NA];
           expand_pair<MODE, NF, DEF>(v1, v2, q);
@@ -277,8 +295,14 @@ __device__ __forceinline__ void banded_unit(const BandedK& a, int64_t gid, doubl
 #pragma unroll kBandedUnroll
         for (int kk = 0; kk < cn; ++kk) {
           double v[C::NP];
+          if constexpr (SAFE) {
+            const int c = source_col(col + c0 + kk, a.nx, a.periodic_x);
 #pragma unroll
-          for (int pl = 0; pl < C::NP; ++pl) v[pl] = __ldg(s + pl * a.plane_stride + kk);
+            for (int pl = 0; pl < C::NP; ++pl) v[pl] = c >= 0 ? __ldg(rowp + pl * a.plane_stride + c) : 0.0;
+          } else {
+#pragma unroll
+            for (int pl = 0; pl < C::NP; ++pl) v[pl] = __ldg(s + pl * a.plane_stride + kk);
+          }
           double q[C::NA];
           expand<MODE, NF, DEF>(v, q);
 #pragma unroll

@@ -112,3 +112,37 @@ def test_filter_with_an_infinite_active_value_matches_direct(c1):
     b = cg.filter_apply(None, f, direct)
     assert np.array_equal(a, b, equal_nan=True)
     assert np.array_equal(~np.isfinite(a), _reach(spec, g, j0, i0) & g.mask)
+
+
+@pytest.mark.parametrize("periodic", [(True, True), (False, False)], ids=["periodic", "bounded"])
+def test_nonfinite_next_to_the_row_ends_matches_direct(periodic):
+    """The row-spectral planes are staged without a column halo, so the direct re-sum of a flagged slice
+    wraps its columns (periodic x) or reads zeros past the row's ends (bounded x) itself: a NaN beside the
+    seam or the edge must still give the direct evaluation's outputs bit for bit."""
+    n = 120
+    m = np.ones((n, n), bool)
+    m[40:60, 50:80] = False
+    g = cg.StructuredGrid(cg.CartesianGeometry(), cg.axis(0, 1000.0, n), cg.axis(0, 1000.0, n), m, periodic)
+    rng = np.random.default_rng(2)
+    u, v = rng.standard_normal(g.shape), rng.standard_normal(g.shape)
+    u[30, 1] = np.nan
+    v[90, n - 2] = np.inf
+    k = cg.GaussianKernel(4.0)
+    spec = cg.plan_filter(g, k, 9000.0, engine="banded")
+    assert spec.row_spectral[0], "the banded Cartesian plan must offer the row-spectral evaluation"
+    spec.set_row_spectral(True)
+    direct = cg.plan_filter(g, k, 9000.0, engine="banded")
+    direct.set_row_spectral(False)
+    for name in ("ZeroFill", "Deformable"):
+        strat = cg.ZeroFill() if name == "ZeroFill" else cg.Deformable()
+        ps = cg.plan_filter(g, k, 9000.0, mask_strategy=strat, engine="banded")
+        pd = cg.plan_filter(g, k, 9000.0, mask_strategy=strat, engine="banded")
+        pd.set_row_spectral(False)
+        a = cg.compute_Pi_fields(u, v, g, k, 9000.0, filter_plan=ps, mask_strategy=strat)
+        b = cg.compute_Pi_fields(u, v, g, k, 9000.0, filter_plan=pd, mask_strategy=strat)
+        for key in OUTS:
+            assert np.array_equal(a[key], b[key], equal_nan=True), (name, key)
+    # a sweep of both evaluations against the direct one
+    res = cg.coarse_grain(u, v, g, scales=[9000.0], kernel=k, spectrum=cg.NoSpectrum(), filter_plans=[spec])
+    ref = cg.coarse_grain(u, v, g, scales=[9000.0], kernel=k, spectrum=cg.NoSpectrum(), filter_plans=[direct])
+    assert np.array_equal(res.Pi, ref.Pi, equal_nan=True)
