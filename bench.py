@@ -380,6 +380,51 @@ def device_steps_ms(run, steps, stream, flush) -> float:
     return float(sum(a.elapsed_time(b) for a, b in ev))
 
 
+def host_link(h2d_bytes: int, d2h_bytes: int, reps: int = 20) -> dict:
+    """The host link's own copy rate for one step's transfers: pinned host -> device and device -> pinned
+    host copies of the step's byte counts, each alone and both at once on two streams (the pipelined
+    steady state), timed with CUDA events on the copying streams after warm-up; the fastest of five
+    turns of each."""
+    import torch
+    hin = torch.empty(h2d_bytes, dtype=torch.uint8).pin_memory()
+    din = torch.empty(h2d_bytes, dtype=torch.uint8, device="cuda")
+    hout = torch.empty(d2h_bytes, dtype=torch.uint8).pin_memory()
+    dout = torch.empty(d2h_bytes, dtype=torch.uint8, device="cuda")
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(do_in, do_out):
+        for _ in range(5):
+            with torch.cuda.stream(s_in):
+                din.copy_(hin, non_blocking=True)
+            with torch.cuda.stream(s_out):
+                hout.copy_(dout, non_blocking=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s_in)
+        s_out.wait_event(a)
+        for _ in range(reps):
+            if do_in:
+                with torch.cuda.stream(s_in):
+                    din.copy_(hin, non_blocking=True)
+            if do_out:
+                with torch.cuda.stream(s_out):
+                    hout.copy_(dout, non_blocking=True)
+        s_in.wait_stream(s_out)
+        b.record(s_in)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    # the three measurements taken in turn five times, the fastest of each kept (the first copies
+    # from freshly pinned pages, and a shared host's other traffic, are slower)
+    t_in = t_out = t_both = float("inf")
+    for _ in range(5):
+        t_in = min(t_in, timed(True, False))
+        t_out = min(t_out, timed(False, True))
+        t_both = min(t_both, timed(True, True))
+    return {"h2d_GBps": h2d_bytes / t_in / 1e6, "d2h_GBps": d2h_bytes / t_out / 1e6,
+            "h2d_ms": t_in, "d2h_ms": t_out, "both_ms": t_both}
+
+
 def mlp_flops_per_point() -> float:
     """Multiply-adds x 2 of the closure MLP per point, unpadded (5-64-64-64-3)."""
     return 2.0 * (5 * 64 + 64 * 64 + 64 * 64 + 64 * 3)
@@ -908,6 +953,16 @@ def measure_sweep(args, name, rank, world, local, dist, *, snapshots=1, scale_km
                      "sweeps (the per-level masks, if any, are copied once at create); no L2 flush: "
                      "each step's inputs arrive by H2D",
            "synchronous": e2e_sync}
+    # what the host link allows: the pipelined steady state can be no faster than the slower of the
+    # step's copies (both directions at once) and its device time
+    link = host_link(e2e["h2d_bytes_per_step"], e2e["d2h_bytes_per_step"])
+    bound_ms = max(link["both_ms"], graph_ms / steps)
+    got_ms = el / n_e2e * 1e3
+    e2e["link_bound"] = dict(link, bound_ms_per_step=bound_ms, achieved_ms_per_step=got_ms,
+                             frac=bound_ms / got_ms,
+                             what="one step's H2D and D2H bytes copied alone and both at once (pinned, CUDA "
+                                  "events); bound = max(both at once, device ms per step); frac = bound / "
+                                  "the streamed e2e's ms per step")
 
     cpu = None
     accuracy = None

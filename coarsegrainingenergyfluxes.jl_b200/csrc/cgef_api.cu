@@ -253,7 +253,7 @@ int compute_pi_device(cgef_plan* p, int dtype, const void* u, const void* v, int
   sa.out_slice_stride = N;
   if (o->energy) {
     void* part = nullptr;
-    const int64_t nblk = static_cast<int64_t>((p->nx + 31) / 32) * ((p->ny + 7) / 8);
+    const int64_t nblk = strain_tiles(p);
     if ((rc = ensure_ws(p, kSlotPartials, sizeof(double) * 2 * nblk * nbatch, &part))) return rc;
     sa.partials = static_cast<double*>(part);
     sa.energy = o->energy;
@@ -367,7 +367,7 @@ int sweep_device(cgef_plan* const* plans, int nscales, int dtype, const void* u,
   if ((rc = ensure_ws(p0, kSlotGather, sizeof(double) * 5 * N * nbatch, &gather))) return rc;
   double* g = static_cast<double*>(gather);
   void* part = nullptr;
-  const int64_t nblk = static_cast<int64_t>((p0->nx + 31) / 32) * ((p0->ny + 7) / 8);
+  const int64_t nblk = strain_tiles(p0);
   if ((rc = ensure_ws(p0, kSlotPartials, sizeof(double) * 2 * nblk * nbatch, &part))) return rc;
   // The row-spectral plans of one FFT length share the source spectra: they depend on the staged fields,
   // not on the scale, so the first such plan transforms them and the others start from its spectra.
@@ -1130,7 +1130,7 @@ int32_t cgef_cumulative_energy(cgef_plan* const* plans, int32_t nscales, int32_t
   double* vf = uf + N;
   double* dE = vf + N;
   void* part = nullptr;
-  const int64_t nblk = static_cast<int64_t>((p->nx + 31) / 32) * ((p->ny + 7) / 8);
+  const int64_t nblk = strain_tiles(p);
   if ((rc = ensure_ws(p, kSlotPartials, sizeof(double) * 2 * nblk, &part))) return rc;
   for (int s = 0; s < nscales; ++s) {
     cgef_plan* q = plans[s];

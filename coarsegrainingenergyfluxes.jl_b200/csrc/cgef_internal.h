@@ -453,6 +453,9 @@ int launch_convert(const double* src, int64_t src_stride, void* dst, int64_t dst
 // Energy of `fields` (ubar, vbar planes) per slice.
 // energy[s * energy_stride] = factor * sum_k partials[s][k][0] / sum_k partials[s][k][1] (0 when the
 // weight is 0), one block per slice, the partials summed in a fixed order: the energies' last step.
+// Target tiles of the strain pass (and of the energy partials) over one slice: the partials buffers
+// hold two doubles per tile and slice.
+int64_t strain_tiles(const cgef_plan* p);
 int launch_energy_finish(const double* partials, int64_t nblk, int nbatch, double* energy, int64_t energy_stride,
                          double factor, cudaStream_t st);
 int launch_energy(const cgef_plan* p, const double* ubar, const double* vbar, int64_t slice_stride,

@@ -862,7 +862,7 @@ int gradients(cgef_plan* p, cgef_closure* c, const double* ub, const double* vb,
   const int64_t N = static_cast<int64_t>(p->nx) * p->ny;
   void* gp = nullptr;
   if ((rc = cl_ws(c, 1, sizeof(float) * 4 * N * nbatch, &gp))) return rc;
-  const int64_t nblk = static_cast<int64_t>((p->nx + 31) / 32) * ((p->ny + 7) / 8);
+  const int64_t nblk = strain_tiles(p);
   void* gm = nullptr;
   if ((rc = cl_ws(c, 2, sizeof(double) * (nbatch + 2 * nblk * nbatch), &gm))) return rc;
   StrainArgs sa{};

@@ -765,7 +765,10 @@ struct StrainK {
   const double* cosphi;
 };
 
-constexpr int kStrainBX = 32, kStrainBY = 8;
+#ifndef CGEF_STRAIN_BY
+#define CGEF_STRAIN_BY 8
+#endif
+constexpr int kStrainBX = 32, kStrainBY = CGEF_STRAIN_BY;
 
 // Finishing of the raw sums: the normalisation of finish_target (inactive targets and denominators
 // at or below kNormEps give 0), then the local-frame velocity of write_outputs.
@@ -800,17 +803,19 @@ __device__ __forceinline__ void raw_load(const StrainK& a, const double* Fs, con
   for (int m = 0; m < NQ; ++m) c.F[m] = Fs[m * plane + pix];
 }
 
-// Finished local velocity at (j, i) from its loaded raw sums.
+// Finished local velocity at (j, i) from its loaded raw sums, and the reciprocal of its denominator
+// (0 where the cell finishes to zero).
 template <int MODE, bool DEF>
 __device__ __forceinline__ void raw_velocity(const StrainK& a, const RawCell<RawFlux<MODE, DEF>::NV>& c, int j, int i,
-                                             double& u, double& v) {
+                                             double& u, double& v, double& inv) {
   using R = RawFlux<MODE, DEF>;
   if (!c.act || !(c.den > kNormEps)) {
     u = 0.0;
     v = 0.0;
+    inv = 0.0;
     return;
   }
-  const double inv = 1.0 / c.den;
+  inv = 1.0 / c.den;
   double F[R::NV];
 #pragma unroll
   for (int m = 0; m < R::NV; ++m) F[m] = c.F[m] * inv;
@@ -822,27 +827,23 @@ __device__ __forceinline__ void raw_velocity(const StrainK& a, const RawCell<Raw
   }
 }
 
-// Finished local velocity and stress at target (j, i) from its loaded raw sums.
+// Finished local stress at target (j, i) from its loaded raw sums and the reciprocal of its denominator
+// that the tile's finishing computed (the same division of the same value); its velocity is the tile's.
 template <int MODE, bool DEF>
 __device__ __forceinline__ void raw_target(const StrainK& a, const RawCell<RawFlux<MODE, DEF>::NA0>& c, int j, int i,
-                                           double& u, double& v, double& txx, double& txy, double& tyy) {
+                                           double inv, double& txx, double& txy, double& tyy) {
   using R = RawFlux<MODE, DEF>;
   if (!c.act || !(c.den > kNormEps)) {
-    u = v = txx = txy = tyy = 0.0;
+    txx = txy = tyy = 0.0;
     return;
   }
-  const double inv = 1.0 / c.den;
   double F[R::NA0];
 #pragma unroll
   for (int m = 0; m < R::NA0; ++m) F[m] = c.F[m] * inv;
   if constexpr (MODE == kModePiSphere) {
-    const double sl = a.sinlam[i], cl = a.coslam[i], sp = a.sinphi[j], cp = a.cosphi[j];
-    local_velocity(F[0], F[1], F[2], sl, cl, sp, cp, u, v);
-    local_tau_sphere(F, sl, cl, sp, cp, txx, txy, tyy);
+    local_tau_sphere(F, a.sinlam[i], a.coslam[i], a.sinphi[j], a.cosphi[j], txx, txy, tyy);
   } else {
     // Diagnostics.jl:525-527
-    u = F[0];
-    v = F[1];
     txx = F[2] - F[0] * F[0];
     txy = F[3] - F[0] * F[1];
     tyy = F[4] - F[1] * F[1];
@@ -906,6 +907,7 @@ __global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a
   __shared__ double tu[TH][TW];
   __shared__ double tv[TH][TW];
   __shared__ unsigned char tm[TH][TW];  // activity (0 off a bounded axis)
+  __shared__ double ti[RAW ? TH : 1][RAW ? TW : 1];  // reciprocal denominators of the finished raw sums
   const int x0 = blockIdx.x * kStrainBX, y0 = blockIdx.y * kStrainBY;
   const int s = blockIdx.z;
   const uint8_t* mk = a.mask ? a.mask + s * a.mask_stride : nullptr;
@@ -975,8 +977,9 @@ __global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a
     const int c = tid + it * kThreads;
     if (c < TW * TH) {
       const int r = c / TW, q = c - r * TW;
-      double u = lu[it], v = lv[it];
-      if (RAW && cin[it]) raw_velocity<MODE, DEF>(a, rc[it], cj[it], ci[it], u, v);
+      double u = lu[it], v = lv[it], inv = 0.0;
+      if (RAW && cin[it]) raw_velocity<MODE, DEF>(a, rc[it], cj[it], ci[it], u, v, inv);
+      if (RAW) ti[r][q] = inv;
       tu[r][q] = cin[it] ? u : 0.0;
       tv[r][q] = cin[it] ? v : 0.0;
       tm[r][q] = cin[it] && rc[it].act ? 1 : 0;
@@ -990,12 +993,11 @@ __global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a
     const bool act = mk == nullptr || mk[pix] != 0;
     double sxx = 0.0, sxy = 0.0, syy = 0.0, pi = 0.0;
     double g1 = 0.0, g2 = 0.0;  // du/dy and dv/dx + u t (the two halves of 2 S_en)
-    double u0, v0, txx, txy, tyy;
+    const double u0 = tu[cy0][cx0], v0 = tv[cy0][cx0];
+    double txx, txy, tyy;
     if (RAW) {
-      raw_target<MODE, DEF>(a, cen, j, i, u0, v0, txx, txy, tyy);
+      raw_target<MODE, DEF>(a, cen, j, i, ti[cy0][cx0], txx, txy, tyy);
     } else {
-      u0 = tu[cy0][cx0];
-      v0 = tv[cy0][cx0];
       txx = ctxx;
       txy = ctxy;
       tyy = ctyy;
@@ -1647,6 +1649,10 @@ int launch_strain(const cgef_plan* p, const StrainArgs& s, cudaStream_t st) {
   if (!s.energy) return CGEF_OK;
   energy_finish_kernel<<<s.nbatch, kFinishThreads, 0, st>>>(s.partials, nblk, s.energy, s.energy_stride, 0.5);
   return check_launch("energy_finish_kernel");
+}
+
+int64_t strain_tiles(const cgef_plan* p) {
+  return static_cast<int64_t>((p->nx + kStrainBX - 1) / kStrainBX) * ((p->ny + kStrainBY - 1) / kStrainBY);
 }
 
 int launch_energy_finish(const double* partials, int64_t nblk, int nbatch, double* energy, int64_t energy_stride,

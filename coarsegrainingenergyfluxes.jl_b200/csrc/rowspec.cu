@@ -214,8 +214,9 @@ __device__ __forceinline__ void dft(double2 (&v)[R]) {
 // (Ns R)), and writes b[(j / Ns) Ns R + j mod Ns + r Ns].  j / Ns is __umulhi(j, ns_magic) with
 // ns_magic = ceil(2^32 / Ns) (Ns > 1), exact for j, Ns < 2^16.  The butterflies of all the sequences
 // are one range over the block's threads (t = sq * M/R + j), so a block of nseq * M/R threads or more
-// does a pass in one round.
-template <int R>
+// does a pass in one round.  TW false: the first pass (Ns = 1), whose twiddles are all 1, applies none
+// (2-4% faster FFT kernels at L = 1440).
+template <int R, bool TW>
 __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int M, int Ns, unsigned ns_magic,
                                               int nseq, const double2* ptw) {
   const int nb = M / R;
@@ -230,8 +231,10 @@ __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int 
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = as[j + r * nb];
+    if constexpr (TW) {
 #pragma unroll
-    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(ptw + (r - 1) * Ns + jm));
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(ptw + (r - 1) * Ns + jm));
+    }
     dft<R>(v);
     double2* bs = b + sq * M + jq * Ns * R + jm;
 #pragma unroll
@@ -287,15 +290,28 @@ __device__ __forceinline__ double2* fft_block(double2* a, double2* b, int nseq, 
     const int R = f.rad[p];
     const unsigned mg = f.magic[p];
     const double2* tp = f.ptw + f.poff[p];
-    switch (R) {
-      case 2: stockham_pass<2>(a, b, f.M, Ns, mg, nseq, tp); break;
-      case 3: stockham_pass<3>(a, b, f.M, Ns, mg, nseq, tp); break;
-      case 4: stockham_pass<4>(a, b, f.M, Ns, mg, nseq, tp); break;
-      case 5: stockham_pass<5>(a, b, f.M, Ns, mg, nseq, tp); break;
-      case 8: stockham_pass<8>(a, b, f.M, Ns, mg, nseq, tp); break;
-      case 9: stockham_pass<9>(a, b, f.M, Ns, mg, nseq, tp); break;
-      case 10: stockham_pass<10>(a, b, f.M, Ns, mg, nseq, tp); break;
-      default: stockham_pass<16>(a, b, f.M, Ns, mg, nseq, tp); break;
+    if (p == 0) {  // the first pass's twiddles are all 1: none are applied
+      switch (R) {
+        case 2: stockham_pass<2, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 3: stockham_pass<3, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 4: stockham_pass<4, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 5: stockham_pass<5, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 8: stockham_pass<8, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 9: stockham_pass<9, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 10: stockham_pass<10, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+        default: stockham_pass<16, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+      }
+    } else {
+      switch (R) {
+        case 2: stockham_pass<2, true>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 3: stockham_pass<3, true>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 4: stockham_pass<4, true>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 5: stockham_pass<5, true>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 8: stockham_pass<8, true>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 9: stockham_pass<9, true>(a, b, f.M, Ns, mg, nseq, tp); break;
+        case 10: stockham_pass<10, true>(a, b, f.M, Ns, mg, nseq, tp); break;
+        default: stockham_pass<16, true>(a, b, f.M, Ns, mg, nseq, tp); break;
+      }
     }
     __syncthreads();
     double2* t = a;
@@ -400,11 +416,21 @@ __device__ __forceinline__ void cp_async_wait() {
 // S_j = sum_dj K_{j,dj} Q_{j+dj} per bin.  A block owns 32 bins x TJ target rows x every quantity and
 // walks the in-domain source rows its band touches; per source row it stages that row's spectra (all
 // quantities) and the TJ kernel-spectrum slices that apply to it in shared memory through a
-// kAccStages-deep cp.async pipeline, and each warp adds them into a register tile of RW target rows x
-// every quantity, so one staged kernel value serves NA quantities and one staged source value RW rows
-// (NA x RW complex multiply-adds per NA + RW shared-memory reads).  Rows off a bounded y axis are
-// skipped (the direct sum skips them); on a periodic y axis they wrap.
-constexpr int kAccStages = 4;
+// kAccStages-deep cp.async pipeline of kAccRps rows a stage (one block barrier per stage), and each
+// warp adds them into a register tile of RW target rows x every quantity, so one staged kernel value
+// serves NA quantities and one staged source value RW rows (NA x RW complex multiply-adds per NA + RW
+// shared-memory reads).  Rows off a bounded y axis are skipped (the direct sum skips them); on a
+// periodic y axis they wrap.  Three rows a stage (104 KB of shared memory a block, two blocks an SM)
+// made the 0.25 degree flux step 4% faster than one row a stage; six one-row stages or two-row
+// stages gained less.
+#ifndef CGEF_ACC_STAGES
+#define CGEF_ACC_STAGES 4
+#endif
+#ifndef CGEF_ACC_RPS
+#define CGEF_ACC_RPS 3
+#endif
+constexpr int kAccStages = CGEF_ACC_STAGES;
+constexpr int kAccRps = CGEF_ACC_RPS;  // source rows a pipeline stage holds (one block barrier each)
 // target rows of an accumulation block: 16 at every band height (32-row blocks, one per SM, were 15%
 // slower at 2000 km: every row's barrier then stalls the whole SM)
 constexpr int kAccRows = 16;
@@ -453,8 +479,7 @@ __global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1) rs_accumulate_
     k_base[i] = (static_cast<int64_t>(k.band_stride ? k_j[i] : 0) * W + k.D - k_j[i]) * nkp + q0 + 2 * (c & 15);
   }
 
-  auto issue = [&](int step, int buf) {
-    unsigned char* b = rs_acc_smem + buf * sbytes;
+  auto issue_row = [&](int step, unsigned char* b) {
     const int jraw = j0 - k.D + step;
     int jr = jraw;
     if (jr < 0 || jr >= k.ny) {  // only reached on a periodic y axis
@@ -477,6 +502,11 @@ __global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1) rs_accumulate_
       }
     }
   };
+  auto issue = [&](int step, int buf) {
+#pragma unroll
+    for (int r = 0; r < kAccRps; ++r)
+      if (step + r < st1) issue_row(step + r, rs_acc_smem + (buf * kAccRps + r) * sbytes);
+  };
 
   double2 acc[RW][NA];
 #pragma unroll
@@ -485,28 +515,33 @@ __global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1) rs_accumulate_
     for (int m = 0; m < NA; ++m) acc[t][m] = make_double2(0.0, 0.0);
 #pragma unroll
   for (int i = 0; i < kAccStages - 1; ++i) {
-    if (st0 + i < st1) issue(st0 + i, i);
+    if (st0 + i * kAccRps < st1) issue(st0 + i * kAccRps, i);
     cp_async_commit();
   }
-  for (int st = st0; st < st1; ++st) {
+  for (int sg = st0; sg < st1; sg += kAccRps) {
     cp_async_wait<kAccStages - 2>();
     __syncthreads();
-    const int nxt = st + kAccStages - 1;
-    if (nxt < st1) issue(nxt, (nxt - st0) % kAccStages);
+    const int nxt = sg + (kAccStages - 1) * kAccRps;
+    if (nxt < st1) issue(nxt, ((nxt - st0) / kAccRps) % kAccStages);
     cp_async_commit();
-    const unsigned char* b = rs_acc_smem + ((st - st0) % kAccStages) * sbytes;
-    const double2* qb = reinterpret_cast<const double2*>(b) + lane;
-    const double* kb = reinterpret_cast<const double*>(b + qbytes) + rg * RW * 32 + lane;
-    double kv[RW];
+    const unsigned char* sb = rs_acc_smem + (((sg - st0) / kAccRps) % kAccStages) * kAccRps * sbytes;
 #pragma unroll
-    for (int t = 0; t < RW; ++t) kv[t] = kb[t * 32];
+    for (int r = 0; r < kAccRps; ++r) {
+      if (sg + r >= st1) break;
+      const unsigned char* b = sb + r * sbytes;
+      const double2* qb = reinterpret_cast<const double2*>(b) + lane;
+      const double* kb = reinterpret_cast<const double*>(b + qbytes) + rg * RW * 32 + lane;
+      double kv[RW];
 #pragma unroll
-    for (int m = 0; m < NA; ++m) {
-      const double2 a = qb[m * 32];
+      for (int t = 0; t < RW; ++t) kv[t] = kb[t * 32];
 #pragma unroll
-      for (int t = 0; t < RW; ++t) {
-        acc[t][m].x = fma(kv[t], a.x, acc[t][m].x);
-        acc[t][m].y = fma(kv[t], a.y, acc[t][m].y);
+      for (int m = 0; m < NA; ++m) {
+        const double2 a = qb[m * 32];
+#pragma unroll
+        for (int t = 0; t < RW; ++t) {
+          acc[t][m].x = fma(kv[t], a.x, acc[t][m].x);
+          acc[t][m].y = fma(kv[t], a.y, acc[t][m].y);
+        }
       }
     }
   }
@@ -733,7 +768,7 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
   }
   if (rc == CGEF_OK) {
     constexpr int RW = AccTile<NA>::RW;
-    const int acc_smem = kAccStages * (NA * 32 * 16 + kAccRows * 32 * 8);
+    const int acc_smem = kAccStages * kAccRps * (NA * 32 * 16 + kAccRows * 32 * 8);
     const dim3 g(p->rs_nkp / 32, (p->ny + kAccRows - 1) / kAccRows, a.nslices);
     if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<kAccRows, NA>))) == CGEF_OK)
       rs_accumulate_kernel<kAccRows, NA><<<g, 32 * (kAccRows / RW), acc_smem, st>>>(k);
