@@ -112,17 +112,24 @@ __global__ void stage_kernel(StageK a) {
   double mval = 0.0;
   if (inside) {
     const int64_t k = s * a.in_slice_stride + static_cast<int64_t>(j) * a.nx + i;
+    // the cell's values load with its mask (one round trip of latency); a masked cell stages zeros
     const bool act = a.mask == nullptr || a.mask[s * a.mask_stride + static_cast<int64_t>(j) * a.nx + i] != 0;
+    double f[4] = {0.0, 0.0, 0.0, 0.0};
+    const int nl = MODE == kModePiSphere ? 2 : a.nf;
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+      if (m < nl) f[m] = load_any(a.f[m], a.dtype, k);
+    double sl = 0.0, cl = 0.0, sp = 0.0, cp = 0.0;
+    if (MODE == kModePiSphere) sl = a.sinlam[i], cl = a.coslam[i], sp = a.sinphi[j], cp = a.cosphi[j];
     mval = act ? 1.0 : 0.0;
     if (act) {
       if (MODE == kModePiSphere) {
-        const double u = load_any(a.f[0], a.dtype, k), v = load_any(a.f[1], a.dtype, k);
-        const double sl = a.sinlam[i], cl = a.coslam[i], sp = a.sinphi[j], cp = a.cosphi[j];
+        const double u = f[0], v = f[1];
         vals[0] = -sl * u - sp * cl * v;
         vals[1] = cl * u - sp * sl * v;
         vals[2] = cp * v;
       } else {
-        for (int m = 0; m < a.nf; ++m) vals[m] = load_any(a.f[m], a.dtype, k);
+        for (int m = 0; m < a.nf; ++m) vals[m] = f[m];
       }
       // an active non-finite value (or product, which the flux accumulates) flags the slice
       const int nv = MODE == kModePiSphere ? 3 : a.nf;

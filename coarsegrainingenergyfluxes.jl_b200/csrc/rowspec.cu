@@ -56,6 +56,7 @@ constexpr int kRsSeq = CGEF_RS_SEQ;          // quantities (rows) transformed to
 constexpr int kRsBatch = 4;                  // spectrum bins a thread loads before it uses any of them
 // longest row: two buffers of kRsSeq half-length rows (16 bytes a point) within 227 KB of shared memory
 constexpr int kRsMaxL = 4096 < (227 * 1024) / (16 * kRsSeq) ? 4096 : (227 * 1024) / (16 * kRsSeq);
+constexpr int kRsFftSmem = 2 * kRsSeq * 16 * (kRsMaxL / 2);  // the FFT kernels' shared-memory limit
 
 struct Fft {
   int L;   // real row length (even)
@@ -245,7 +246,7 @@ __device__ __forceinline__ void stockham_pass(const double2* a, double2* b, int 
 // The same pass with its input and output through functors: src(sq, n) gives element n of sequence sq,
 // sink(sq, n, v) takes element n of the pass's output.  The inverse transform writes its last pass
 // straight out as real samples, so that pass needs no shared-memory round trip and no barrier after it.
-template <int R, typename Src, typename Sink>
+template <int R, bool TW, typename Src, typename Sink>
 __device__ __forceinline__ void stockham_pass_io(Src src, Sink sink, int M, int Ns, unsigned ns_magic, int nseq,
                                                  const double2* ptw) {
   const int nb = M / R;
@@ -259,26 +260,30 @@ __device__ __forceinline__ void stockham_pass_io(Src src, Sink sink, int M, int 
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src(sq, j + r * nb);
+    if constexpr (TW) {
 #pragma unroll
-    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(ptw + (r - 1) * Ns + jm));
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(ptw + (r - 1) * Ns + jm));
+    }
     dft<R>(v);
 #pragma unroll
     for (int r = 0; r < R; ++r) sink(sq, jq * Ns * R + jm + r * Ns, v[r]);
   }
 }
 
-template <typename Src, typename Sink>
+template <bool TW, typename Src, typename Sink>
 __device__ __forceinline__ void pass_io(int R, Src src, Sink sink, int M, int Ns, unsigned mg, int nseq,
                                         const double2* ptw) {
   switch (R) {
-    case 2: stockham_pass_io<2>(src, sink, M, Ns, mg, nseq, ptw); break;
-    case 3: stockham_pass_io<3>(src, sink, M, Ns, mg, nseq, ptw); break;
-    case 4: stockham_pass_io<4>(src, sink, M, Ns, mg, nseq, ptw); break;
-    case 5: stockham_pass_io<5>(src, sink, M, Ns, mg, nseq, ptw); break;
-    case 8: stockham_pass_io<8>(src, sink, M, Ns, mg, nseq, ptw); break;
-    case 9: stockham_pass_io<9>(src, sink, M, Ns, mg, nseq, ptw); break;
-    case 10: stockham_pass_io<10>(src, sink, M, Ns, mg, nseq, ptw); break;
-    default: stockham_pass_io<16>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 2: stockham_pass_io<2, TW>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 3: stockham_pass_io<3, TW>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 4: stockham_pass_io<4, TW>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 5: stockham_pass_io<5, TW>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 8: stockham_pass_io<8, TW>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 9: stockham_pass_io<9, TW>(src, sink, M, Ns, mg, nseq, ptw); break;
+    case 10: stockham_pass_io<10, TW>(src, sink, M, Ns, mg, nseq, ptw); break;
+    default:  // radix 16; callers pass TW false only for the others (a third inlined copy spills)
+      if constexpr (TW) stockham_pass_io<16, true>(src, sink, M, Ns, mg, nseq, ptw);
+      break;
   }
 }
 
@@ -290,7 +295,7 @@ __device__ __forceinline__ double2* fft_block(double2* a, double2* b, int nseq, 
     const int R = f.rad[p];
     const unsigned mg = f.magic[p];
     const double2* tp = f.ptw + f.poff[p];
-    if (p == 0) {  // the first pass's twiddles are all 1: none are applied
+    if (p == 0 && R != 16) {  // the first pass's twiddles are all 1: none are applied (radix 16 below)
       switch (R) {
         case 2: stockham_pass<2, false>(a, b, f.M, Ns, mg, nseq, tp); break;
         case 3: stockham_pass<3, false>(a, b, f.M, Ns, mg, nseq, tp); break;
@@ -299,7 +304,7 @@ __device__ __forceinline__ double2* fft_block(double2* a, double2* b, int nseq, 
         case 8: stockham_pass<8, false>(a, b, f.M, Ns, mg, nseq, tp); break;
         case 9: stockham_pass<9, false>(a, b, f.M, Ns, mg, nseq, tp); break;
         case 10: stockham_pass<10, false>(a, b, f.M, Ns, mg, nseq, tp); break;
-        default: stockham_pass<16, false>(a, b, f.M, Ns, mg, nseq, tp); break;
+        default: break;
       }
     } else {
       switch (R) {
@@ -432,8 +437,11 @@ __device__ __forceinline__ void cp_async_wait() {
 constexpr int kAccStages = CGEF_ACC_STAGES;
 constexpr int kAccRps = CGEF_ACC_RPS;  // source rows a pipeline stage holds (one block barrier each)
 // target rows of an accumulation block: 16 at every band height (32-row blocks, one per SM, were 15%
-// slower at 2000 km: every row's barrier then stalls the whole SM)
-constexpr int kAccRows = 16;
+// slower at 2000 km and 14% slower at 100 km: every stage's barrier then stalls the whole SM)
+#ifndef CGEF_ACC_ROWS
+#define CGEF_ACC_ROWS 16
+#endif
+constexpr int kAccRows = CGEF_ACC_ROWS;
 
 template <int NA>
 struct AccTile {
@@ -613,11 +621,14 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(Rs
     const double2* src = a;
     auto from_smem = [src, M](int e, int n) { return src[e * M + n]; };
     if (pass == np - 1) {
-      pass_io(R, from_smem, to_row, M, Ns, mg, nseq, k.f.ptw + k.f.poff[pass]);
+      pass_io<true>(R, from_smem, to_row, M, Ns, mg, nseq, k.f.ptw + k.f.poff[pass]);
     } else {
       double2* dst = b;
-      pass_io(R, from_smem, [dst, M](int e, int n, double2 v) { dst[e * M + n] = v; }, M, Ns, mg, nseq,
-              k.f.ptw + k.f.poff[pass]);
+      auto to_smem = [dst, M](int e, int n, double2 v) { dst[e * M + n] = v; };
+      if (pass == 0 && R != 16)  // the first pass's twiddles are all 1: none are applied
+        pass_io<false>(R, from_smem, to_smem, M, Ns, mg, nseq, k.f.ptw + k.f.poff[pass]);
+      else
+        pass_io<true>(R, from_smem, to_smem, M, Ns, mg, nseq, k.f.ptw + k.f.poff[pass]);
       __syncthreads();
       double2* t = a;
       a = b;
@@ -693,17 +704,16 @@ int rs_check(const char* what) {
   return CGEF_OK;
 }
 
-// Opts an FFT kernel into the shared memory its two L-point buffers need (once per kernel and
-// device).
-int rs_smem_attr(const void* kernel) {
+// Opts a row-spectral kernel into `bytes` of dynamic shared memory (once per kernel and device): the
+// FFT kernels' two L-point buffers, or the accumulation's pipeline stages.
+int rs_smem_attr(const void* kernel, int bytes) {
   static std::mutex mu;
   static std::set<std::pair<const void*, int>> done;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
   std::lock_guard<std::mutex> lock(mu);
   if (done.count({kernel, dev})) return CGEF_OK;
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       2 * kRsSeq * static_cast<int>(sizeof(double2)) * (kRsMaxL / 2));
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(row-spectral FFT)");
   done.insert({kernel, dev});
   return CGEF_OK;
@@ -758,8 +768,10 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
   k.F = scratch;
   const int smem = 2 * kRsSeq * static_cast<int>(sizeof(double2)) * (p->rs_L / 2);
   int rc;
-  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_forward_kernel<MODE, NF, DEF>))) != CGEF_OK) return rc;
-  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_inverse_kernel<NA>))) != CGEF_OK) return rc;
+  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_forward_kernel<MODE, NF, DEF>), kRsFftSmem)) != CGEF_OK)
+    return rc;
+  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_inverse_kernel<NA>), kRsFftSmem)) != CGEF_OK)
+    return rc;
   prof_begin(CGEF_KERNEL_ROWSPEC, st);
   const dim3 rows(NC, p->ny, a.nslices);
   if (share.in == nullptr) {
@@ -770,7 +782,8 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
     constexpr int RW = AccTile<NA>::RW;
     const int acc_smem = kAccStages * kAccRps * (NA * 32 * 16 + kAccRows * 32 * 8);
     const dim3 g(p->rs_nkp / 32, (p->ny + kAccRows - 1) / kAccRows, a.nslices);
-    if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<kAccRows, NA>))) == CGEF_OK)
+    rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<kAccRows, NA>), acc_smem);
+    if (rc == CGEF_OK)
       rs_accumulate_kernel<kAccRows, NA><<<g, 32 * (kAccRows / RW), acc_smem, st>>>(k);
     if (rc == CGEF_OK) rc = rs_check("rs_accumulate_kernel");
   }
@@ -1079,8 +1092,10 @@ int run_spectral(const cgef_plan* p, const double* planes, int pitch, int np, in
   const int smem = 2 * kRsSeq * static_cast<int>(sizeof(double2)) * (p->rs_L / 2);
   const int csmem = 2 * c.cb * (p->ny + 1) * static_cast<int>(sizeof(double2));
   int rc;
-  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_forward_kernel<MODE, NF, DEF>))) != CGEF_OK) return rc;
-  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_inverse_kernel<NA>))) != CGEF_OK) return rc;
+  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_forward_kernel<MODE, NF, DEF>), kRsFftSmem)) != CGEF_OK)
+    return rc;
+  if ((rc = rs_smem_attr(reinterpret_cast<const void*>(rs_inverse_kernel<NA>), kRsFftSmem)) != CGEF_OK)
+    return rc;
   if ((rc = sp_smem_attr()) != CGEF_OK) return rc;
   prof_begin(CGEF_KERNEL_ROWSPEC, st);
   const dim3 rows(NC, p->ny, nbatch);
@@ -1174,7 +1189,7 @@ int build_row_spectra(cgef_plan* p) {
   p->rs_nkp = nkp;
   p->rs_nrad = static_cast<int>(rad.size());
   for (size_t i = 0; i < rad.size(); ++i) p->rs_rad[i] = rad[i];
-  int rc = rs_smem_attr(reinterpret_cast<const void*>(rs_kspec_kernel));
+  int rc = rs_smem_attr(reinterpret_cast<const void*>(rs_kspec_kernel), kRsFftSmem);
   if (rc == CGEF_OK) {
     const int smem = 2 * kRsSeq * static_cast<int>(sizeof(double2)) * (L / 2);
     rs_kspec_kernel<<<static_cast<unsigned>((nrows + kRsSeq - 1) / kRsSeq), kRsThreads, smem>>>(
