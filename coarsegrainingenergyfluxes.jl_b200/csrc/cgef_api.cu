@@ -753,7 +753,29 @@ int32_t cgef_plan_autotune(cgef_plan* p, int32_t nbatch, double* chosen) {
   }
   p->rs_on = false;
   double best = p->sched[0].waves, best_ms = 1e300;
-  if (rc == CGEF_OK) rc = time_pass(flux_pass, &best_ms);
+  // a lower bound on the direct gather's time: its multiply-adds (one per quantity and entry pair of
+  // each active target: mirrored columns are paired) at 22.5e12 a second, above the B200's FP64 peak.
+  // Where even that is twice the spectral evaluation's time, the direct gather is not timed at all.
+  // Only where every target has its band's full entry count: on the sphere (bands hold in-domain rows
+  // only, x periodic) and on doubly periodic planes.
+  bool direct_hopeless = false;
+  if (rc == CGEF_OK && rs_avail && p->periodic_x && (p->geometry == CGEF_SPHERICAL || p->periodic_y)) {
+    const int na = (p->geometry == CGEF_SPHERICAL ? 9 : 5) + (p->strategy == CGEF_DEFORMABLE ? 1 : 0);
+    double fma = 0.0;
+    for (int j = 0; j < p->ny; ++j) {
+      const size_t band = p->geometry == CGEF_SPHERICAL ? static_cast<size_t>(j) : 0;
+      if (band + 1 >= p->h_ptr.size()) break;
+      int64_t act = p->nx;
+      if (!p->h_mask.empty()) {
+        act = 0;
+        for (int i = 0; i < p->nx; ++i) act += p->h_mask[static_cast<size_t>(j) * p->nx + i] != 0;
+      }
+      fma += static_cast<double>(p->h_ptr[band + 1] - p->h_ptr[band]) * static_cast<double>(act);
+    }
+    const double lb_ms = 1e3 * fma * nbatch * na * 0.5 / 22.5e12;
+    direct_hopeless = lb_ms > 2.0 * ms_rs;
+  }
+  if (rc == CGEF_OK && !direct_hopeless) rc = time_pass(flux_pass, &best_ms);
   const bool spectral_clear = rc == CGEF_OK && rs_avail && best_ms > 2.0 * ms_rs;
   // 1. split granularity of the direct flux gather's schedule
   const double cand[4] = {2.0, 4.0, 8.0, 16.0};
