@@ -29,6 +29,9 @@
 #include <utility>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "banded_common.cuh"
 #include "cgef_internal.h"
 
@@ -427,7 +430,7 @@ __device__ __forceinline__ void cp_async_wait() {
 // shared-memory reads).  Rows off a bounded y axis are skipped (the direct sum skips them); on a
 // periodic y axis they wrap.  Three rows a stage (104 KB of shared memory a block, two blocks an SM)
 // made the 0.25 degree flux step 4% faster than one row a stage; six one-row stages or two-row
-// stages gained less.
+// stages gained less.  Banded spheres stage through tensor copies instead (rs_accumulate_tma_kernel).
 #ifndef CGEF_ACC_STAGES
 #define CGEF_ACC_STAGES 4
 #endif
@@ -559,6 +562,162 @@ __global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1) rs_accumulate_
   for (int t = 0; t < RW; ++t) {
     const int j = j0 + rg * RW + t;
     if (j >= k.ny) break;
+    double2* sr = Ss + static_cast<int64_t>(j) * NA * nkp;
+#pragma unroll
+    for (int m = 0; m < NA; ++m) sr[m * nkp] = acc[t][m];
+  }
+}
+
+// The same sums with each source row staged by two tensor copies (TMA): one box of the row's spectra
+// (32 bins x every quantity) and one of the TJ target rows' kernel-spectrum slices, the latter through a
+// 3-D view of the kernel spectra whose axes are the bin, D + the source row and the target row (the
+// entry of target j, source row jr is row j (2D) + D + jr of the table, so the target axis has stride
+// 2D rows).  One thread issues both copies onto the stage's mbarrier; there is no per-thread copy
+// arithmetic.  Slices of target rows out of the band are read (finite neighbours in the table) and
+// ignored: their kernel values are taken as 0.  Banded spheres (one band per row, bounded y, D >= 1)
+// only; every wait is bounded and a block whose barrier does not complete writes NaN sums.
+#ifndef CGEF_ACC_TMA
+#define CGEF_ACC_TMA 1
+#endif
+constexpr long long kAccWaitCycles = 200000000LL;  // about 0.1 s
+
+__device__ __forceinline__ uint32_t tma_smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void tma_bar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tma_bar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool tma_bar_wait(uint32_t bar, uint32_t parity, long long limit) {
+  const long long start = clock64();
+  for (int it = 1;; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 63) == 0 && clock64() - start > limit) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+template <int TJ, int NA>
+__global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1)
+    rs_accumulate_tma_kernel(RsK k, const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap kmap) {
+  extern __shared__ __align__(128) unsigned char rs_tma_smem[];
+  __shared__ __align__(8) uint64_t full[kAccStages];
+  constexpr int RW = AccTile<NA>::RW;
+  constexpr int qbytes = NA * 32 * 16;
+  constexpr int sbytes = qbytes + TJ * 32 * 8;  // one source row's boxes, both multiples of 128 bytes
+  static_assert(qbytes % 128 == 0 && sbytes % 128 == 0, "tensor-copy destinations 128-byte aligned");
+  const int lane = threadIdx.x & 31;
+  const int rg = threadIdx.x >> 5;  // the warp's rows: rg * RW .. rg * RW + RW - 1
+  const int q0 = blockIdx.x * 32;
+  const int j0 = blockIdx.y * TJ;
+  const int s = blockIdx.z;
+  const int nkp = k.f.nkp;
+  const int D = k.D, ny = k.ny;
+  const int st0 = max(0, D - j0), st1 = min(TJ + 2 * D, ny - j0 + D);  // in-domain source rows only
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kAccStages; ++b) tma_bar_init(tma_smem_u32(&full[b]));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // thread 0: the copies of the stage that starts at source step sg, into buffer buf
+  auto issue = [&](int sg, int buf) {
+    const uint32_t bar = tma_smem_u32(&full[buf]);
+    const int nrows = min(kAccRps, st1 - sg);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tma_bar_expect(bar, static_cast<uint32_t>(nrows * sbytes));
+    for (int r = 0; r < nrows; ++r) {
+      const int jraw = j0 - D + sg + r;
+      const uint32_t dst = tma_smem_u32(rs_tma_smem + (buf * kAccRps + r) * sbytes);
+      tma_load_2d(dst, &qmap, 2 * q0, (s * ny + jraw) * NA, bar);
+      tma_load_3d(dst + qbytes, &kmap, q0, D + jraw, j0, bar);
+    }
+  };
+  double2 acc[RW][NA];
+#pragma unroll
+  for (int t = 0; t < RW; ++t)
+#pragma unroll
+    for (int m = 0; m < NA; ++m) acc[t][m] = make_double2(0.0, 0.0);
+  const int ng = (st1 - st0 + kAccRps - 1) / kAccRps;  // stages of this block
+  if (threadIdx.x == 0)
+    for (int i = 0; i < kAccStages - 1 && i < ng; ++i) issue(st0 + i * kAccRps, i);
+  int failed = -1;
+  for (int gi = 0; gi < ng; ++gi) {
+    const int sg = st0 + gi * kAccRps, buf = gi % kAccStages;
+    const bool got = tma_bar_wait(tma_smem_u32(&full[buf]), (gi / kAccStages) & 1, kAccWaitCycles);
+    if (__syncthreads_or(!got)) {
+      failed = gi;
+      break;
+    }
+    const int nx = gi + kAccStages - 1;
+    if (threadIdx.x == 0 && nx < ng) issue(st0 + nx * kAccRps, nx % kAccStages);
+    const unsigned char* sb = rs_tma_smem + buf * kAccRps * sbytes;
+#pragma unroll
+    for (int r = 0; r < kAccRps; ++r) {
+      const int st = sg + r;
+      if (st >= st1) break;
+      const unsigned char* b = sb + r * sbytes;
+      const double2* qb = reinterpret_cast<const double2*>(b) + lane;
+      const double* kb = reinterpret_cast<const double*>(b + qbytes) + rg * RW * 32 + lane;
+      double kv[RW];
+#pragma unroll
+      for (int t = 0; t < RW; ++t)  // target row j0 + rg RW + t is in this source row's band
+        kv[t] = static_cast<unsigned>(st - rg * RW - t) <= static_cast<unsigned>(2 * D) ? kb[t * 32] : 0.0;
+#pragma unroll
+      for (int m = 0; m < NA; ++m) {
+        const double2 a = qb[m * 32];
+#pragma unroll
+        for (int t = 0; t < RW; ++t) {
+          acc[t][m].x = fma(kv[t], a.x, acc[t][m].x);
+          acc[t][m].y = fma(kv[t], a.y, acc[t][m].y);
+        }
+      }
+    }
+  }
+  if (failed >= 0) {
+    // a barrier did not complete: let the copies still in flight land (bounded again), then give NaN
+    // sums so the result cannot pass for a valid one
+    const int issued = min(ng, failed + kAccStages - 1);
+    for (int gi = failed; gi < issued; ++gi)
+      tma_bar_wait(tma_smem_u32(&full[gi % kAccStages]), (gi / kAccStages) & 1, kAccWaitCycles / 8);
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+    for (int t = 0; t < RW; ++t)
+#pragma unroll
+      for (int m = 0; m < NA; ++m) acc[t][m] = make_double2(nan, nan);
+  }
+  double2* Ss = k.S + static_cast<int64_t>(s) * ny * NA * nkp + q0 + lane;
+#pragma unroll
+  for (int t = 0; t < RW; ++t) {
+    const int j = j0 + rg * RW + t;
+    if (j >= ny) break;
     double2* sr = Ss + static_cast<int64_t>(j) * NA * nkp;
 #pragma unroll
     for (int m = 0; m < NA; ++m) sr[m * nkp] = acc[t][m];
@@ -704,6 +863,46 @@ int rs_check(const char* what) {
   return CGEF_OK;
 }
 
+// The driver's tensor-map encoder, through the runtime (no link against the driver library); null
+// when the driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// The accumulation's two tensor maps: the source spectra as doubles [slice row quantity][2 nkp] with
+// 64 x NA boxes, and the kernel spectra as [target row][D + source row][bin] with 32 x 1 x kAccRows
+// boxes (the target axis strides 2D table rows).  False where a map cannot be encoded.
+bool rs_tma_maps(const RsK& k, int na, CUtensorMap* qm, CUtensorMap* km) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t nkp = static_cast<cuuint64_t>(k.f.nkp);
+  const cuuint32_t one[3] = {1, 1, 1};
+  const cuuint64_t qdim[2] = {2 * nkp, static_cast<cuuint64_t>(k.nslices) * k.ny * na};
+  const cuuint64_t qstr[1] = {2 * nkp * sizeof(double)};
+  const cuuint32_t qbox[2] = {64, static_cast<cuuint32_t>(na)};
+  if (enc(qm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, static_cast<void*>(k.Q), qdim, qstr, qbox, one,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  const cuuint64_t kdim[3] = {nkp, static_cast<cuuint64_t>(k.ny + 2 * k.D), static_cast<cuuint64_t>(k.ny)};
+  const cuuint64_t kstr[2] = {nkp * sizeof(double), static_cast<cuuint64_t>(2 * k.D) * nkp * sizeof(double)};
+  const cuuint32_t kbox[3] = {32, 1, static_cast<cuuint32_t>(kAccRows)};
+  return enc(km, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(k.kspec), kdim, kstr, kbox, one,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Opts a row-spectral kernel into `bytes` of dynamic shared memory (once per kernel and device): the
 // FFT kernels' two L-point buffers, or the accumulation's pipeline stages.
 int rs_smem_attr(const void* kernel, int bytes) {
@@ -782,9 +981,17 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
     constexpr int RW = AccTile<NA>::RW;
     const int acc_smem = kAccStages * kAccRps * (NA * 32 * 16 + kAccRows * 32 * 8);
     const dim3 g(p->rs_nkp / 32, (p->ny + kAccRows - 1) / kAccRows, a.nslices);
-    rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<kAccRows, NA>), acc_smem);
-    if (rc == CGEF_OK)
-      rs_accumulate_kernel<kAccRows, NA><<<g, 32 * (kAccRows / RW), acc_smem, st>>>(k);
+    CUtensorMap qm, km;
+    const bool tma = CGEF_ACC_TMA && k.band_stride != 0 && !k.periodic_y && k.D >= 1 && rs_tma_maps(k, NA, &qm, &km);
+    if (tma) {
+      rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_tma_kernel<kAccRows, NA>), acc_smem);
+      if (rc == CGEF_OK)
+        rs_accumulate_tma_kernel<kAccRows, NA><<<g, 32 * (kAccRows / RW), acc_smem, st>>>(k, qm, km);
+    } else {
+      rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<kAccRows, NA>), acc_smem);
+      if (rc == CGEF_OK)
+        rs_accumulate_kernel<kAccRows, NA><<<g, 32 * (kAccRows / RW), acc_smem, st>>>(k);
+    }
     if (rc == CGEF_OK) rc = rs_check("rs_accumulate_kernel");
   }
   if (rc == CGEF_OK) {
