@@ -330,6 +330,53 @@ __device__ __forceinline__ double2* fft_block(double2* a, double2* b, int nseq, 
   return a;
 }
 
+// The same passes with every size known at compile time, for the transform length the 0.25 degree
+// sphere uses (M = 720 = 10 x 9 x 8): no radix dispatch, the butterfly range and Ns fixed, the
+// division by Ns a constant one.  Same arithmetic, same results.
+#ifndef CGEF_RS_CT720
+#define CGEF_RS_CT720 1
+#endif
+
+template <int R, int NS, int M, bool TW, typename Src, typename Sink>
+__device__ __forceinline__ void stockham_pass_ct(Src src, Sink sink, int nseq, const double2* ptw) {
+  constexpr int nb = M / R;
+  for (int t = threadIdx.x; t < nseq * nb; t += kRsThreads) {
+    int sq = 0, j = t;
+#pragma unroll
+    for (int e = 1; e < kRsSeq; ++e)
+      if (j >= nb) j -= nb, ++sq;
+    const int jq = j / NS, jm = j - jq * NS;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src(sq, j + r * nb);
+    if constexpr (TW) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(ptw + (r - 1) * NS + jm));
+    }
+    dft<R>(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) sink(sq, jq * NS * R + jm + r * NS, v[r]);
+  }
+}
+
+// The three passes of a 720-point transform through shared memory (a, then b as scratch); the last
+// pass's output goes to `last` (a sink); returns after the passes (no barrier after the last).
+template <typename Last>
+__device__ __forceinline__ void fft720(double2* a, double2* b, int nseq, const Fft& f, Last last) {
+  constexpr int M = 720;
+  auto from = [](const double2* s) { return [s](int e, int n) { return s[e * M + n]; }; };
+  auto to = [](double2* d) { return [d](int e, int n, double2 v) { d[e * M + n] = v; }; };
+  stockham_pass_ct<10, 1, M, false>(from(a), to(b), nseq, f.ptw + f.poff[0]);
+  __syncthreads();
+  stockham_pass_ct<9, 10, M, true>(from(b), to(a), nseq, f.ptw + f.poff[1]);
+  __syncthreads();
+  stockham_pass_ct<8, 90, M, true>(from(a), last, nseq, f.ptw + f.poff[2]);
+}
+
+__host__ __device__ inline bool is_fft720(const Fft& f) {
+  return f.M == 720 && f.nrad == 3 && f.rad[0] == 10 && f.rad[1] == 9 && f.rad[2] == 8;
+}
+
 struct RsK {
   Fft f;
   const double* planes;
@@ -378,7 +425,14 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(Rs
     }
   }
   __syncthreads();
-  const double2* z = fft_block(a, b, nseq, k.f);
+  const double2* z;
+  if (CGEF_RS_CT720 && is_fft720(k.f)) {
+    fft720(a, b, nseq, k.f, [b](int e, int n, double2 v) { b[e * 720 + n] = v; });
+    __syncthreads();
+    z = b;
+  } else {
+    z = fft_block(a, b, nseq, k.f);
+  }
   // bin q of sequence e is item t = e * nk + q; a thread loads kRsBatch items' operands, then stores
   const int nk = k.f.nk, items = nseq * nk;
   double2* Q0 = k.Q + ((static_cast<int64_t>(s) * k.ny + jr) * C::NA + m0) * k.f.nkp;
@@ -772,6 +826,10 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(Rs
     if (2 * n < nx) Fe[2 * n] = z.x;
     if (2 * n + 1 < nx) Fe[2 * n + 1] = -z.y;
   };
+  if (CGEF_RS_CT720 && is_fft720(k.f)) {
+    fft720(a, b, nseq, k.f, to_row);
+    return;
+  }
   const int np = k.f.nrad;
   int Ns = 1;
   for (int pass = 0; pass < np; ++pass) {
