@@ -679,8 +679,16 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
+// Two source rows a stage and three blocks an SM (168 registers, 70 KB of shared memory a block) where
+// the tile fits without spilling (NA <= 9): 2.8% faster on the 24-scale sweep than three rows a stage
+// at two blocks an SM.
+constexpr int kTmaRps = 2;
+template <int NA>
+constexpr int tma_min_blocks() {
+  return NA <= 9 ? 3 : 1;
+}
 template <int TJ, int NA>
-__global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1)
+__global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), tma_min_blocks<NA>())
     rs_accumulate_tma_kernel(RsK k, const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap kmap) {
   extern __shared__ __align__(128) unsigned char rs_tma_smem[];
   __shared__ __align__(8) uint64_t full[kAccStages];
@@ -704,12 +712,12 @@ __global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1)
   // thread 0: the copies of the stage that starts at source step sg, into buffer buf
   auto issue = [&](int sg, int buf) {
     const uint32_t bar = tma_smem_u32(&full[buf]);
-    const int nrows = min(kAccRps, st1 - sg);
+    const int nrows = min(kTmaRps, st1 - sg);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tma_bar_expect(bar, static_cast<uint32_t>(nrows * sbytes));
     for (int r = 0; r < nrows; ++r) {
       const int jraw = j0 - D + sg + r;
-      const uint32_t dst = tma_smem_u32(rs_tma_smem + (buf * kAccRps + r) * sbytes);
+      const uint32_t dst = tma_smem_u32(rs_tma_smem + (buf * kTmaRps + r) * sbytes);
       tma_load_2d(dst, &qmap, 2 * q0, (s * ny + jraw) * NA, bar);
       tma_load_3d(dst + qbytes, &kmap, q0, D + jraw, j0, bar);
     }
@@ -719,22 +727,22 @@ __global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), 1)
   for (int t = 0; t < RW; ++t)
 #pragma unroll
     for (int m = 0; m < NA; ++m) acc[t][m] = make_double2(0.0, 0.0);
-  const int ng = (st1 - st0 + kAccRps - 1) / kAccRps;  // stages of this block
+  const int ng = (st1 - st0 + kTmaRps - 1) / kTmaRps;  // stages of this block
   if (threadIdx.x == 0)
-    for (int i = 0; i < kAccStages - 1 && i < ng; ++i) issue(st0 + i * kAccRps, i);
+    for (int i = 0; i < kAccStages - 1 && i < ng; ++i) issue(st0 + i * kTmaRps, i);
   int failed = -1;
   for (int gi = 0; gi < ng; ++gi) {
-    const int sg = st0 + gi * kAccRps, buf = gi % kAccStages;
+    const int sg = st0 + gi * kTmaRps, buf = gi % kAccStages;
     const bool got = tma_bar_wait(tma_smem_u32(&full[buf]), (gi / kAccStages) & 1, kAccWaitCycles);
     if (__syncthreads_or(!got)) {
       failed = gi;
       break;
     }
     const int nx = gi + kAccStages - 1;
-    if (threadIdx.x == 0 && nx < ng) issue(st0 + nx * kAccRps, nx % kAccStages);
-    const unsigned char* sb = rs_tma_smem + buf * kAccRps * sbytes;
+    if (threadIdx.x == 0 && nx < ng) issue(st0 + nx * kTmaRps, nx % kAccStages);
+    const unsigned char* sb = rs_tma_smem + buf * kTmaRps * sbytes;
 #pragma unroll
-    for (int r = 0; r < kAccRps; ++r) {
+    for (int r = 0; r < kTmaRps; ++r) {
       const int st = sg + r;
       if (st >= st1) break;
       const unsigned char* b = sb + r * sbytes;
@@ -1038,13 +1046,14 @@ int run_rowspec(const cgef_plan* p, const BandedK& a, double* scratch, const RsS
   if (rc == CGEF_OK) {
     constexpr int RW = AccTile<NA>::RW;
     const int acc_smem = kAccStages * kAccRps * (NA * 32 * 16 + kAccRows * 32 * 8);
+    const int tma_smem = kAccStages * kTmaRps * (NA * 32 * 16 + kAccRows * 32 * 8);
     const dim3 g(p->rs_nkp / 32, (p->ny + kAccRows - 1) / kAccRows, a.nslices);
     CUtensorMap qm, km;
     const bool tma = CGEF_ACC_TMA && k.band_stride != 0 && !k.periodic_y && k.D >= 1 && rs_tma_maps(k, NA, &qm, &km);
     if (tma) {
-      rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_tma_kernel<kAccRows, NA>), acc_smem);
+      rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_tma_kernel<kAccRows, NA>), tma_smem);
       if (rc == CGEF_OK)
-        rs_accumulate_tma_kernel<kAccRows, NA><<<g, 32 * (kAccRows / RW), acc_smem, st>>>(k, qm, km);
+        rs_accumulate_tma_kernel<kAccRows, NA><<<g, 32 * (kAccRows / RW), tma_smem, st>>>(k, qm, km);
     } else {
       rc = rs_smem_attr(reinterpret_cast<const void*>(rs_accumulate_kernel<kAccRows, NA>), acc_smem);
       if (rc == CGEF_OK)
