@@ -860,9 +860,9 @@ def measure_sweep(args, name, rank, world, local, dist, *, snapshots=1, scale_km
         traffic, traffic_basis, traffic_one = committed_traffic(f"{name}:rowspec", nsl, scale_km)
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": traffic, "traffic_basis": traffic_basis, "traffic_one_snapshot": traffic_one,
-                    "kernel": "rs_forward_kernel + rs_accumulate_kernel + rs_inverse_kernel (row-spectral footprint "
-                              "sums: FFTs along x, banded spectral sums, inverse FFTs; the epilogue runs in the strain "
-                              "pass)",
+                    "kernel": "rs_forward_kernel + rs_accumulate_tma_kernel (rs_accumulate_kernel off the sphere) + "
+                              "rs_inverse_kernel (row-spectral footprint sums: FFTs along x, banded spectral sums, "
+                              "inverse FFTs; the epilogue runs in the strain pass)",
                     "per_launch_ms": per_launch_ms, "launches": cnt, "algorithmic_bytes_per_launch": bytes_launch,
                     "direct_sum_equivalent_tflops": flops_all / launches_per_step / (per_launch_ms * 1e-3) / 1e12
                     if not direct_plans else None,
