@@ -393,11 +393,14 @@ struct RsK {
 // row's even and odd samples form one half-length complex sequence z, and with Z = FFT(z) the row's
 // spectrum is X_k = E_k + exp(-2 pi i k / L) O_k, E_k = (Z_k + conj Z_{M-k}) / 2,
 // O_k = (Z_k - conj Z_{M-k}) / 2i, for k = 0 .. M (Z_M = Z_0).
-template <int MODE, int NF, bool DEF>
-__global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(RsK k) {
+// LC: the real row length when known at compile time (1440 with the 720-point passes), else 0.
+template <int MODE, int NF, bool DEF, int LC>
+__device__ __forceinline__ void forward_body(const RsK& k) {
   using C = Cfg<MODE, NF, DEF>;
   extern __shared__ double2 rs_smem[];
-  const int M = k.f.M;
+  const int L = LC ? LC : k.f.L;
+  const int M = LC ? LC / 2 : k.f.M;
+  const int nkp = LC ? (LC / 2 + 1 + 31) / 32 * 32 : k.f.nkp;
   double2* a = rs_smem;
   double2* b = rs_smem + kRsSeq * M;
   const int m0 = blockIdx.x * kRsSeq, jr = blockIdx.y, s = blockIdx.z;
@@ -405,7 +408,7 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(Rs
   const double* row = k.planes + s * k.slice_stride + static_cast<int64_t>(jr) * k.pitch + k.halo;
   double* ad = reinterpret_cast<double*>(a);
   // kRsCols columns per thread at a time, their loads issued together
-  for (int i0 = 0; i0 < k.f.L; i0 += kRsCols * kRsThreads) {
+  for (int i0 = 0; i0 < L; i0 += kRsCols * kRsThreads) {
     double v[kRsCols][C::NP];
 #pragma unroll
     for (int c = 0; c < kRsCols; ++c) {
@@ -417,16 +420,16 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(Rs
 #pragma unroll
     for (int c = 0; c < kRsCols; ++c) {
       const int i = i0 + c * kRsThreads + threadIdx.x;
-      if (i >= k.f.L) break;
+      if (i >= L) break;
 #pragma unroll
       for (int e = 0; e < kRsSeq; ++e)
         if (e < nseq)  // sample i of sequence e: z[i/2].x (even i) or .y (odd)
-          ad[e * k.f.L + i] = i < k.nx ? quantity<MODE, NF, DEF>(v[c], m0 + e) : 0.0;
+          ad[e * L + i] = i < k.nx ? quantity<MODE, NF, DEF>(v[c], m0 + e) : 0.0;
     }
   }
   __syncthreads();
   const double2* z;
-  if (CGEF_RS_CT720 && is_fft720(k.f)) {
+  if constexpr (LC == 1440) {
     fft720(a, b, nseq, k.f, [b](int e, int n, double2 v) { b[e * 720 + n] = v; });
     __syncthreads();
     z = b;
@@ -434,8 +437,8 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(Rs
     z = fft_block(a, b, nseq, k.f);
   }
   // bin q of sequence e is item t = e * nk + q; a thread loads kRsBatch items' operands, then stores
-  const int nk = k.f.nk, items = nseq * nk;
-  double2* Q0 = k.Q + ((static_cast<int64_t>(s) * k.ny + jr) * C::NA + m0) * k.f.nkp;
+  const int nk = LC ? LC / 2 + 1 : k.f.nk, items = nseq * nk;
+  double2* Q0 = k.Q + ((static_cast<int64_t>(s) * k.ny + jr) * C::NA + m0) * nkp;
   for (int t0 = 0; t0 < items; t0 += kRsBatch * kRsThreads) {
     double2 w[kRsBatch], zq[kRsBatch], zc[kRsBatch];
 #pragma unroll
@@ -458,10 +461,18 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(Rs
           if (q >= nk) q -= nk, ++e;
         const double2 E = make_double2(0.5 * (zq[u].x + zc[u].x), 0.5 * (zq[u].y + zc[u].y));
         const double2 O = make_double2(0.5 * (zq[u].y - zc[u].y), -0.5 * (zq[u].x - zc[u].x));  // (zq - zc) / 2i
-        Q0[e * k.f.nkp + q] = cadd(E, cmul(w[u], O));
+        Q0[e * nkp + q] = cadd(E, cmul(w[u], O));
       }
     }
   }
+}
+
+template <int MODE, int NF, bool DEF>
+__global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_forward_kernel(RsK k) {
+  if (CGEF_RS_CT720 && is_fft720(k.f))
+    forward_body<MODE, NF, DEF, 1440>(k);
+  else
+    forward_body<MODE, NF, DEF, 0>(k);
 }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, bool fill) {
@@ -790,15 +801,16 @@ __global__ void __launch_bounds__(32 * (TJ / AccTile<NA>::RW), tma_min_blocks<NA
 // and O'_k = (S_k - conj S_{M-k}) exp(2 pi i k / L), z = IDFT_M(E' + i O') (unnormalised, taken as
 // the conjugate of the forward FFT of the conjugate) holds the row's even samples in its real parts
 // and its odd samples in its imaginary parts (the kernel spectra carry the 1/L).
-template <int NA>
-__global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(RsK k) {
+template <int NA, int LC>
+__device__ __forceinline__ void inverse_body(const RsK& k) {
   extern __shared__ double2 rs_smem[];
-  const int M = k.f.M;
+  const int M = LC ? LC / 2 : k.f.M;
+  const int nkp = LC ? (LC / 2 + 1 + 31) / 32 * 32 : k.f.nkp;
   double2* a = rs_smem;
   double2* b = rs_smem + kRsSeq * M;
   const int m0 = blockIdx.x * kRsSeq, j = blockIdx.y, s = blockIdx.z;
   const int nseq = min(kRsSeq, NA - m0);
-  const double2* S = k.S + ((static_cast<int64_t>(s) * k.ny + j) * NA + m0) * k.f.nkp;
+  const double2* S = k.S + ((static_cast<int64_t>(s) * k.ny + j) * NA + m0) * nkp;
   // bin q of sequence e is item t = e * M + q; a thread loads kRsBatch items' operands, then stores
   const int items = nseq * M;
   for (int t0 = 0; t0 < items; t0 += kRsBatch * kRsThreads) {
@@ -810,8 +822,8 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(Rs
       for (int i = 1; i < kRsSeq; ++i)
         if (q >= M) q -= M, ++e;
       w[u] = __ldg(k.f.tw + q);
-      sq[u] = S[e * k.f.nkp + q];
-      sc[u] = conj2(S[e * k.f.nkp + M - q]);
+      sq[u] = S[e * nkp + q];
+      sc[u] = conj2(S[e * nkp + M - q]);
     }
 #pragma unroll
     for (int u = 0; u < kRsBatch; ++u) {
@@ -834,7 +846,7 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(Rs
     if (2 * n < nx) Fe[2 * n] = z.x;
     if (2 * n + 1 < nx) Fe[2 * n + 1] = -z.y;
   };
-  if (CGEF_RS_CT720 && is_fft720(k.f)) {
+  if constexpr (LC == 1440) {
     fft720(a, b, nseq, k.f, to_row);
     return;
   }
@@ -861,6 +873,14 @@ __global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(Rs
     }
     Ns *= R;
   }
+}
+
+template <int NA>
+__global__ void __launch_bounds__(kRsThreads, kRsMinBlocks) rs_inverse_kernel(RsK k) {
+  if (CGEF_RS_CT720 && is_fft720(k.f))
+    inverse_body<NA, 1440>(k);
+  else
+    inverse_body<NA, 0>(k);
 }
 
 template <int MODE, int NF, bool DEF>
