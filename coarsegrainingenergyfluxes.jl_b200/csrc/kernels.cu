@@ -775,6 +775,9 @@ struct StrainK {
 #ifndef CGEF_STRAIN_BY
 #define CGEF_STRAIN_BY 8
 #endif
+#ifndef CGEF_STRAIN_LEAN
+#define CGEF_STRAIN_LEAN 1
+#endif
 constexpr int kStrainBX = 32, kStrainBY = CGEF_STRAIN_BY;
 
 // Finishing of the raw sums: the normalisation of finish_target (inactive targets and denominators
@@ -907,7 +910,7 @@ __device__ __forceinline__ StencilCase tile_case(unsigned char am1, unsigned cha
   return c;
 }
 
-template <bool RAW, int MODE, bool DEF>
+template <bool RAW, int MODE, bool DEF, bool FULL = true>
 __global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a) {
   constexpr int TW = kStrainBX + 2 * kStrainHalo, TH = kStrainBY + 2 * kStrainHalo;
   __shared__ double sh[2 * (kStrainBX * kStrainBY / 32)];
@@ -1046,6 +1049,7 @@ __global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a
       e_area = ar;
     }
     if (a.pi) store_any(a.pi, a.dtype, o, pi);
+    if constexpr (FULL) {  // FULL false: Pi and E only (no intermediate fields, splits or closure features)
     if (a.ub_o) store_any(a.ub_o, a.dtype, o, u0);
     if (a.vb_o) store_any(a.vb_o, a.dtype, o, v0);
     if (a.txx_o) store_any(a.txx_o, a.dtype, o, txx);
@@ -1080,8 +1084,9 @@ __global__ void __launch_bounds__(kStrainBX * kStrainBY) strain_kernel(StrainK a
         g_cnt = 1.0;
       }
     }
+    }
   }
-  if (a.gpartials) {
+  if (FULL && a.gpartials) {
     block_sum2(g_sum, g_cnt, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) {
       const int64_t nblk = static_cast<int64_t>(gridDim.x) * gridDim.y;
@@ -1636,8 +1641,18 @@ int launch_strain(const cgef_plan* p, const StrainArgs& s, cudaStream_t st) {
   dim3 block(kStrainBX, kStrainBY), grid((p->nx + kStrainBX - 1) / kStrainBX, (p->ny + kStrainBY - 1) / kStrainBY,
                                          s.nbatch);
   const bool sph = p->geometry == CGEF_SPHERICAL, def = p->strategy == CGEF_DEFORMABLE;
+  bool extra = a.ub_o || a.vb_o || a.txx_o || a.txy_o || a.tyy_o || a.sxx_o || a.sxy_o || a.syy_o || a.grad ||
+               a.gpartials;
+  for (int k = 0; k < 5; ++k) extra = extra || a.sc[k];
+  const bool lean = CGEF_STRAIN_LEAN && s.raw != nullptr && !extra;
   prof_begin(CGEF_KERNEL_STRAIN, st);
-  if (s.raw == nullptr)
+  if (lean && sph)
+    def ? strain_kernel<true, kModePiSphere, true, false><<<grid, block, 0, st>>>(a)
+        : strain_kernel<true, kModePiSphere, false, false><<<grid, block, 0, st>>>(a);
+  else if (lean)
+    def ? strain_kernel<true, kModePiCart, true, false><<<grid, block, 0, st>>>(a)
+        : strain_kernel<true, kModePiCart, false, false><<<grid, block, 0, st>>>(a);
+  else if (s.raw == nullptr)
     strain_kernel<false, kModePiSphere, false><<<grid, block, 0, st>>>(a);
   else if (sph)
     def ? strain_kernel<true, kModePiSphere, true><<<grid, block, 0, st>>>(a)
